@@ -1,0 +1,310 @@
+"""Throughput benchmark of the FDTD timestep hot path on B200.
+
+Workload: the two-sphere dielectric scene at 512^3 (spheres eps 4.0 r=80 at
+(160,256,256) and eps 2.25 r=60 at (352,256,256)), 16-cell CPML, Gaussian Ez
+source at (256,256,64), 8 Ez DFT probes on a line at z=448, FP32 fields.
+A step is one full Yee timestep of the whole grid (H, E, CPML psi, source,
+probes).  Metric: Mcell-updates/s = cells * steps / seconds / 1e6.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm prints one JSON line with `value` (device-resident, CUDA events on
+the handle's stream), `e2e` (through the C ABI from host buffers: upload of
+the scene, K steps, download of probe sums and one snapshot), `roofline`
+(fused kernel: algorithmic bytes per launch / event-timed launch duration),
+`cpu_baseline` (the CPU oracle restating the reference, timed on this host),
+and `clocks` sampled by nvidia-smi during the timed region.  With N > 1 each
+rank runs its own replica of the workload (the path needs no collective).
+The reference arm times the reference's CPU algorithm (the oracle port; the
+Rust reference cannot be built here) with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS = 512 ** 3
+METRIC = "Mcell-updates/s"
+WORKLOAD = "two_spheres_512^3_fp32_cpml16_gaussian_8probes"
+
+
+def algorithmic_bytes(sc) -> int:
+    """Per fused-kernel launch: 49 B per cell (6 f32 fields read + written, 1 B
+    material id) plus 32 B per (cell, axis) inside that axis's graded slab
+    (4 psi values read + written)."""
+    n = (sc.dims.nx, sc.dims.ny, sc.dims.nz)
+    cells = sc.dims.voxel_count()
+    b = 49 * cells
+    for ax in range(3):
+        t = sc.pml.thickness_voxels[ax] if sc.pml else 0
+        if t:
+            b += 32 * (cells // n[ax]) * min(2 * t, n[ax])
+    return b
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(", ") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(sc, seconds=15.0):
+    """The oracle (C restatement of the reference, AVX2 rows, one worker
+    thread per host core splitting each phase into contiguous block ranges
+    like the reference's rayon Z-slabs) on a bounded sample: as many full
+    512^3 steps as fit in about `seconds`."""
+    from oracle import oracle as O
+    nt = os.cpu_count() or 1
+    sim = O.sim_from_scenario(sc, steps=64)
+    sim.step(1, nt)  # warm-up (page-in)
+    t0 = time.perf_counter()
+    n = 0
+    while n < 64:
+        sim.step(1, nt)
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    el = time.perf_counter() - t0
+    sim.close()
+    return {"value": round(sc.dims.voxel_count() * n / el / 1e6, 2), "unit": METRIC, "cores": nt,
+            "kind": "port", "sample": f"{n} full 512^3 steps after 1 warm-up step, {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from wavefront_b200 import configs
+    sc = configs.two_spheres(n=512, steps=args.warmup + args.steps)
+    from oracle import oracle as O
+    nt = os.cpu_count() or 1
+    sim = O.sim_from_scenario(sc, steps=args.warmup + args.steps)
+    budget = float(os.environ.get("WF_REF_SECONDS", "120"))
+    for _ in range(min(args.warmup, 1)):
+        sim.step(1, nt)
+    t0 = time.perf_counter()
+    n = 0
+    while n < args.steps:
+        sim.step(1, nt)
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    sim.close()
+    v = N_CELLS * n / el / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": METRIC,
+        "n_gpus": world, "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": round(el / n * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "grid": [512, 512, 512],
+                                        "l2": "inputs larger than L2 (3.2 GB of fields)"},
+        "cpu_baseline": {"value": round(v, 2), "unit": METRIC, "cores": nt, "kind": "port",
+                         "sample": f"{n} of {args.steps} requested 512^3 steps in {el:.1f} s "
+                                   "(time-bounded); the Rust reference cannot be built here, so "
+                                   "this is the oracle's C restatement of its f32 AVX2 path"},
+        "e2e": {"value": round(v, 2), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from wavefront_b200 import configs
+    from wavefront_b200.engine import DeviceFieldGrid
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    total = args.warmup + args.steps
+    sc = configs.two_spheres(n=512, steps=total)
+
+    def build(kernel="fused"):
+        g = configs.device_grid(sc, kernel=kernel, device=local_rank)
+        if args.tiling:
+            g.set_tiling(*[int(v) for v in args.tiling.split(",")])
+        for s in sc.sources:
+            g.add_source_values(s.x, s.y, s.z, s.component, s.values(sc.dt, total))
+        for p in sc.probes:
+            c, si = p.tables(sc.dt, total)
+            g.add_probe_tables(p.x, p.y, p.z, p.component, c, si, p.first_step(sc.dt))
+        return g
+
+    # ---- device-resident throughput (value) + fused-kernel roofline -------
+    g = build()
+    g.step(args.warmup)
+    g.sync()
+    g.set_timing(True)
+    stream = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        g.step(args.steps)
+        e1.record(stream)
+        g.sync()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    kern_ms, launches = g.timing()
+    g.set_timing(False)
+    g.close()
+    clocks = clk.summary()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * N_CELLS * args.steps / (ms / 1e3) / 1e6
+
+    alg = algorithmic_bytes(sc)
+    per_launch_ms = kern_ms / max(launches, 1)
+    achieved = alg / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            traffic = json.load(f).get("fused_two_spheres_512_bytes_per_launch")
+
+    # ---- end to end through the C ABI from host buffers -----------------
+    pin_ids = torch.from_numpy(sc.grid.ids).pin_memory()
+    snap = torch.empty(N_CELLS * 6, dtype=torch.float32).pin_memory()
+    sc.grid.ids = pin_ids.numpy()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = build()
+    g.step(args.steps)
+    g.sync()
+    sums = [g.probe_sums(i, 1) for i in range(len(sc.probes))]
+    import ctypes as C
+    from wavefront_b200 import _lib as L
+    L.check(L.lib().wf_download_blocks(g._h, C.c_void_p(snap.data_ptr())), g._h)
+    e2e_s = time.perf_counter() - t0
+    g.close()
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        dist.barrier()
+    e2e = world * N_CELLS * args.steps / e2e_s / 1e6
+    h2d = N_CELLS + 256 * 16 + total * (4 + 8 * 16)
+    d2h = len(sums) * (8 * 2 + 8) + N_CELLS * 24
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [512, 512, 512], "cpml_cells": 16,
+                       "probes": 8, "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
+                       "tiling": list(build_tiling(args)),
+                       "l2": "inputs larger than L2 (3.2 GB of fields per state buffer)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "e2e": {"value": round(e2e, 1), "unit": METRIC,
+                    "h2d_bytes_per_step": int(h2d / args.steps),
+                    "d2h_bytes_per_step": int(d2h / args.steps),
+                    "includes": "handle creation, scene + table upload, K steps, probe sums, "
+                                "one FieldBlock snapshot download (pinned host buffers)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": alg,
+                         "kernel_ms_per_launch": round(per_launch_ms, 4)},
+            "gpu_launches": int(launches) + args.steps,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(sc)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def build_tiling(args):
+    if args.tiling:
+        return tuple(int(v) for v in args.tiling.split(","))
+    return (8, 64, 3)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--tiling", default="", help="tile_rows,z_chunk,stages")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

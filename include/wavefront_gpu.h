@@ -1,0 +1,236 @@
+/*
+ * wavefront_gpu.h -- C ABI of the B200 (sm_100a) FDTD timestep library.
+ *
+ * The library replaces the per-step hot path of the reference engine
+ * (AndrejRumenovski/wavefront):
+ *
+ *   src/engine.rs:291-422  step_all_slabs   (H phase, barrier, E phase over
+ *                                            rayon Z-slabs, calling the four
+ *                                            src/fdtd.rs kernels per block)
+ *   src/source.rs:79-95    Source::inject   (soft E source, after E)
+ *   src/probe.rs:126-138   Probe::accumulate (f64 running DFT, after inject)
+ *
+ * with device code, while the setup math (src/layout.rs material table, CPML
+ * profiles, src/scene.rs voxelizer, waveform evaluation) stays on the host.
+ * The host helpers at the end of this header restate that setup math in the
+ * library so a caller without the Rust crate gets identical tables.
+ *
+ * Conventions (no exceptions or aborts cross this ABI):
+ *   - every call returns wf_status; wf_last_error() gives a message;
+ *   - the handle owns all device memory; the caller owns host buffers, which
+ *     are copied during the call;
+ *   - a handle is not thread-safe; separate handles on separate streams are;
+ *   - device-side error flags (bounded-wait timeouts) are latched and
+ *     reported by the next wf_sync().
+ *
+ * Device layout (not visible through the ABI): six SoA field arrays, x
+ * fastest ((z*ny+y)*nx+x), double-buffered so one fused kernel can read a
+ * step's inputs and write its outputs with no cross-block hazard; a 1-byte
+ * material id per voxel plus a 256-entry coefficient table; CPML psi stored
+ * per axis only inside that axis's graded slab.
+ */
+#ifndef WAVEFRONT_GPU_H
+#define WAVEFRONT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  WF_OK = 0,
+  WF_ERR_ARG = 1,         /* bad argument (dims, index, table length)        */
+  WF_ERR_CUDA = 2,        /* a CUDA runtime/driver call failed               */
+  WF_ERR_OOM = 3,         /* device allocation failed                        */
+  WF_ERR_TIMEOUT = 4,     /* a bounded device wait gave up (flag latched)    */
+  WF_ERR_DEVICE_FLAG = 5, /* another device-side error flag was set          */
+  WF_ERR_STATE = 6,       /* call not valid in the handle's current state    */
+  WF_ERR_UNSUPPORTED = 7  /* option not supported on this device/build       */
+} wf_status;
+
+typedef enum { WF_BOUNDARY_ZERO = 0, WF_BOUNDARY_PERIODIC = 1 } wf_boundary;
+
+typedef enum {
+  WF_ARITH_EXACT = 0, /* separate IEEE mul/add: bit-exact with the reference */
+  WF_ARITH_FMA = 1    /* fused multiply-add (<= 1e-6 relative L2)           */
+} wf_arith;
+
+typedef enum {
+  WF_KERNEL_AUTO = 0,  /* fused when the grid allows it, else split          */
+  WF_KERNEL_FUSED = 1, /* one TMA z-march kernel per step (zero boundaries)  */
+  WF_KERNEL_SPLIT = 2  /* an H kernel then an E kernel (any boundaries)      */
+} wf_kernel;
+
+typedef enum {
+  WF_PREC_F32 = 0,  /* FP32 field storage (reference parity)               */
+  WF_PREC_BF16 = 1, /* BF16 storage, per-slab power-of-two scale, FP32 math */
+  WF_PREC_F16 = 2   /* FP16 storage, per-slab power-of-two scale, FP32 math */
+} wf_precision;
+
+/* Field component order of FieldBlock, src/layout.rs:699-706. */
+enum { WF_EX = 0, WF_EY = 1, WF_EZ = 2, WF_HX = 3, WF_HY = 4, WF_HZ = 5 };
+
+/* Source modes. */
+enum {
+  WF_SRC_SOFT = 0,        /* E_c[x,y,z] += v[step]; Source::inject          */
+  WF_SRC_HARD_SHEET_X = 1 /* E_c[x, every y, every z] = v[step]: the hard
+                             sheet source of examples/convergence_study.rs:
+                             165-173 and examples/pml_reflection_study.rs   */
+};
+
+typedef struct {
+  int32_t nx, ny, nz;  /* voxels; multiples of 8 (GridDims::new, src/layout.rs:60-67) */
+  int32_t boundary[3]; /* wf_boundary per axis x, y, z                       */
+  int32_t arith;       /* wf_arith                                           */
+  int32_t kernel;      /* wf_kernel                                          */
+  int32_t precision;   /* wf_precision                                       */
+  int32_t device;      /* CUDA device ordinal                                */
+  void *stream;        /* cudaStream_t to run on, or NULL for a private one  */
+} wf_grid_desc;
+
+typedef struct wf_handle wf_handle;
+
+/* ---- lifetime -------------------------------------------------------- */
+
+/* Allocates a zero-filled field grid (FieldGrid::zeroed, src/layout.rs:740)
+ * with every voxel vacuum-id 0 and no CPML. */
+wf_status wf_create(const wf_grid_desc *desc, wf_handle **out);
+wf_status wf_destroy(wf_handle *h);
+/* Message for the last failing call on h (or on this thread when h is NULL). */
+const char *wf_last_error(const wf_handle *h);
+const char *wf_status_string(wf_status s);
+
+/* ---- scene upload ------------------------------------------------------ */
+
+/* Material ids, nz*ny*nx bytes in MaterialGrid order (z,y,x; x fastest,
+ * src/layout.rs:327-329), and the 256-entry Q16.16 coefficient table
+ * {ca, cb, da, db} (MaterialTable, src/layout.rs:167-216).  Together they
+ * replace CoeffGrid::build (src/layout.rs:230-260): the kernels dequantize
+ * with FixedQ16_16::to_f32, so the FP32 multipliers are identical. */
+wf_status wf_set_materials(wf_handle *h, const uint8_t *ids,
+                           const int32_t (*table_q16)[4]);
+
+/* CPML on one axis (0=x, 1=y, 2=z): the graded profile of that axis (n
+ * entries each of b, a, 1/kappa: PmlProfile1D::build, src/layout.rs:471-513)
+ * and the graded thickness T in voxels.  psi memory is kept for the cells
+ * with that axis coordinate in [0,T) or [n-T,n).  Passing the same T on all
+ * three axes with T a multiple of 8 reproduces PmlContext::build and the
+ * PmlAuxGrid shell (src/layout.rs:594-656) bit for bit; other T values give
+ * the exact per-cell layer.  T=0 removes the axis's CPML. */
+wf_status wf_set_pml(wf_handle *h, int axis, int thickness_voxels,
+                     const float *b, const float *a, const float *inv_kappa);
+
+/* ---- sources and probes ------------------------------------------------ */
+
+/* Adds a source driving E component comp (0..2) with per-step values
+ * values[s] = amplitude * waveform(t_s), t_s = (s+1)*dt in f32, s counting
+ * from the handle's first step (src/engine.rs:769).  Sources apply in the
+ * order added, after the E update of each step. */
+wf_status wf_add_source(wf_handle *h, int x, int y, int z, int comp, int mode,
+                        const float *values, int nvalues, int *out_index);
+
+/* Adds a DFT probe on component comp (0..5).  cos_tab/sin_tab hold
+ * nsteps*nfreq doubles, [s*nfreq + f] = cos/sin(omega_f * (double)t_s), with
+ * omega_f = 2*pi*(double)freq_f (src/probe.rs:126-138).  Steps s >=
+ * first_step are accumulated (the t >= start_recording_at_s test of
+ * src/probe.rs:127).  record_trace keeps the raw f32 sample of every step. */
+wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
+                       const double *cos_tab, const double *sin_tab,
+                       int nsteps, int first_step, int record_trace,
+                       int *out_index);
+
+/* ---- stepping ------------------------------------------------------------ */
+
+/* Enqueues nsteps full timesteps: H everywhere, E everywhere, sources in
+ * order, probes (src/engine.rs:747-782).  Asynchronous on the handle's
+ * stream; long runs replay captured CUDA graphs. */
+wf_status wf_step(wf_handle *h, int nsteps);
+/* Waits for the stream and reports any latched device error. */
+wf_status wf_sync(wf_handle *h);
+int64_t wf_steps_done(const wf_handle *h);
+
+/* ---- read-back ----------------------------------------------------------- */
+
+wf_status wf_probe_sums(wf_handle *h, int probe, double *cos_out,
+                        double *sin_out, uint64_t *n_out);
+wf_status wf_probe_trace(wf_handle *h, int probe, float *out, int n);
+/* Six SoA host arrays (6*nz*ny*nx floats, component-major, x fastest). */
+wf_status wf_get_fields(wf_handle *h, float *out6);
+wf_status wf_set_fields(wf_handle *h, const float *in6);
+/* Snapshot bytes in the reference's FieldBlock order (serialize_snapshot,
+ * src/engine.rs:622-640): blocks (bz*nby+by)*nbx+bx, each ex..hz x 512. */
+wf_status wf_download_blocks(wf_handle *h, void *out);
+wf_status wf_upload_blocks(wf_handle *h, const void *in);
+/* psi of the reference PmlAux array `which` (0..11 in the declaration order
+ * of src/layout.rs:545-558), as an nz*ny*nx grid, zero where none is kept. */
+wf_status wf_get_psi(wf_handle *h, int which, float *out);
+/* Device pointers of the current six field arrays (FP32 precision only). */
+wf_status wf_device_fields(wf_handle *h, float **out6);
+
+/* The handle's CUDA stream (cudaStream_t) for event timing and interop. */
+wf_status wf_get_stream(wf_handle *h, void **out_stream);
+/* Kernel timing: while enabled, every step kernel launch (fused, or the
+ * split H+E pair) is bracketed by CUDA events on the handle's stream and
+ * steps are launched directly instead of through graphs.  wf_get_timing
+ * waits for the stream and returns the summed kernel time and launch count
+ * since timing was enabled. */
+wf_status wf_set_timing(wf_handle *h, int enable);
+wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches);
+
+/* ---- fused-kernel tiling (autotuner surface) --------------------------- */
+
+typedef struct {
+  int32_t tile_rows;  /* y rows per CTA tile (x width is fixed at 128)      */
+  int32_t z_chunk;    /* planes per CTA z-march                            */
+  int32_t stages;     /* TMA pipeline depth                                */
+} wf_tiling;
+
+wf_status wf_get_tiling(const wf_handle *h, wf_tiling *out);
+wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t);
+/* Times each candidate tiling for `steps` steps and keeps the fastest. */
+wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms);
+
+/* ---- host helpers: the reference's setup math ---------------------------- */
+
+int32_t wf_q16_from_f32(float v);   /* FixedQ16_16::from_f32, src/layout.rs:114-116 */
+float wf_q16_to_f32(int32_t q);     /* FixedQ16_16::to_f32,   src/layout.rs:123-125 */
+/* MaterialTable::coeffs_from_physical, src/layout.rs:194-208 */
+void wf_material_coeffs(float eps_r, float mu_r, float sigma, float dt, float d,
+                        int32_t out_q16[4]);
+/* effective_pml_thickness_blocks, src/layout.rs:525-533 */
+int wf_effective_pml_thickness_blocks(int nx, int ny, int nz, int requested_voxels);
+/* PmlProfile1D::build, src/layout.rs:471-513 (PmlConfig fields spelled out) */
+void wf_pml_profile(int n, float grading_order, float kappa_max,
+                    float alpha_max, float target_reflection, float dt,
+                    float dx, int thickness_voxels, float *b, float *a,
+                    float *inv_kappa);
+/* Waveform::evaluate, src/source.rs:46-59.  kind 0 GaussianPulse(p0=t0,
+ * p1=spread), 1 Sinusoid(p0=freq), 2 RickerWavelet(p0=peak_freq, p1=t0). */
+float wf_waveform_eval(int kind, float p0, float p1, float t);
+/* values[i] = amplitude * evaluate(((first_step+i) as f32 + 1) * dt). */
+void wf_source_values(int kind, float p0, float p1, float amplitude, float dt,
+                      int first_step, int nsteps, float *values);
+/* First step index whose t=(s+1)*dt is not below start (src/probe.rs:127). */
+int wf_probe_first_step(float start_recording_at_s, float dt);
+/* cos/sin tables for wf_add_probe, steps [first_step, first_step+nsteps). */
+void wf_probe_tables(const float *freqs, int nfreq, float dt, int first_step,
+                     int nsteps, double *cos_tab, double *sin_tab);
+/* Probe::spectrum, src/probe.rs:143-167. */
+void wf_spectrum(const double *sum_cos, const double *sum_sin, uint64_t n,
+                 int nfreq, double *amplitude, double *phase_rad);
+/* Scene::parse + Scene::voxelize, src/scene.rs:81-230.  grid must hold
+ * nx*ny*nz bytes (left as given outside primitives); table[id] receives the
+ * Q16.16 coefficients of each registered material.  Returns WF_ERR_ARG with
+ * the reference's message in err on a parse error. */
+wf_status wf_scene_voxelize(const char *text, int nx, int ny, int nz, float dt,
+                            float dx, uint8_t *grid, int32_t (*table)[4],
+                            int *n_materials, char *err, int errlen);
+/* voxelize_demo_sphere, src/main.rs:403-425 (material id 1). */
+void wf_demo_sphere(int nx, int ny, int nz, uint8_t *grid);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WAVEFRONT_GPU_H */

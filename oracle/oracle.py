@@ -59,6 +59,10 @@ def _declare(L: C.CDLL) -> None:
     L.or_pml_profile.argtypes = [C.c_int] + [C.c_float] * 6 + [C.c_int, _f32p, _f32p, _f32p]
     L.or_waveform_eval.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float]
     L.or_waveform_eval.restype = C.c_float
+    L.or_source_values.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, _f32p]
+    L.or_probe_tables.argtypes = [_f32p, C.c_int, C.c_float, C.c_int, _f64p, _f64p]
+    L.or_probe_first_step.argtypes = [C.c_float, C.c_float]
+    L.or_probe_first_step.restype = C.c_int
     L.or_scene_voxelize.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float,
                                     C.c_float, _u8p, _i32p, C.c_char_p, C.c_int]
     L.or_scene_voxelize.restype = C.c_int
@@ -129,6 +133,24 @@ def pml_profile(n, dt, dx, thickness_voxels, grading_order=3.0, kappa_max=7.0,
 
 def waveform_eval(kind: int, p0: float, p1: float, t: float) -> np.float32:
     return np.float32(lib().or_waveform_eval(kind, p0, p1, t))
+
+
+def source_values(kind, p0, p1, amplitude, dt, nsteps) -> np.ndarray:
+    out = np.zeros(nsteps, np.float32)
+    lib().or_source_values(kind, p0, p1, amplitude, dt, nsteps, _ptr(out, _f32p))
+    return out
+
+
+def probe_tables(freqs, dt, nsteps):
+    f = np.ascontiguousarray(freqs, np.float32)
+    c = np.zeros((nsteps, len(f)), np.float64)
+    s = np.zeros((nsteps, len(f)), np.float64)
+    lib().or_probe_tables(_ptr(f, _f32p), len(f), dt, nsteps, _ptr(c, _f64p), _ptr(s, _f64p))
+    return c, s
+
+
+def probe_first_step(start, dt) -> int:
+    return int(lib().or_probe_first_step(start, dt))
 
 
 def scene_voxelize(text: str, nx, ny, nz, dt, dx, table=None):
@@ -220,7 +242,7 @@ class Sim:
     def add_probe(self, x, y, z, comp, cos_tab, sin_tab, nsteps, first_step=0, record_trace=False):
         c = np.ascontiguousarray(cos_tab, np.float64).reshape(nsteps, -1)
         s = np.ascontiguousarray(sin_tab, np.float64).reshape(nsteps, -1)
-        nf = c.shape[1]
+        nf = c.shape[1] if nsteps else 0
         if self._f("add_probe")(self._h, x, y, z, comp, nf, _ptr(c, _f64p), _ptr(s, _f64p), nsteps,
                                 first_step, int(record_trace)) != 0:
             raise ValueError("bad probe")
@@ -262,3 +284,29 @@ class Sim:
         out = np.zeros(nsteps, np.float64)
         self._f("probe_trace")(self._h, p, _ptr(out, _f64p))
         return out
+
+
+def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None):
+    """Builds an oracle Sim for a wavefront_b200.configs.Scenario, computing every
+    table (CPML profiles, source values, probe twiddles) with the oracle's own
+    C code; only the scenario's description and its material ids are shared."""
+    steps = sc.steps if steps is None else steps
+    d = sc.dims
+    sim = Sim(d.nx, d.ny, d.nz, sc.grid.ids, sc.table.q16, periodic, dtype)
+    if sc.pml is not None:
+        n = (d.nx, d.ny, d.nz)
+        profs, shell = [], []
+        for ax in range(3):
+            t = sc.pml.thickness_voxels[ax]
+            profs.append(pml_profile(n[ax], sc.dt, sc.dx, t))
+            shell.append((t + 7) // 8)
+        sim.set_pml(profs, shell)
+    for s in sc.sources:
+        w = s.waveform
+        sim.add_source(s.x, s.y, s.z, int(s.component),
+                       source_values(w.kind, w.p0, w.p1, s.amplitude, sc.dt, steps), s.mode)
+    for p in sc.probes:
+        c, si = probe_tables(p.frequencies_hz, sc.dt, steps)
+        sim.add_probe(p.x, p.y, p.z, int(p.component), c, si, steps,
+                      probe_first_step(p.start_recording_at_s, sc.dt), p.record_trace)
+    return sim

@@ -105,6 +105,33 @@ float or_waveform_eval(int kind, float p0, float p1, float t) {
   return 0.0f;
 }
 
+void or_source_values(int kind, float p0, float p1, float amplitude, float dt,
+                      int nsteps, float *values) {
+  for (int s = 0; s < nsteps; s++) {
+    float t = ((float)s + 1.0f) * dt;
+    values[s] = amplitude * or_waveform_eval(kind, p0, p1, t);
+  }
+}
+
+void or_probe_tables(const float *freqs, int nfreq, float dt, int nsteps,
+                     double *cos_tab, double *sin_tab) {
+  for (int s = 0; s < nsteps; s++) {
+    float t = ((float)s + 1.0f) * dt;
+    for (int f = 0; f < nfreq; f++) {
+      double omega = 2.0 * PI_D * (double)freqs[f];
+      double ph = omega * (double)t;
+      cos_tab[(size_t)s * nfreq + f] = cos(ph);
+      sin_tab[(size_t)s * nfreq + f] = sin(ph);
+    }
+  }
+}
+
+int or_probe_first_step(float start, float dt) {
+  int s = 0;
+  while (((float)s + 1.0f) * dt < start) s++;
+  return s;
+}
+
 /* ------------------------------------------------------------------------ */
 /* scene format + voxelizer, src/scene.rs:81-230                             */
 /* ------------------------------------------------------------------------ */

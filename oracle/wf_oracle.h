@@ -40,6 +40,15 @@ void    or_pml_profile(int n, float grading_order, float kappa_max,
 /* kind: 0 Gaussian(p0=t0, p1=spread), 1 Sinusoid(p0=freq), 2 Ricker(p0=freq, p1=t0) */
 float   or_waveform_eval(int kind, float p0, float p1, float t); /* src/source.rs:46-59 */
 
+/* values[i] = amplitude * waveform(((i as f32) + 1) * dt), src/engine.rs:769 */
+void    or_source_values(int kind, float p0, float p1, float amplitude, float dt,
+                         int nsteps, float *values);
+/* [s*nfreq+f] = cos/sin(2*pi*(double)freq_f * (double)t_s), src/probe.rs:133-136 */
+void    or_probe_tables(const float *freqs, int nfreq, float dt, int nsteps,
+                        double *cos_tab, double *sin_tab);
+/* first step s with !(t_s < start), src/probe.rs:127 */
+int     or_probe_first_step(float start, float dt);
+
 /* ---- scene format + voxelizer (src/scene.rs:81-230) -------------------- */
 /* Voxelizes scene text into `grid` (nx*ny*nz bytes, pre-filled by caller) and
  * writes Q16.16 coefficients of every registered material into table[id].

@@ -4,7 +4,8 @@ The reference (AndrejRumenovski/wavefront) commits the outputs of its two
 validation studies as CSV files:
   validation/convergence_data.csv    <- examples/convergence_study.rs
   validation/pml_reflection_data.csv <- examples/pml_reflection_study.rs
-They are data, not code, and they pin the oracle (oracle/wf_oracle.c) to the
+The reference's example scene scenes/two_spheres.scene is copied too, as a
+scene-format fixture.  They are data, not code, and they pin the oracle (oracle/wf_oracle.c) to the
 reference's arithmetic: the oracle's restated studies must reproduce them.
 
 Run from the repository root with the reference checked out at REF_ROOT
@@ -17,8 +18,10 @@ import sys
 REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
-for name in ("convergence_data.csv", "pml_reflection_data.csv"):
-    src = os.path.join(REF_ROOT, "validation", name)
+for sub, name in (("validation", "convergence_data.csv"),
+                  ("validation", "pml_reflection_data.csv"),
+                  ("scenes", "two_spheres.scene")):
+    src = os.path.join(REF_ROOT, sub, name)
     if not os.path.exists(src):
         sys.exit(f"missing {src}")
     shutil.copyfile(src, os.path.join(HERE, name))

@@ -1,0 +1,68 @@
+"""The C-ABI library: it loads, exports every symbol include/wavefront_gpu.h
+declares, and reports argument and device errors as status codes (no aborts),
+which is checkable without a GPU."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from wavefront_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "wavefront_gpu.h")
+
+
+def _declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(wf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.lib()
+    declared = _declared()
+    assert len(declared) >= 30
+    out = subprocess.run(["nm", "-D", "--defined-only", L.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\sT\s(wf_[a-z0-9_]+)$", out, flags=re.M))
+    missing = [s for s in declared if s not in exported]
+    assert not missing, missing
+    for s in declared:
+        getattr(lib, s)
+    assert sorted(L.EXPORTS) == declared
+
+
+def test_library_is_built_for_sm100a_only():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", L.LIB_PATH],
+                         capture_output=True, text=True).stdout
+    archs = set(re.findall(r"sm_\d+a?", out))
+    assert archs == {"sm_100a"}, archs
+
+
+def test_bad_dims_are_an_argument_error_not_a_crash():
+    d = L.GridDesc()
+    d.nx, d.ny, d.nz = 12, 16, 16
+    h = C.c_void_p()
+    st = L.lib().wf_create(C.byref(d), C.byref(h))
+    assert st == L.WF_ERR_ARG
+    assert b"multiples of BLOCK_DIM" in L.lib().wf_last_error(None)
+
+
+def test_create_without_a_device_reports_status(monkeypatch):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    d = L.GridDesc()
+    d.nx = d.ny = d.nz = 16
+    h = C.c_void_p()
+    st = L.lib().wf_create(C.byref(d), C.byref(h))
+    assert st == L.WF_ERR_CUDA and not h.value
+
+
+def test_null_handle_calls_fail_cleanly():
+    lib = L.lib()
+    assert lib.wf_step(None, 1) == L.WF_ERR_ARG
+    assert lib.wf_sync(None) == L.WF_ERR_ARG
+    assert lib.wf_destroy(None) == L.WF_OK
+    assert lib.wf_status_string(L.WF_ERR_TIMEOUT) == b"device wait timed out"

@@ -1,0 +1,150 @@
+"""ctypes binding of libwavefront_gpu.so (include/wavefront_gpu.h).
+
+The library is built in-tree (wavefront_b200/lib/) by wavefront_b200/build.py.
+There is no fallback: if the library is missing, loading raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libwavefront_gpu.so")
+
+WF_OK, WF_ERR_ARG, WF_ERR_CUDA, WF_ERR_OOM, WF_ERR_TIMEOUT, WF_ERR_DEVICE_FLAG, \
+    WF_ERR_STATE, WF_ERR_UNSUPPORTED = range(8)
+
+# Every symbol include/wavefront_gpu.h declares (checked by tests).
+EXPORTS = [
+    "wf_create", "wf_destroy", "wf_last_error", "wf_status_string", "wf_set_materials",
+    "wf_set_pml", "wf_add_source", "wf_add_probe", "wf_step", "wf_sync", "wf_steps_done",
+    "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
+    "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
+    "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
+    "wf_material_coeffs", "wf_effective_pml_thickness_blocks", "wf_pml_profile",
+    "wf_waveform_eval", "wf_source_values", "wf_probe_first_step", "wf_probe_tables",
+    "wf_spectrum", "wf_scene_voxelize", "wf_demo_sphere",
+]
+
+
+class WfError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"wavefront_gpu error {status}: {msg}")
+        self.status = status
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("boundary", C.c_int32 * 3), ("arith", C.c_int32), ("kernel", C.c_int32),
+                ("precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p)]
+
+
+class Tiling(C.Structure):
+    _fields_ = [("tile_rows", C.c_int32), ("z_chunk", C.c_int32), ("stages", C.c_int32)]
+
+
+_f32p = C.POINTER(C.c_float)
+_f64p = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_u8p = C.POINTER(C.c_uint8)
+_h = C.c_void_p
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python wavefront_b200/build.py` "
+                "(nvcc, sm_100a). There is no CPU fallback.")
+        L = C.CDLL(LIB_PATH)
+        S = C.c_int
+        L.wf_create.argtypes = [C.POINTER(GridDesc), C.POINTER(_h)]
+        L.wf_create.restype = S
+        L.wf_destroy.argtypes = [_h]
+        L.wf_destroy.restype = S
+        L.wf_last_error.argtypes = [_h]
+        L.wf_last_error.restype = C.c_char_p
+        L.wf_status_string.argtypes = [S]
+        L.wf_status_string.restype = C.c_char_p
+        L.wf_set_materials.argtypes = [_h, _u8p, _i32p]
+        L.wf_set_materials.restype = S
+        L.wf_set_pml.argtypes = [_h, C.c_int, C.c_int, _f32p, _f32p, _f32p]
+        L.wf_set_pml.restype = S
+        L.wf_add_source.argtypes = [_h, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_int,
+                                    C.POINTER(C.c_int)]
+        L.wf_add_source.restype = S
+        L.wf_add_probe.argtypes = [_h, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
+                                   C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]
+        L.wf_add_probe.restype = S
+        L.wf_step.argtypes = [_h, C.c_int]
+        L.wf_step.restype = S
+        L.wf_sync.argtypes = [_h]
+        L.wf_sync.restype = S
+        L.wf_steps_done.argtypes = [_h]
+        L.wf_steps_done.restype = C.c_int64
+        L.wf_probe_sums.argtypes = [_h, C.c_int, _f64p, _f64p, C.POINTER(C.c_uint64)]
+        L.wf_probe_sums.restype = S
+        L.wf_probe_trace.argtypes = [_h, C.c_int, _f32p, C.c_int]
+        L.wf_probe_trace.restype = S
+        L.wf_get_fields.argtypes = [_h, _f32p]
+        L.wf_get_fields.restype = S
+        L.wf_set_fields.argtypes = [_h, _f32p]
+        L.wf_set_fields.restype = S
+        L.wf_download_blocks.argtypes = [_h, C.c_void_p]
+        L.wf_download_blocks.restype = S
+        L.wf_upload_blocks.argtypes = [_h, C.c_void_p]
+        L.wf_upload_blocks.restype = S
+        L.wf_get_psi.argtypes = [_h, C.c_int, _f32p]
+        L.wf_get_psi.restype = S
+        L.wf_device_fields.argtypes = [_h, C.POINTER(C.c_void_p)]
+        L.wf_device_fields.restype = S
+        L.wf_get_stream.argtypes = [_h, C.POINTER(C.c_void_p)]
+        L.wf_get_stream.restype = S
+        L.wf_set_timing.argtypes = [_h, C.c_int]
+        L.wf_set_timing.restype = S
+        L.wf_get_timing.argtypes = [_h, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.wf_get_timing.restype = S
+        L.wf_get_tiling.argtypes = [_h, C.POINTER(Tiling)]
+        L.wf_get_tiling.restype = S
+        L.wf_set_tiling.argtypes = [_h, C.POINTER(Tiling)]
+        L.wf_set_tiling.restype = S
+        L.wf_autotune.argtypes = [_h, C.c_int, C.POINTER(Tiling), _f32p]
+        L.wf_autotune.restype = S
+        L.wf_q16_from_f32.argtypes = [C.c_float]
+        L.wf_q16_from_f32.restype = C.c_int32
+        L.wf_q16_to_f32.argtypes = [C.c_int32]
+        L.wf_q16_to_f32.restype = C.c_float
+        L.wf_material_coeffs.argtypes = [C.c_float] * 5 + [_i32p]
+        L.wf_effective_pml_thickness_blocks.argtypes = [C.c_int] * 4
+        L.wf_effective_pml_thickness_blocks.restype = C.c_int
+        L.wf_pml_profile.argtypes = [C.c_int] + [C.c_float] * 6 + [C.c_int, _f32p, _f32p, _f32p]
+        L.wf_waveform_eval.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float]
+        L.wf_waveform_eval.restype = C.c_float
+        L.wf_source_values.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                       C.c_int, _f32p]
+        L.wf_probe_first_step.argtypes = [C.c_float, C.c_float]
+        L.wf_probe_first_step.restype = C.c_int
+        L.wf_probe_tables.argtypes = [_f32p, C.c_int, C.c_float, C.c_int, C.c_int, _f64p, _f64p]
+        L.wf_spectrum.argtypes = [_f64p, _f64p, C.c_uint64, C.c_int, _f64p, _f64p]
+        L.wf_scene_voxelize.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                        _u8p, _i32p, C.POINTER(C.c_int), C.c_char_p, C.c_int]
+        L.wf_scene_voxelize.restype = S
+        L.wf_demo_sphere.argtypes = [C.c_int, C.c_int, C.c_int, _u8p]
+        _lib = L
+    return _lib
+
+
+def check(status: int, handle=None) -> None:
+    if status != WF_OK:
+        msg = lib().wf_last_error(handle)
+        raise WfError(status, msg.decode() if msg else "")
+
+
+def ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+f32p, f64p, i32p, u8p = _f32p, _f64p, _i32p, _u8p

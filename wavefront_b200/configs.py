@@ -1,0 +1,112 @@
+"""Scenario builders for the workloads this project measures and tests.
+
+Each builder returns a `Scenario`: grid dims, dx/dt, material ids + Q16.16
+table (voxelized with the reference's scene rules), the CPML context,
+sources and probes, the way src/main.rs:508-600 wires a run.
+
+  plain_cube_64       64^3 vacuum, 10-cell CPML request (rounds to 16),
+                      Ricker Ez at the centre with 20 cells per wavelength,
+                      one Ez probe 16 cells from the source, 500 steps.
+  two_spheres(n=512)  two dielectric spheres, 16-cell CPML, Gaussian Ez at
+                      (n/2, n/2, n/8), 8 Ez probes on a line at z = 7n/8,
+                      1000 steps (the headline throughput workload).
+  demo_sphere_cube    the reference's benchmark shape: demo sphere (eps 4)
+                      at the centre, 8-cell CPML, dt 1.5 ps, Ricker.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from .layout import GridDims, MaterialGrid, MaterialTable, PmlConfig, PmlContext
+from .probe import FieldComponent as PC
+from .probe import Probe
+from .scene import Scene, demo_sphere
+from .source import FieldComponent, Source, Waveform, default_waveform
+
+C0 = 299792458.0
+
+
+def courant_dt(dx: float, factor: float = 0.99) -> float:
+    """dt = factor/sqrt(3) * dx / c, rounded to f32 (the engine's dt is f32)."""
+    return float(np.float32(factor / np.sqrt(3.0) * dx / C0))
+
+
+@dataclass
+class Scenario:
+    name: str
+    dims: GridDims
+    dx: float
+    dt: float
+    grid: MaterialGrid
+    table: MaterialTable
+    pml: Optional[PmlContext]
+    sources: List[Source]
+    probes: List[Probe]
+    steps: int
+    meta: dict = field(default_factory=dict)
+
+
+def plain_cube_64(steps: int = 500, pml_cells: int = 10, exact_pml: bool = False,
+                  n: int = 64) -> Scenario:
+    dims = GridDims(n, n, n)
+    dx = 1.0e-3
+    dt = courant_dt(dx)
+    f0 = float(np.float32(C0 / (20.0 * dx)))
+    grid = MaterialGrid(dims)
+    table = MaterialTable.vacuum_filled(dt, dx)
+    cfg = PmlConfig(thickness=pml_cells)
+    pml = (PmlContext.build_exact(dims, cfg, dt, dx) if exact_pml
+           else PmlContext.build(dims, cfg, dt, dx)) if pml_cells else None
+    c = n // 2
+    src = Source(c, c, c, FieldComponent.Ez, 1.0, default_waveform("ricker", f0))
+    prb = Probe(c + 16, c, c, PC.Ez, [f0], 0.0)
+    return Scenario("plain_cube_64", dims, dx, dt, grid, table, pml, [src], [prb], steps,
+                    {"f0": f0})
+
+
+def two_spheres_text(n: int) -> str:
+    s = n / 512.0
+    return (f"sphere 4.0 1.0 0.0 {160 * s:g} {256 * s:g} {256 * s:g} {80 * s:g}\n"
+            f"sphere 2.25 1.0 0.0 {352 * s:g} {256 * s:g} {256 * s:g} {60 * s:g}\n")
+
+
+def two_spheres(n: int = 512, steps: int = 1000, pml_cells: int = 16) -> Scenario:
+    dims = GridDims(n, n, n)
+    dx = 1.0e-3
+    dt = courant_dt(dx)
+    f = float(np.float32(C0 / (20.0 * dx)))
+    grid = MaterialGrid(dims)
+    table = MaterialTable.vacuum_filled(dt, dx)
+    Scene.parse(two_spheres_text(n)).voxelize(grid, table, dt, dx)
+    pml = PmlContext.build(dims, PmlConfig(thickness=pml_cells), dt, dx) if pml_cells else None
+    src = Source(n // 2, n // 2, n // 8, FieldComponent.Ez, 1.0, default_waveform("gaussian", f))
+    zp = (7 * n) // 8
+    probes = [Probe(n // 16 + (n // 8) * k, n // 2, zp, PC.Ez, [f], 0.0) for k in range(8)]
+    return Scenario(f"two_spheres_{n}", dims, dx, dt, grid, table, pml, [src], probes, steps,
+                    {"f": f})
+
+
+def demo_sphere_cube(n: int = 256, steps: int = 150, pml_cells: int = 8) -> Scenario:
+    dims = GridDims(n, n, n)
+    dx, dt = 1.0e-3, 1.5e-12
+    grid = MaterialGrid(dims)
+    demo_sphere(grid)
+    table = MaterialTable.vacuum_filled(dt, dx)
+    table.set_material(1, 4.0, 1.0, 0.0, dt, dx)
+    pml = PmlContext.build(dims, PmlConfig(thickness=pml_cells), dt, dx) if pml_cells else None
+    f = float(np.float32(1.0) / (np.float32(20.0) * np.float32(dt)))
+    src = Source(n // 2, n // 2, n // 2, FieldComponent.Ez, 1.0, default_waveform("ricker", f))
+    return Scenario(f"demo_sphere_{n}", dims, dx, dt, grid, table, pml, [src], [], steps, {"f": f})
+
+
+def device_grid(sc: Scenario, **kw):
+    """A DeviceFieldGrid loaded with the scenario's materials and CPML."""
+    from .engine import DeviceFieldGrid
+    g = DeviceFieldGrid(sc.dims, **kw)
+    g.set_materials(sc.grid, sc.table)
+    if sc.pml is not None:
+        g.set_pml(sc.pml)
+    return g

@@ -1,0 +1,833 @@
+// wf_engine.cu -- the C ABI of include/wavefront_gpu.h: device state, upload,
+// step orchestration (fused or split step + tail kernel, replayed through
+// captured CUDA graphs), and read-back in the reference's formats.
+//
+// Engine semantics follow src/engine.rs:747-782: each step is H everywhere,
+// E everywhere, then every source in order, then every probe.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/wavefront_gpu.h"
+#include "wf_launch.h"
+
+using wf::FusedArgs;
+using wf::FusedConfig;
+using wf::GridArgs;
+using wf::ProbeDev;
+using wf::SrcDev;
+using wf::TailArgs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct SrcRec {
+  SrcDev d;       // device view (vals points into device memory)
+  float *vals;    // device
+};
+
+struct ProbeRec {
+  ProbeDev d;
+  double *cos_tab, *sin_tab, *sc, *ss, *base;
+  unsigned long long *n;
+  float *trace;
+};
+
+struct AxisState {
+  int T = 0, W = 0;
+  float *prof = nullptr;       // [3][W]
+  float *psi[2] = {nullptr, nullptr};
+  long long cells = 0;
+};
+
+}  // namespace
+
+struct wf_handle {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int nx = 0, ny = 0, nz = 0;
+  long long N = 0;
+  int periodic[3] = {0, 0, 0};
+  int arith = WF_ARITH_EXACT;
+  int kernel_pref = WF_KERNEL_AUTO;
+  int precision = WF_PREC_F32;
+  float *fld[2] = {nullptr, nullptr};
+  int cur = 0;
+  uint8_t *mat = nullptr;
+  int mat_pitch = 0;
+  float4 *coef = nullptr;
+  AxisState ax[3];
+  std::vector<SrcRec> srcs;
+  std::vector<ProbeRec> probes;
+  SrcDev *d_src = nullptr;
+  ProbeDev *d_probe = nullptr;
+  long long *d_step = nullptr;
+  int *d_err = nullptr;
+  long long steps_done = 0;
+  FusedConfig cfg{8, 64, 3};
+  CUtensorMap tmE[2], tmH[2], tmM;
+  bool maps_ok = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_steps = 0;
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;   // pairs: start, end per timed launch
+  size_t ev_used = 0;
+  std::string err;
+};
+
+namespace {
+
+wf_status fail(wf_handle *h, wf_status s, const std::string &msg) {
+  if (h) h->err = msg;
+  g_last_error = msg;
+  return s;
+}
+
+wf_status cuda_fail(wf_handle *h, cudaError_t e, const char *what) {
+  const wf_status s = (e == cudaErrorMemoryAllocation) ? WF_ERR_OOM : WF_ERR_CUDA;
+  return fail(h, s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define WF_CUDA(h, call)                                \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+void drop_graphs(wf_handle *h) {
+  for (auto &g : h->graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+bool fused_allowed(const wf_handle *h) {
+  return h->precision == WF_PREC_F32 && !h->periodic[0] && !h->periodic[1] && !h->periodic[2];
+}
+
+bool use_fused(const wf_handle *h) {
+  if (h->kernel_pref == WF_KERNEL_SPLIT) return false;
+  return fused_allowed(h) && encode_fn() != nullptr;
+}
+
+// TMA descriptors: fields as a 4D tensor {nx, ny, nz, 6} per buffer, ids as
+// {nx, ny, nz} with a 16-byte-multiple row pitch.
+wf_status build_maps(wf_handle *h) {
+  h->maps_ok = false;
+  auto enc = encode_fn();
+  if (!enc) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  unsigned eb[4], hb[4], mb[3];
+  wf::fused_boxes(h->cfg.ty, eb, hb, mb);
+  const cuuint64_t fdim[4] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz, 6};
+  const cuuint64_t fstr[3] = {(cuuint64_t)h->nx * 4, (cuuint64_t)h->nx * h->ny * 4,
+                              (cuuint64_t)h->N * 4};
+  const cuuint32_t ones[4] = {1, 1, 1, 1};
+  for (int b = 0; b < 2; ++b) {
+    const cuuint32_t ebox[4] = {eb[0], eb[1], eb[2], eb[3]};
+    const cuuint32_t hbox[4] = {hb[0], hb[1], hb[2], hb[3]};
+    CUresult r1 = enc(&h->tmE[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, ebox,
+                      ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r2 = enc(&h->tmH[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, hbox,
+                      ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS)
+      return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(fields) failed");
+  }
+  const cuuint64_t mdim[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz};
+  const cuuint64_t mstr[2] = {(cuuint64_t)h->mat_pitch, (cuuint64_t)h->mat_pitch * h->ny};
+  const cuuint32_t mbox[3] = {mb[0], mb[1], mb[2]};
+  CUresult r3 = enc(&h->tmM, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->mat, mdim, mstr, mbox, ones,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r3 != CUDA_SUCCESS) return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(ids) failed");
+  WF_CUDA(h, wf::fused_prepare(h->cfg));
+  h->maps_ok = true;
+  return WF_OK;
+}
+
+GridArgs grid_args(const wf_handle *h) {
+  GridArgs g{};
+  g.nx = h->nx;
+  g.ny = h->ny;
+  g.nz = h->nz;
+  g.N = h->N;
+  for (int i = 0; i < 3; ++i) g.periodic[i] = h->periodic[i];
+  g.cur = h->fld[h->cur];
+  g.nxt = h->fld[h->cur ^ 1];
+  g.mat = h->mat;
+  g.mat_pitch = h->mat_pitch;
+  g.coef = h->coef;
+  for (int a = 0; a < 3; ++a) {
+    const AxisState &A = h->ax[a];
+    g.pml[a].T = A.T;
+    g.pml[a].W = A.W;
+    g.pml[a].prof = A.prof;
+    g.pml[a].psi_cur = A.psi[h->cur];
+    g.pml[a].psi_nxt = A.psi[h->cur ^ 1];
+    g.pml[a].cells = A.cells;
+  }
+  g.err = h->d_err;
+  return g;
+}
+
+bool has_pml(const wf_handle *h) { return h->ax[0].T > 0 || h->ax[1].T > 0 || h->ax[2].T > 0; }
+
+// One full step on h->stream: step kernel(s) cur -> nxt, then the tail.
+cudaEvent_t timing_event(wf_handle *h) {
+  if (h->ev_used == h->ev_pool.size()) {
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+    h->ev_pool.push_back(ev);
+  }
+  return h->ev_pool[h->ev_used++];
+}
+
+wf_status enqueue_one(wf_handle *h) {
+  GridArgs g = grid_args(h);
+  const bool fma = h->arith == WF_ARITH_FMA;
+  cudaError_t e;
+  if (h->timing) {
+    cudaEvent_t ev = timing_event(h);
+    if (!ev) return fail(h, WF_ERR_CUDA, "cudaEventCreate");
+    WF_CUDA(h, cudaEventRecord(ev, h->stream));
+  }
+  if (use_fused(h)) {
+    if (!h->maps_ok) {
+      wf_status s = build_maps(h);
+      if (s != WF_OK) return s;
+    }
+    FusedArgs a{};
+    a.g = g;
+    a.tiles_x = (h->nx + wf::kTileX - 1) / wf::kTileX;
+    a.tiles_y = (h->ny + h->cfg.ty - 1) / h->cfg.ty;
+    a.zchunk = h->cfg.zchunk;
+    a.has_pml = has_pml(h) ? 1 : 0;
+    e = wf::launch_fused(h->cfg, h->tmE[h->cur], h->tmH[h->cur], h->tmM, a, fma, h->stream);
+  } else {
+    e = wf::launch_split(g, fma, h->stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
+  if (h->timing) {
+    cudaEvent_t ev = timing_event(h);
+    if (!ev) return fail(h, WF_ERR_CUDA, "cudaEventCreate");
+    WF_CUDA(h, cudaEventRecord(ev, h->stream));
+  }
+  if (!h->srcs.empty() || !h->probes.empty()) {
+    TailArgs t{};
+    t.f = h->fld[h->cur ^ 1];
+    t.nx = h->nx;
+    t.ny = h->ny;
+    t.nz = h->nz;
+    t.src = h->d_src;
+    t.nsrc = static_cast<int>(h->srcs.size());
+    t.probe = h->d_probe;
+    t.nprobe = static_cast<int>(h->probes.size());
+    t.step = h->d_step;
+    e = wf::launch_tail(t, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "tail kernel launch");
+  }
+  h->cur ^= 1;
+  return WF_OK;
+}
+
+wf_status upload_src_probe_tables(wf_handle *h) {
+  drop_graphs(h);
+  if (h->d_src) cudaFree(h->d_src);
+  if (h->d_probe) cudaFree(h->d_probe);
+  h->d_src = nullptr;
+  h->d_probe = nullptr;
+  if (!h->srcs.empty()) {
+    std::vector<SrcDev> v;
+    for (auto &s : h->srcs) v.push_back(s.d);
+    WF_CUDA(h, cudaMalloc(&h->d_src, sizeof(SrcDev) * v.size()));
+    WF_CUDA(h, cudaMemcpy(h->d_src, v.data(), sizeof(SrcDev) * v.size(), cudaMemcpyHostToDevice));
+  }
+  if (!h->probes.empty()) {
+    std::vector<ProbeDev> v;
+    for (auto &p : h->probes) v.push_back(p.d);
+    WF_CUDA(h, cudaMalloc(&h->d_probe, sizeof(ProbeDev) * v.size()));
+    WF_CUDA(h, cudaMemcpy(h->d_probe, v.data(), sizeof(ProbeDev) * v.size(), cudaMemcpyHostToDevice));
+  }
+  return WF_OK;
+}
+
+bool tables_cover(const wf_handle *h, long long upto, std::string *why) {
+  for (size_t i = 0; i < h->srcs.size(); ++i)
+    if (h->srcs[i].d.nvals < upto) {
+      *why = "source " + std::to_string(i) + " has values for " + std::to_string(h->srcs[i].d.nvals) +
+             " steps, run needs " + std::to_string(upto);
+      return false;
+    }
+  for (size_t i = 0; i < h->probes.size(); ++i)
+    if (h->probes[i].d.nsteps < upto) {
+      *why = "probe " + std::to_string(i) + " has tables for " + std::to_string(h->probes[i].d.nsteps) +
+             " steps, run needs " + std::to_string(upto);
+      return false;
+    }
+  return true;
+}
+
+wf_status check_device_error(wf_handle *h) {
+  int flag = 0;
+  WF_CUDA(h, cudaMemcpy(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag & wf::kErrTimeout)
+    return fail(h, WF_ERR_TIMEOUT, "a device-side bounded wait timed out (TMA stage never arrived)");
+  if (flag) return fail(h, WF_ERR_DEVICE_FLAG, "device error flag set: " + std::to_string(flag));
+  return WF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *wf_status_string(wf_status s) {
+  switch (s) {
+    case WF_OK: return "ok";
+    case WF_ERR_ARG: return "invalid argument";
+    case WF_ERR_CUDA: return "CUDA error";
+    case WF_ERR_OOM: return "out of device memory";
+    case WF_ERR_TIMEOUT: return "device wait timed out";
+    case WF_ERR_DEVICE_FLAG: return "device error flag";
+    case WF_ERR_STATE: return "invalid state";
+    case WF_ERR_UNSUPPORTED: return "unsupported";
+  }
+  return "unknown";
+}
+
+const char *wf_last_error(const wf_handle *h) {
+  return h ? h->err.c_str() : g_last_error.c_str();
+}
+
+wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
+  if (!d || !out) return fail(nullptr, WF_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0 || d->nx % 8 || d->ny % 8 || d->nz % 8)
+    return fail(nullptr, WF_ERR_ARG,
+                "grid dimensions must be positive multiples of BLOCK_DIM (8)");
+  if (d->arith != WF_ARITH_EXACT && d->arith != WF_ARITH_FMA)
+    return fail(nullptr, WF_ERR_ARG, "unknown arith mode");
+  if (d->precision != WF_PREC_F32)
+    return fail(nullptr, WF_ERR_UNSUPPORTED, "only FP32 storage is available in this handle type");
+  for (int i = 0; i < 3; ++i)
+    if (d->boundary[i] != WF_BOUNDARY_ZERO && d->boundary[i] != WF_BOUNDARY_PERIODIC)
+      return fail(nullptr, WF_ERR_ARG, "unknown boundary kind");
+  if (d->kernel == WF_KERNEL_FUSED &&
+      (d->boundary[0] || d->boundary[1] || d->boundary[2]))
+    return fail(nullptr, WF_ERR_UNSUPPORTED, "the fused kernel supports zero-field boundaries only");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, WF_ERR_CUDA, "no CUDA device");
+  if (d->device < 0 || d->device >= ndev) return fail(nullptr, WF_ERR_ARG, "bad device ordinal");
+  DeviceGuard guard(d->device);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, d->device) != cudaSuccess || prop.major < 10)
+    return fail(nullptr, WF_ERR_UNSUPPORTED, "this library is built for sm_100a (B200)");
+
+  wf_handle *h = new wf_handle();
+  h->dev = d->device;
+  h->nx = d->nx;
+  h->ny = d->ny;
+  h->nz = d->nz;
+  h->N = static_cast<long long>(d->nx) * d->ny * d->nz;
+  for (int i = 0; i < 3; ++i) h->periodic[i] = d->boundary[i] == WF_BOUNDARY_PERIODIC;
+  h->arith = d->arith;
+  h->kernel_pref = d->kernel;
+  h->precision = d->precision;
+  h->mat_pitch = (d->nx + 15) / 16 * 16;
+  auto cleanup_fail = [&](wf_status s) {
+    wf_destroy(h);
+    return s;
+  };
+  cudaError_t e;
+  if (d->stream) {
+    h->stream = static_cast<cudaStream_t>(d->stream);
+  } else {
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaStreamCreate"));
+    h->own_stream = true;
+  }
+  for (int b = 0; b < 2; ++b) {
+    e = cudaMalloc(&h->fld[b], sizeof(float) * 6 * h->N);
+    if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(fields)"));
+    e = cudaMemsetAsync(h->fld[b], 0, sizeof(float) * 6 * h->N, h->stream);
+    if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMemset(fields)"));
+  }
+  const size_t mbytes = static_cast<size_t>(h->mat_pitch) * d->ny * d->nz;
+  if ((e = cudaMalloc(&h->mat, mbytes)) != cudaSuccess ||
+      (e = cudaMemsetAsync(h->mat, 0, mbytes, h->stream)) != cudaSuccess ||
+      (e = cudaMalloc(&h->coef, sizeof(float4) * 256)) != cudaSuccess ||
+      (e = cudaMemsetAsync(h->coef, 0, sizeof(float4) * 256, h->stream)) != cudaSuccess ||
+      (e = cudaMalloc(&h->d_step, sizeof(long long))) != cudaSuccess ||
+      (e = cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream)) != cudaSuccess ||
+      (e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess ||
+      (e = cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream)) != cudaSuccess)
+    return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(state)"));
+  if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
+    return cleanup_fail(cuda_fail(nullptr, e, "cudaStreamSynchronize"));
+  *out = h;
+  return WF_OK;
+}
+
+wf_status wf_destroy(wf_handle *h) {
+  if (!h) return WF_OK;
+  DeviceGuard guard(h->dev);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graphs(h);
+  for (auto ev : h->ev_pool) cudaEventDestroy(ev);
+  for (auto &f : h->fld) cudaFree(f);
+  cudaFree(h->mat);
+  cudaFree(h->coef);
+  cudaFree(h->d_step);
+  cudaFree(h->d_err);
+  cudaFree(h->d_src);
+  cudaFree(h->d_probe);
+  for (auto &a : h->ax) {
+    cudaFree(a.prof);
+    cudaFree(a.psi[0]);
+    cudaFree(a.psi[1]);
+  }
+  for (auto &s : h->srcs) cudaFree(s.vals);
+  for (auto &p : h->probes) {
+    cudaFree(p.base);
+    cudaFree(p.n);
+    cudaFree(p.trace);
+  }
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return WF_OK;
+}
+
+wf_status wf_set_materials(wf_handle *h, const uint8_t *ids, const int32_t (*table)[4]) {
+  if (!h || !ids || !table) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  // FixedQ16_16::to_f32 (src/layout.rs:123-125): q as f32 * (1/65536)
+  float4 coef[256];
+  for (int m = 0; m < 256; ++m)
+    coef[m] = make_float4(wf_q16_to_f32(table[m][0]), wf_q16_to_f32(table[m][1]),
+                          wf_q16_to_f32(table[m][2]), wf_q16_to_f32(table[m][3]));
+  WF_CUDA(h, cudaMemcpyAsync(h->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, h->stream));
+  WF_CUDA(h, cudaMemcpy2DAsync(h->mat, h->mat_pitch, ids, h->nx, h->nx,
+                               static_cast<size_t>(h->ny) * h->nz, cudaMemcpyHostToDevice,
+                               h->stream));
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WF_OK;
+}
+
+wf_status wf_set_pml(wf_handle *h, int axis, int T, const float *b, const float *a,
+                     const float *ik) {
+  if (!h || axis < 0 || axis > 2) return fail(h, WF_ERR_ARG, "bad axis");
+  const int n = axis == 0 ? h->nx : (axis == 1 ? h->ny : h->nz);
+  if (T < 0 || T > n) return fail(h, WF_ERR_ARG, "CPML thickness out of range");
+  if (T > 0 && (!b || !a || !ik)) return fail(h, WF_ERR_ARG, "null profile");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  drop_graphs(h);
+  AxisState &A = h->ax[axis];
+  cudaFree(A.prof);
+  cudaFree(A.psi[0]);
+  cudaFree(A.psi[1]);
+  A = AxisState();
+  if (T == 0) return WF_OK;
+  A.T = T;
+  A.W = std::min(2 * T, n);
+  const long long cross = axis == 0 ? static_cast<long long>(h->ny) * h->nz
+                        : axis == 1 ? static_cast<long long>(h->nx) * h->nz
+                                    : static_cast<long long>(h->nx) * h->ny;
+  A.cells = cross * A.W;
+  std::vector<float> prof(3 * A.W);
+  for (int s = 0; s < A.W; ++s) {
+    const int c = s < T ? s : s + (n - A.W);  // slab position -> axis coordinate
+    prof[s] = b[c];
+    prof[A.W + s] = a[c];
+    prof[2 * A.W + s] = ik[c];
+  }
+  WF_CUDA(h, cudaMalloc(&A.prof, sizeof(float) * prof.size()));
+  WF_CUDA(h, cudaMemcpy(A.prof, prof.data(), sizeof(float) * prof.size(), cudaMemcpyHostToDevice));
+  for (int k = 0; k < 2; ++k) {
+    WF_CUDA(h, cudaMalloc(&A.psi[k], sizeof(float) * 4 * A.cells));
+    WF_CUDA(h, cudaMemset(A.psi[k], 0, sizeof(float) * 4 * A.cells));  // PmlAux::ZERO
+  }
+  return WF_OK;
+}
+
+wf_status wf_add_source(wf_handle *h, int x, int y, int z, int comp, int mode,
+                        const float *values, int nvalues, int *out_index) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  if (x < 0 || x >= h->nx || y < 0 || y >= h->ny || z < 0 || z >= h->nz)
+    return fail(h, WF_ERR_ARG, "source position outside the domain");
+  if (comp < 0 || comp > 2) return fail(h, WF_ERR_ARG, "source component must be Ex, Ey or Ez");
+  if (mode != WF_SRC_SOFT && mode != WF_SRC_HARD_SHEET_X) return fail(h, WF_ERR_ARG, "bad source mode");
+  if (nvalues < 0 || (nvalues > 0 && !values)) return fail(h, WF_ERR_ARG, "bad source values");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  SrcRec r{};
+  WF_CUDA(h, cudaMalloc(&r.vals, sizeof(float) * std::max(nvalues, 1)));
+  if (nvalues > 0)
+    WF_CUDA(h, cudaMemcpy(r.vals, values, sizeof(float) * nvalues, cudaMemcpyHostToDevice));
+  r.d.comp = comp;
+  r.d.mode = mode;
+  r.d.x = x;
+  r.d.y = y;
+  r.d.z = z;
+  r.d.nvals = nvalues;
+  r.d.vals = r.vals;
+  h->srcs.push_back(r);
+  if (out_index) *out_index = static_cast<int>(h->srcs.size()) - 1;
+  return upload_src_probe_tables(h);
+}
+
+wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
+                       const double *cos_tab, const double *sin_tab, int nsteps, int first_step,
+                       int record_trace, int *out_index) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  if (x < 0 || x >= h->nx || y < 0 || y >= h->ny || z < 0 || z >= h->nz)
+    return fail(h, WF_ERR_ARG, "probe position outside the domain");
+  if (comp < 0 || comp > 5) return fail(h, WF_ERR_ARG, "probe component must be 0..5");
+  if (nfreq < 0 || nsteps < 0 || first_step < 0) return fail(h, WF_ERR_ARG, "bad probe sizes");
+  if (nfreq > 0 && nsteps > 0 && (!cos_tab || !sin_tab)) return fail(h, WF_ERR_ARG, "null probe tables");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  ProbeRec r{};
+  const size_t tab = static_cast<size_t>(nsteps) * nfreq;
+  const size_t total = 2 * tab + 2 * static_cast<size_t>(nfreq) + 1;
+  WF_CUDA(h, cudaMalloc(&r.base, sizeof(double) * total));
+  WF_CUDA(h, cudaMemset(r.base, 0, sizeof(double) * total));
+  r.cos_tab = r.base;
+  r.sin_tab = r.base + tab;
+  r.sc = r.base + 2 * tab;
+  r.ss = r.sc + nfreq;
+  if (tab) {
+    WF_CUDA(h, cudaMemcpy(r.cos_tab, cos_tab, sizeof(double) * tab, cudaMemcpyHostToDevice));
+    WF_CUDA(h, cudaMemcpy(r.sin_tab, sin_tab, sizeof(double) * tab, cudaMemcpyHostToDevice));
+  }
+  WF_CUDA(h, cudaMalloc(&r.n, sizeof(unsigned long long)));
+  WF_CUDA(h, cudaMemset(r.n, 0, sizeof(unsigned long long)));
+  WF_CUDA(h, cudaMalloc(&r.trace, sizeof(float) * std::max(nsteps, 1)));
+  WF_CUDA(h, cudaMemset(r.trace, 0, sizeof(float) * std::max(nsteps, 1)));
+  r.d.comp = comp;
+  r.d.x = x;
+  r.d.y = y;
+  r.d.z = z;
+  r.d.nfreq = nfreq;
+  r.d.nsteps = nsteps;
+  r.d.first_step = first_step;
+  r.d.record = record_trace ? 1 : 0;
+  r.d.cos_tab = r.cos_tab;
+  r.d.sin_tab = r.sin_tab;
+  r.d.sc = r.sc;
+  r.d.ss = r.ss;
+  r.d.n = r.n;
+  r.d.trace = r.trace;
+  h->probes.push_back(r);
+  if (out_index) *out_index = static_cast<int>(h->probes.size()) - 1;
+  return upload_src_probe_tables(h);
+}
+
+wf_status wf_step(wf_handle *h, int nsteps) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  if (nsteps < 0) return fail(h, WF_ERR_ARG, "negative step count");
+  if (nsteps == 0) return WF_OK;
+  std::string why;
+  if (!tables_cover(h, h->steps_done + nsteps, &why)) return fail(h, WF_ERR_ARG, why);
+  DeviceGuard guard(h->dev);
+  if (use_fused(h) && !h->maps_ok) {  // descriptors + smem limit, outside any capture
+    wf_status s = build_maps(h);
+    if (s != WF_OK) return s;
+  }
+  // Long runs replay a captured graph of an even number of steps (the
+  // state buffers ping-pong, so an even count returns to the same parity).
+  const int G = h->graph_steps > 0 ? h->graph_steps : 32;
+  int left = nsteps;
+  while (left >= G && !h->timing) {
+    cudaGraphExec_t &ge = h->graph[h->cur];
+    if (!ge) {
+      const int cur0 = h->cur;
+      cudaGraph_t graph;
+      WF_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      wf_status st = WF_OK;
+      for (int i = 0; i < G && st == WF_OK; ++i) st = enqueue_one(h);
+      cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
+      h->cur = cur0;
+      if (st != WF_OK) return st;
+      if (ec != cudaSuccess) return cuda_fail(h, ec, "cudaStreamEndCapture");
+      ec = cudaGraphInstantiate(&ge, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ec != cudaSuccess) return cuda_fail(h, ec, "cudaGraphInstantiate");
+    }
+    WF_CUDA(h, cudaGraphLaunch(ge, h->stream));
+    left -= G;
+    h->steps_done += G;
+    if (G % 2) h->cur ^= 1;
+  }
+  for (; left > 0; --left) {
+    wf_status st = enqueue_one(h);
+    if (st != WF_OK) return st;
+    h->steps_done += 1;
+  }
+  return WF_OK;
+}
+
+wf_status wf_sync(wf_handle *h) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return check_device_error(h);
+}
+
+int64_t wf_steps_done(const wf_handle *h) { return h ? h->steps_done : -1; }
+
+wf_status wf_probe_sums(wf_handle *h, int p, double *c, double *s, uint64_t *n) {
+  if (!h || p < 0 || p >= static_cast<int>(h->probes.size())) return fail(h, WF_ERR_ARG, "bad probe index");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  const ProbeRec &r = h->probes[p];
+  if (c && r.d.nfreq) WF_CUDA(h, cudaMemcpy(c, r.sc, sizeof(double) * r.d.nfreq, cudaMemcpyDeviceToHost));
+  if (s && r.d.nfreq) WF_CUDA(h, cudaMemcpy(s, r.ss, sizeof(double) * r.d.nfreq, cudaMemcpyDeviceToHost));
+  if (n) {
+    unsigned long long v = 0;
+    WF_CUDA(h, cudaMemcpy(&v, r.n, sizeof(v), cudaMemcpyDeviceToHost));
+    *n = v;
+  }
+  return check_device_error(h);
+}
+
+wf_status wf_probe_trace(wf_handle *h, int p, float *out, int n) {
+  if (!h || p < 0 || p >= static_cast<int>(h->probes.size()) || !out) return fail(h, WF_ERR_ARG, "bad probe index");
+  const ProbeRec &r = h->probes[p];
+  if (n < 0 || n > r.d.nsteps) return fail(h, WF_ERR_ARG, "trace length exceeds the probe's steps");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (n) WF_CUDA(h, cudaMemcpy(out, r.trace, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return WF_OK;
+}
+
+wf_status wf_get_fields(wf_handle *h, float *out6) {
+  if (!h || !out6) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  WF_CUDA(h, cudaMemcpy(out6, h->fld[h->cur], sizeof(float) * 6 * h->N, cudaMemcpyDeviceToHost));
+  return WF_OK;
+}
+
+wf_status wf_set_fields(wf_handle *h, const float *in6) {
+  if (!h || !in6) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  WF_CUDA(h, cudaMemcpy(h->fld[h->cur], in6, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice));
+  return WF_OK;
+}
+
+wf_status wf_download_blocks(wf_handle *h, void *out) {
+  if (!h || !out) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  // the next-state buffer is dead between steps: use it to reorder
+  float *tmp = h->fld[h->cur ^ 1];
+  WF_CUDA(h, wf::launch_soa_to_blocks(h->fld[h->cur], tmp, h->nx, h->ny, h->nz, h->stream));
+  WF_CUDA(h, cudaMemcpyAsync(out, tmp, sizeof(float) * 6 * h->N, cudaMemcpyDeviceToHost, h->stream));
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WF_OK;
+}
+
+wf_status wf_upload_blocks(wf_handle *h, const void *in) {
+  if (!h || !in) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  float *tmp = h->fld[h->cur ^ 1];
+  WF_CUDA(h, cudaMemcpyAsync(tmp, in, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice, h->stream));
+  WF_CUDA(h, wf::launch_blocks_to_soa(tmp, h->fld[h->cur], h->nx, h->ny, h->nz, h->stream));
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WF_OK;
+}
+
+wf_status wf_get_psi(wf_handle *h, int which, float *out) {
+  if (!h || !out || which < 0 || which > 11) return fail(h, WF_ERR_ARG, "bad psi index");
+  // PmlAux order (src/layout.rs:545-558) -> (axis, slot)
+  static const int kAxis[12] = {0, 0, 1, 1, 2, 2, 0, 0, 1, 1, 2, 2};
+  static const int kSlot[12] = {0, 1, 0, 1, 0, 1, 2, 3, 3, 2, 2, 3};
+  const int axis = kAxis[which], slot = kSlot[which];
+  std::fill(out, out + h->N, 0.0f);
+  const AxisState &A = h->ax[axis];
+  if (A.T == 0) return WF_OK;
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::vector<float> buf(A.cells);
+  WF_CUDA(h, cudaMemcpy(buf.data(), A.psi[h->cur] + slot * A.cells, sizeof(float) * A.cells,
+                        cudaMemcpyDeviceToHost));
+  const int n = axis == 0 ? h->nx : (axis == 1 ? h->ny : h->nz);
+  for (int z = 0; z < h->nz; ++z)
+    for (int y = 0; y < h->ny; ++y)
+      for (int x = 0; x < h->nx; ++x) {
+        const int c = axis == 0 ? x : (axis == 1 ? y : z);
+        int s = -1;
+        if (c < A.T) s = c;
+        else if (c >= n - A.T) s = c - (n - A.W);
+        if (s < 0) continue;
+        long long idx;
+        if (axis == 0) idx = (static_cast<long long>(z) * h->ny + y) * A.W + s;
+        else if (axis == 1) idx = (static_cast<long long>(z) * A.W + s) * h->nx + x;
+        else idx = (static_cast<long long>(s) * h->ny + y) * h->nx + x;
+        out[(static_cast<long long>(z) * h->ny + y) * h->nx + x] = buf[idx];
+      }
+  return WF_OK;
+}
+
+wf_status wf_device_fields(wf_handle *h, float **out6) {
+  if (!h || !out6) return fail(h, WF_ERR_ARG, "null argument");
+  for (int c = 0; c < 6; ++c) out6[c] = h->fld[h->cur] + c * h->N;
+  return WF_OK;
+}
+
+wf_status wf_get_stream(wf_handle *h, void **out) {
+  if (!h || !out) return fail(h, WF_ERR_ARG, "null argument");
+  *out = h->stream;
+  return WF_OK;
+}
+
+wf_status wf_set_timing(wf_handle *h, int enable) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->timing = enable != 0;
+  h->ev_used = 0;
+  return WF_OK;
+}
+
+wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches) {
+  if (!h || !total_ms || !launches) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  double tot = 0.0;
+  for (size_t i = 0; i + 1 < h->ev_used; i += 2) {
+    float ms = 0.0f;
+    WF_CUDA(h, cudaEventElapsedTime(&ms, h->ev_pool[i], h->ev_pool[i + 1]));
+    tot += ms;
+  }
+  *total_ms = tot;
+  *launches = static_cast<int64_t>(h->ev_used / 2);
+  return WF_OK;
+}
+
+wf_status wf_get_tiling(const wf_handle *h, wf_tiling *out) {
+  if (!h || !out) return WF_ERR_ARG;
+  out->tile_rows = h->cfg.ty;
+  out->z_chunk = h->cfg.zchunk;
+  out->stages = h->cfg.stages;
+  return WF_OK;
+}
+
+wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t) {
+  if (!h || !t) return fail(h, WF_ERR_ARG, "null argument");
+  FusedConfig c{t->tile_rows, t->z_chunk, t->stages};
+  if (!wf::fused_supported(c)) return fail(h, WF_ERR_ARG, "tiling not instantiated");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  drop_graphs(h);
+  h->cfg = c;
+  h->maps_ok = false;
+  return WF_OK;
+}
+
+wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) {
+  if (!h || steps <= 0) return fail(h, WF_ERR_ARG, "bad autotune arguments");
+  if (!use_fused(h)) return fail(h, WF_ERR_UNSUPPORTED, "autotuning applies to the fused kernel");
+  if (h->steps_done != 0)
+    return fail(h, WF_ERR_STATE, "autotune before the first step (it runs trial steps)");
+  DeviceGuard guard(h->dev);
+  // Tuning must not disturb the run: snapshot the state and restore it.
+  std::vector<float> saved(6 * h->N);
+  wf_status st = wf_get_fields(h, saved.data());
+  if (st != WF_OK) return st;
+  const FusedConfig orig = h->cfg;
+  const int orig_cur = h->cur;
+  std::vector<FusedConfig> cands;
+  const int tys[] = {4, 8, 12, 16};
+  const int stg[] = {2, 3, 4};
+  const int zcs[] = {16, 32, 64, 128, 1 << 20};
+  for (int ty : tys)
+    for (int s : stg)
+      for (int zc : zcs) {
+        FusedConfig c{ty, std::min(zc, h->nz), s};
+        if (wf::fused_supported(c)) cands.push_back(c);
+      }
+  cudaEvent_t e0, e1;
+  WF_CUDA(h, cudaEventCreate(&e0));
+  WF_CUDA(h, cudaEventCreate(&e1));
+  float bms = 1e30f;
+  FusedConfig bc = orig;
+  // Source/probe tails are excluded: tuning times the stencil alone.
+  std::vector<SrcRec> srcs;
+  std::vector<ProbeRec> probes;
+  srcs.swap(h->srcs);
+  probes.swap(h->probes);
+  for (const FusedConfig &c : cands) {
+    h->cfg = c;
+    h->maps_ok = false;
+    if (enqueue_one(h) != WF_OK) continue;  // warm-up and attribute set
+    cudaEventRecord(e0, h->stream);
+    bool okc = true;
+    for (int i = 0; i < steps && okc; ++i) okc = enqueue_one(h) == WF_OK;
+    cudaEventRecord(e1, h->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess || !okc) continue;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= steps;
+    if (ms < bms) {
+      bms = ms;
+      bc = c;
+    }
+  }
+  srcs.swap(h->srcs);
+  probes.swap(h->probes);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->cfg = bc;
+  h->maps_ok = false;
+  drop_graphs(h);
+  h->cur = orig_cur;
+  // the trial steps advanced fields and psi: put the initial state back
+  st = wf_set_fields(h, saved.data());
+  if (st != WF_OK) return st;
+  for (auto &A : h->ax)
+    for (int k = 0; k < 2; ++k)
+      if (A.psi[k]) WF_CUDA(h, cudaMemset(A.psi[k], 0, sizeof(float) * 4 * A.cells));
+  WF_CUDA(h, cudaMemset(h->d_err, 0, sizeof(int)));
+  if (best) {
+    best->tile_rows = bc.ty;
+    best->z_chunk = bc.zchunk;
+    best->stages = bc.stages;
+  }
+  if (best_ms) *best_ms = bms;
+  return WF_OK;
+}
+
+}  // extern "C"

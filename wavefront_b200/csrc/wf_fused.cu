@@ -1,0 +1,484 @@
+// wf_fused.cu -- one-pass fused H->E Yee step for sm_100a.
+//
+// Replaces, for zero-field boundaries, one whole step_all_slabs call of the
+// reference (src/engine.rs:291-422: an H phase over every 8^3 block with
+// update_h_field[_pml], a barrier, then an E phase with update_e_field[_pml])
+// with a single kernel in which every field value crosses HBM once:
+//
+//  * a CTA owns a 128 x TY column of cells and marches it through a chunk of
+//    z planes;
+//  * plane p's E box (tile + 1-cell halo), H box (tile + -x/-y halo) and the
+//    material-id box are staged into shared memory by TMA
+//    (cp.async.bulk.tensor, no multicast) through an S-deep mbarrier ring;
+//    out-of-domain box cells arrive as zeros, which is exactly the
+//    reference's OUTER_ZERO_BLOCK (src/engine.rs:83);
+//  * H of plane p is computed for the tile plus the -x column and -y row
+//    the E update needs (recomputed, never exchanged between CTAs), E of
+//    plane p follows at once from registers and a shared-memory H plane;
+//    the -z neighbour H(p-1) rides along in registers (register-rotated z);
+//  * the state is double-buffered: the kernel reads buffer `cur` and writes
+//    buffer `nxt`, so halo recomputation never races a neighbour's writes;
+//  * CPML psi is read/written only by CTAs whose tile or z chunk meets a
+//    graded slab; interior CTAs run a body with no CPML code at all.
+//
+// All per-cell arithmetic goes through wf_internal.cuh, so results are
+// bit-identical to the split kernels and to the reference.
+#include "wf_internal.cuh"
+#include "wf_launch.h"
+
+namespace wf {
+
+namespace {
+
+template <int TY, int S>
+struct Layout {
+  static constexpr int EW = kTileX + 8, EH = TY + 2;   // E box: x0-4..x0+131, y0-1..y0+TY
+  static constexpr int HW = kTileX + 4, HH = TY + 1;   // H box: x0-4..x0+127, y0-1..y0+TY-1
+  static constexpr int MW = kTileX + 16, MH = TY + 1;  // ids:   x0-16..x0+127
+  static constexpr int E_BYTES = 3 * EH * EW * 4;
+  static constexpr int H_BYTES = 3 * HH * HW * 4;
+  static constexpr int M_BYTES = MH * MW;
+  static constexpr int al(int v) { return (v + 127) / 128 * 128; }
+  static constexpr int H_OFF = al(E_BYTES);
+  static constexpr int M_OFF = H_OFF + al(H_BYTES);
+  static constexpr int STAGE = M_OFF + al(M_BYTES);
+  static constexpr int STAGE_OFF = 4096;  // after the 256-entry float4 coefficient table
+  static constexpr int PROWS = TY + 1;    // plane rows: 0 = y0-1, 1..TY = tile rows
+  static constexpr int PLANE_FLOATS = 2 * PROWS * kTileX + 64;  // hz, hx rows; x-halo hz, hy
+  static constexpr int PLANE_OFF = STAGE_OFF + S * STAGE;
+  static constexpr int BAR_OFF = PLANE_OFF + 2 * PLANE_FLOATS * 4;
+  static constexpr int BYTES = BAR_OFF + S * 8 + 128;  // +128: base alignment slack
+  static constexpr int THREADS = 32 * (TY + 1);
+  static_assert(TY + 1 <= 32, "x-halo column is handled by one warp");
+};
+
+struct HIn {
+  float ex, ey, ez, ex_py, ez_py, ex_pz, ey_pz, ez_px, ey_px, hx, hy, hz;
+};
+
+// update_h_field[_pml] for one cell (src/fdtd.rs:194-345)
+template <bool FMA, bool PML>
+__device__ __forceinline__ void h_cell(const HIn &c, float da, float db, const GridArgs &g, int x,
+                                       int y, int p, bool pml_ok, bool write_psi, float &hxo,
+                                       float &hyo, float &hzo) {
+  float d_ez_dy = sub(c.ez_py, c.ez), d_ex_dy = sub(c.ex_py, c.ex);
+  float d_ey_dz = sub(c.ey_pz, c.ey), d_ex_dz = sub(c.ex_pz, c.ex);
+  float d_ez_dx = sub(c.ez_px, c.ez), d_ey_dx = sub(c.ey_px, c.ey);
+  if (PML && pml_ok) {
+    {
+      const PmlAxis &P = g.pml[0];
+      const int s = slab_pos(x, g.nx, P.T, P.W);
+      if (s >= 0) {
+        const long long idx = (static_cast<long long>(p) * g.ny + y) * P.W + s;
+        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+        float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
+        d_ez_dx = pml_corr<FMA>(d_ez_dx, b, a, ik, p0);
+        d_ey_dx = pml_corr<FMA>(d_ey_dx, b, a, ik, p1);
+        if (write_psi) {
+          P.psi_nxt[idx] = p0;
+          P.psi_nxt[P.cells + idx] = p1;
+        }
+      }
+    }
+    {
+      const PmlAxis &P = g.pml[1];
+      const int s = slab_pos(y, g.ny, P.T, P.W);
+      if (s >= 0) {
+        const long long idx = (static_cast<long long>(p) * P.W + s) * g.nx + x;
+        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+        float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
+        d_ez_dy = pml_corr<FMA>(d_ez_dy, b, a, ik, p0);
+        d_ex_dy = pml_corr<FMA>(d_ex_dy, b, a, ik, p1);
+        if (write_psi) {
+          P.psi_nxt[idx] = p0;
+          P.psi_nxt[P.cells + idx] = p1;
+        }
+      }
+    }
+    {
+      const PmlAxis &P = g.pml[2];
+      const int s = slab_pos(p, g.nz, P.T, P.W);
+      if (s >= 0) {
+        const long long idx = (static_cast<long long>(s) * g.ny + y) * g.nx + x;
+        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+        float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
+        d_ey_dz = pml_corr<FMA>(d_ey_dz, b, a, ik, p0);
+        d_ex_dz = pml_corr<FMA>(d_ex_dz, b, a, ik, p1);
+        if (write_psi) {
+          P.psi_nxt[idx] = p0;
+          P.psi_nxt[P.cells + idx] = p1;
+        }
+      }
+    }
+  }
+  hxo = h_new<FMA>(da, c.hx, db, sub(d_ez_dy, d_ey_dz));
+  hyo = h_new<FMA>(da, c.hy, db, sub(d_ex_dz, d_ez_dx));
+  hzo = h_new<FMA>(da, c.hz, db, sub(d_ey_dx, d_ex_dy));
+}
+
+struct EIn {
+  float hx, hy, hz, hz_my, hx_my, hy_mz, hx_mz, hz_mx, hy_mx, ex, ey, ez;
+};
+
+// update_e_field[_pml] for one cell (src/fdtd.rs:369-509)
+template <bool FMA, bool PML>
+__device__ __forceinline__ void e_cell(const EIn &c, float ca, float cb, const GridArgs &g, int x,
+                                       int y, int p, bool pml_ok, float &exo, float &eyo,
+                                       float &ezo) {
+  float d_hz_dy = sub(c.hz, c.hz_my), d_hx_dy = sub(c.hx, c.hx_my);
+  float d_hy_dz = sub(c.hy, c.hy_mz), d_hx_dz = sub(c.hx, c.hx_mz);
+  float d_hz_dx = sub(c.hz, c.hz_mx), d_hy_dx = sub(c.hy, c.hy_mx);
+  if (PML && pml_ok) {
+    {
+      const PmlAxis &P = g.pml[0];
+      const int s = slab_pos(x, g.nx, P.T, P.W);
+      if (s >= 0) {
+        const long long idx = (static_cast<long long>(p) * g.ny + y) * P.W + s;
+        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+        float p2 = __ldg(P.psi_cur + 2 * P.cells + idx), p3 = __ldg(P.psi_cur + 3 * P.cells + idx);
+        d_hz_dx = pml_corr<FMA>(d_hz_dx, b, a, ik, p2);
+        d_hy_dx = pml_corr<FMA>(d_hy_dx, b, a, ik, p3);
+        P.psi_nxt[2 * P.cells + idx] = p2;
+        P.psi_nxt[3 * P.cells + idx] = p3;
+      }
+    }
+    {
+      const PmlAxis &P = g.pml[1];
+      const int s = slab_pos(y, g.ny, P.T, P.W);
+      if (s >= 0) {
+        const long long idx = (static_cast<long long>(p) * P.W + s) * g.nx + x;
+        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+        float p2 = __ldg(P.psi_cur + 2 * P.cells + idx), p3 = __ldg(P.psi_cur + 3 * P.cells + idx);
+        d_hz_dy = pml_corr<FMA>(d_hz_dy, b, a, ik, p2);
+        d_hx_dy = pml_corr<FMA>(d_hx_dy, b, a, ik, p3);
+        P.psi_nxt[2 * P.cells + idx] = p2;
+        P.psi_nxt[3 * P.cells + idx] = p3;
+      }
+    }
+    {
+      const PmlAxis &P = g.pml[2];
+      const int s = slab_pos(p, g.nz, P.T, P.W);
+      if (s >= 0) {
+        const long long idx = (static_cast<long long>(s) * g.ny + y) * g.nx + x;
+        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+        float p2 = __ldg(P.psi_cur + 2 * P.cells + idx), p3 = __ldg(P.psi_cur + 3 * P.cells + idx);
+        d_hy_dz = pml_corr<FMA>(d_hy_dz, b, a, ik, p2);
+        d_hx_dz = pml_corr<FMA>(d_hx_dz, b, a, ik, p3);
+        P.psi_nxt[2 * P.cells + idx] = p2;
+        P.psi_nxt[3 * P.cells + idx] = p3;
+      }
+    }
+  }
+  exo = e_new<FMA>(ca, c.ex, cb, sub(d_hz_dy, d_hy_dz));
+  eyo = e_new<FMA>(ca, c.ey, cb, sub(d_hx_dz, d_hz_dx));
+  ezo = e_new<FMA>(ca, c.ez, cb, sub(d_hy_dx, d_hx_dy));
+}
+
+__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float comp(const float4 &v, int q) {
+  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+
+template <int TY, int S, bool FMA, bool PML>
+__device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtensorMap *tmH,
+                                           const CUtensorMap *tmM, const FusedArgs &a,
+                                           unsigned char *smem, int x0, int y0, int k0, int k1) {
+  using L = Layout<TY, S>;
+  const GridArgs &g = a.g;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const float4 *s_coef = reinterpret_cast<const float4 *>(smem);
+  unsigned char *s_stage = smem + L::STAGE_OFF;
+  float *s_plane = reinterpret_cast<float *>(smem + L::PLANE_OFF);
+  uint64_t *s_bar = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+
+  const int nx = g.nx, ny = g.ny;
+  const long long N = g.N;
+  const int kfirst = k0 > 0 ? k0 - 1 : 0;  // k0-1: warm-up plane for H(k0-1)
+  const int np = k1 - kfirst + 1;          // planes staged; plane k1 brings only E
+
+  auto issue = [&](int j) {
+    const int p = kfirst + j;
+    const int slot = j % S;
+    unsigned char *st = s_stage + slot * L::STAGE;
+    const uint32_t bar = smem_u32(&s_bar[slot]);
+    const bool e_only = (p == k1);
+    mbar_expect_tx(bar, e_only ? L::E_BYTES : (L::E_BYTES + L::H_BYTES + L::M_BYTES));
+    tma_load_4d(smem_u32(st), tmE, x0 - 4, y0 - 1, p, 0, bar);
+    if (!e_only) {
+      tma_load_4d(smem_u32(st + L::H_OFF), tmH, x0 - 4, y0 - 1, p, 3, bar);
+      tma_load_3d(smem_u32(st + L::M_OFF), tmM, x0 - 16, y0 - 1, p, bar);
+    }
+  };
+
+  int issued = 0;
+  if (tid == 0) {
+    const int pro = np < S ? np : S;
+    for (int j = 0; j < pro; ++j) issue(j);
+    issued = pro;
+  }
+  bool ok = mbar_wait(smem_u32(&s_bar[0]), 0);
+  int done = ok ? 1 : 0;  // stages [0, done) seen complete, in order
+
+  const bool tile_warp = warp < TY;
+  const int r = tile_warp ? warp + 1 : 0;  // smem row: 0 is the -y halo row y0-1
+  const int y = y0 - 1 + r;
+  const int xg = x0 + 4 * lane;
+  const bool row_in = (y >= 0) && (y < ny);
+  const bool x_in = xg < nx;  // nx % 8 == 0: a lane's 4 cells are all in or all out
+  const int cE = 4 + 4 * lane;
+  float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;  // H(p-1), own cells
+
+  for (int j = 0; j < np - 1; ++j) {
+    const int p = kfirst + j;
+    const bool warm = p < k0;
+    const bool arrived = mbar_wait(smem_u32(&s_bar[(j + 1) % S]), ((j + 1) / S) & 1);
+    if (arrived && done == j + 1) done = j + 2;
+    ok = arrived && ok;
+    const unsigned char *stc = s_stage + (j % S) * L::STAGE;
+    const float *Ec = reinterpret_cast<const float *>(stc);
+    const float *En = reinterpret_cast<const float *>(s_stage + ((j + 1) % S) * L::STAGE);
+    const float *Hc = reinterpret_cast<const float *>(stc + L::H_OFF);
+    const uint8_t *Mc = stc + L::M_OFF;
+    float *pl = s_plane + (p & 1) * L::PLANE_FLOATS;
+    float *pl_hz = pl, *pl_hx = pl + L::PROWS * kTileX;
+    float *pl_hzh = pl + 2 * L::PROWS * kTileX, *pl_hyh = pl_hzh + 32;
+
+    // ---------------- H phase ----------------
+    float ha[4], hb[4], hc[4];  // new hx, hy, hz of this lane's 4 cells
+    float4 ex4, ey4, ez4;
+    uchar4 m4;
+    if (tile_warp || !warm) {
+      auto E4 = [&](const float *B, int c, int row) { return lds4(B + (c * L::EH + row) * L::EW + cE); };
+      ex4 = E4(Ec, 0, r);
+      ey4 = E4(Ec, 1, r);
+      ez4 = E4(Ec, 2, r);
+      const float4 ex_py = E4(Ec, 0, r + 1), ez_py = E4(Ec, 2, r + 1);
+      const float4 ex_pz = E4(En, 0, r), ey_pz = E4(En, 1, r);
+      float ez_n = __shfl_down_sync(0xffffffffu, ez4.x, 1);
+      float ey_n = __shfl_down_sync(0xffffffffu, ey4.x, 1);
+      if (lane == 31) {
+        ez_n = Ec[(2 * L::EH + r) * L::EW + 4 + kTileX];
+        ey_n = Ec[(1 * L::EH + r) * L::EW + 4 + kTileX];
+      }
+      const float4 hx4 = lds4(Hc + (0 * L::HH + r) * L::HW + cE);
+      const float4 hy4 = lds4(Hc + (1 * L::HH + r) * L::HW + cE);
+      const float4 hz4 = lds4(Hc + (2 * L::HH + r) * L::HW + cE);
+      m4 = *reinterpret_cast<const uchar4 *>(Mc + r * L::MW + 16 + 4 * lane);
+      const bool cell_ok = row_in && x_in;
+      const bool wpsi = tile_warp && !warm && cell_ok;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        HIn c;
+        c.ex = comp(ex4, q); c.ey = comp(ey4, q); c.ez = comp(ez4, q);
+        c.ex_py = comp(ex_py, q); c.ez_py = comp(ez_py, q);
+        c.ex_pz = comp(ex_pz, q); c.ey_pz = comp(ey_pz, q);
+        c.ez_px = q < 3 ? comp(ez4, q + 1) : ez_n;
+        c.ey_px = q < 3 ? comp(ey4, q + 1) : ey_n;
+        c.hx = comp(hx4, q); c.hy = comp(hy4, q); c.hz = comp(hz4, q);
+        const unsigned char id = q == 0 ? m4.x : (q == 1 ? m4.y : (q == 2 ? m4.z : m4.w));
+        const float4 cf = s_coef[id];
+        h_cell<FMA, PML>(c, cf.z, cf.w, g, xg + q, y, p, cell_ok, wpsi, ha[q], hb[q], hc[q]);
+      }
+      if (!row_in) {  // outside the domain in y: zero field (OUTER_ZERO_BLOCK)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ha[q] = hb[q] = hc[q] = 0.0f;
+      }
+      if (!warm) {
+        *reinterpret_cast<float4 *>(pl_hz + r * kTileX + 4 * lane) = make_float4(hc[0], hc[1], hc[2], hc[3]);
+        *reinterpret_cast<float4 *>(pl_hx + r * kTileX + 4 * lane) = make_float4(ha[0], ha[1], ha[2], ha[3]);
+        if (tile_warp && cell_ok) {
+          float *Hn = g.nxt + 3 * N + (static_cast<long long>(p) * ny + y) * nx + xg;
+          *reinterpret_cast<float4 *>(Hn) = make_float4(ha[0], ha[1], ha[2], ha[3]);
+          *reinterpret_cast<float4 *>(Hn + N) = make_float4(hb[0], hb[1], hb[2], hb[3]);
+          *reinterpret_cast<float4 *>(Hn + 2 * N) = make_float4(hc[0], hc[1], hc[2], hc[3]);
+        }
+      }
+      // -x halo column (x0-1, y0..y0+TY-1): Hz and Hy for the E update at x0
+      if (!tile_warp && !warm && lane < TY) {
+        const int rh = lane + 1, yh = y0 + lane, xh = x0 - 1;
+        float hzv = 0.0f, hyv = 0.0f;
+        if (x0 > 0 && yh < ny) {
+          HIn c;
+          c.ex = Ec[(0 * L::EH + rh) * L::EW + 3];
+          c.ey = Ec[(1 * L::EH + rh) * L::EW + 3];
+          c.ez = Ec[(2 * L::EH + rh) * L::EW + 3];
+          c.ex_py = Ec[(0 * L::EH + rh + 1) * L::EW + 3];
+          c.ez_py = Ec[(2 * L::EH + rh + 1) * L::EW + 3];
+          c.ex_pz = En[(0 * L::EH + rh) * L::EW + 3];
+          c.ey_pz = En[(1 * L::EH + rh) * L::EW + 3];
+          c.ez_px = Ec[(2 * L::EH + rh) * L::EW + 4];
+          c.ey_px = Ec[(1 * L::EH + rh) * L::EW + 4];
+          c.hx = Hc[(0 * L::HH + rh) * L::HW + 3];
+          c.hy = Hc[(1 * L::HH + rh) * L::HW + 3];
+          c.hz = Hc[(2 * L::HH + rh) * L::HW + 3];
+          const float4 cf = s_coef[Mc[rh * L::MW + 15]];
+          float hxv;
+          h_cell<FMA, PML>(c, cf.z, cf.w, g, xh, yh, p, true, false, hxv, hyv, hzv);
+        }
+        pl_hzh[rh] = hzv;
+        pl_hyh[rh] = hyv;
+      }
+    }
+
+    ok = __syncthreads_or(ok ? 0 : 1) == 0;
+    if (!ok) break;
+    if (tid == 0 && issued < np) {  // stage j is consumed: refill its slot
+      fence_proxy_async();
+      issue(issued);
+      ++issued;
+    }
+
+    // ---------------- E phase ----------------
+    if (tile_warp) {
+      if (!warm) {
+        const float4 hz_my = lds4(pl_hz + (r - 1) * kTileX + 4 * lane);
+        const float4 hx_my = lds4(pl_hx + (r - 1) * kTileX + 4 * lane);
+        float hz_w = __shfl_up_sync(0xffffffffu, hc[3], 1);
+        float hy_w = __shfl_up_sync(0xffffffffu, hb[3], 1);
+        if (lane == 0) {
+          hz_w = pl_hzh[r];
+          hy_w = pl_hyh[r];
+        }
+        const bool cell_ok = row_in && x_in;
+        float eo[3][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          EIn c;
+          c.hx = ha[q]; c.hy = hb[q]; c.hz = hc[q];
+          c.hz_my = comp(hz_my, q); c.hx_my = comp(hx_my, q);
+          c.hy_mz = comp(hyp, q); c.hx_mz = comp(hxp, q);
+          c.hz_mx = q == 0 ? hz_w : hc[q - 1];
+          c.hy_mx = q == 0 ? hy_w : hb[q - 1];
+          c.ex = comp(ex4, q); c.ey = comp(ey4, q); c.ez = comp(ez4, q);
+          const unsigned char id = q == 0 ? m4.x : (q == 1 ? m4.y : (q == 2 ? m4.z : m4.w));
+          const float4 cf = s_coef[id];
+          e_cell<FMA, PML>(c, cf.x, cf.y, g, xg + q, y, p, cell_ok, eo[0][q], eo[1][q], eo[2][q]);
+        }
+        if (cell_ok) {
+          float *Ep = g.nxt + (static_cast<long long>(p) * ny + y) * nx + xg;
+          *reinterpret_cast<float4 *>(Ep) = make_float4(eo[0][0], eo[0][1], eo[0][2], eo[0][3]);
+          *reinterpret_cast<float4 *>(Ep + N) = make_float4(eo[1][0], eo[1][1], eo[1][2], eo[1][3]);
+          *reinterpret_cast<float4 *>(Ep + 2 * N) = make_float4(eo[2][0], eo[2][1], eo[2][2], eo[2][3]);
+        }
+      }
+      hxp = make_float4(ha[0], ha[1], ha[2], ha[3]);
+      hyp = make_float4(hb[0], hb[1], hb[2], hb[3]);
+    }
+  }
+
+  if (!ok) {
+    // A staged plane never arrived within the wait limit: latch the error and
+    // wait (again bounded) for this CTA's copies still in flight before its
+    // shared memory is released.
+    if (tid == 0) {
+      atomicOr(g.err, kErrTimeout);
+      for (int jj = done; jj < issued; ++jj) mbar_wait(smem_u32(&s_bar[jj % S]), (jj / S) & 1);
+    }
+  }
+}
+
+template <int TY, int S, bool FMA>
+__global__ void __launch_bounds__(32 * (TY + 1))
+    k_fused(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
+            const __grid_constant__ CUtensorMap tmM, const FusedArgs a) {
+  using L = Layout<TY, S>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *smem = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
+  int item = blockIdx.x;
+  const int txi = item % a.tiles_x;
+  item /= a.tiles_x;
+  const int tyi = item % a.tiles_y;
+  const int zc = item / a.tiles_y;
+  const int x0 = txi * kTileX, y0 = tyi * TY;
+  const int k0 = zc * a.zchunk;
+  const int k1 = min(k0 + a.zchunk, a.g.nz);
+
+  float4 *s_coef = reinterpret_cast<float4 *>(smem);
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) s_coef[i] = a.g.coef[i];
+  if (threadIdx.x == 0) {
+    uint64_t *s_bar = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+    for (int s = 0; s < S; ++s) mbar_init(smem_u32(&s_bar[s]), 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  // Does this CTA meet a graded CPML slab?  Interior CTAs skip all psi code.
+  bool pml = false;
+  if (a.has_pml) {
+    const PmlAxis &X = a.g.pml[0], &Y = a.g.pml[1], &Z = a.g.pml[2];
+    const int xh = min(x0 + kTileX, a.g.nx) - 1, yh = min(y0 + TY, a.g.ny) - 1;
+    if (X.T > 0 && (x0 - 1 < X.T || xh >= a.g.nx - X.T)) pml = true;
+    if (Y.T > 0 && (y0 - 1 < Y.T || yh >= a.g.ny - Y.T)) pml = true;
+    if (Z.T > 0 && (k0 - 1 < Z.T || k1 - 1 >= a.g.nz - Z.T)) pml = true;
+  }
+  if (pml)
+    fused_body<TY, S, FMA, true>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
+  else
+    fused_body<TY, S, FMA, false>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
+}
+
+template <int TY, int S>
+cudaError_t prepare_t() {
+  using L = Layout<TY, S>;
+  cudaError_t e = cudaFuncSetAttribute(k_fused<TY, S, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_fused<TY, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              L::BYTES);
+}
+
+template <int TY, int S, bool FMA>
+cudaError_t launch_t(const CUtensorMap &tmE, const CUtensorMap &tmH, const CUtensorMap &tmM,
+                     const FusedArgs &a, cudaStream_t s) {
+  using L = Layout<TY, S>;
+  const long long nz_chunks = (a.g.nz + a.zchunk - 1) / a.zchunk;
+  const long long items = static_cast<long long>(a.tiles_x) * a.tiles_y * nz_chunks;
+  k_fused<TY, S, FMA><<<static_cast<unsigned>(items), L::THREADS, L::BYTES, s>>>(tmE, tmH, tmM, a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+void fused_boxes(int ty, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]) {
+  e_box[0] = kTileX + 8; e_box[1] = ty + 2; e_box[2] = 1; e_box[3] = 3;
+  h_box[0] = kTileX + 4; h_box[1] = ty + 1; h_box[2] = 1; h_box[3] = 3;
+  m_box[0] = kTileX + 16; m_box[1] = ty + 1; m_box[2] = 1;
+}
+
+#define WF_FUSED_CONFIGS(X) \
+  X(4, 3) X(4, 4) X(8, 3) X(8, 4) X(12, 3) X(16, 2) X(16, 3)
+
+bool fused_supported(const FusedConfig &c) {
+#define X(T, S_) if (c.ty == T && c.stages == S_) return c.zchunk >= 1;
+  WF_FUSED_CONFIGS(X)
+#undef X
+  return false;
+}
+
+int fused_smem_bytes(const FusedConfig &c) {
+#define X(T, S_) if (c.ty == T && c.stages == S_) return Layout<T, S_>::BYTES;
+  WF_FUSED_CONFIGS(X)
+#undef X
+  return -1;
+}
+
+cudaError_t fused_prepare(const FusedConfig &c) {
+#define X(T, S_) if (c.ty == T && c.stages == S_) return prepare_t<T, S_>();
+  WF_FUSED_CONFIGS(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fused(const FusedConfig &c, const CUtensorMap &tmE, const CUtensorMap &tmH,
+                         const CUtensorMap &tmM, const FusedArgs &a, bool fma, cudaStream_t s) {
+#define X(T, S_)                                                         \
+  if (c.ty == T && c.stages == S_)                                      \
+    return fma ? launch_t<T, S_, true>(tmE, tmH, tmM, a, s)             \
+               : launch_t<T, S_, false>(tmE, tmH, tmM, a, s);
+  WF_FUSED_CONFIGS(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace wf

@@ -1,0 +1,245 @@
+"""The device field grid and the run loop, mirroring src/engine.rs of the reference.
+
+`DeviceFieldGrid` owns one C-ABI handle: the double-buffered SoA field state,
+material ids, coefficient table, CPML psi, sources and probes on one GPU.
+`run()` keeps engine::run's contract (src/engine.rs:653-819): each step is
+H everywhere, E everywhere, sources in order, probes, and an optional
+snapshot when step % snapshot_every == 0, handed to a callback in the
+reference's FieldBlock byte order (the host writer stays with the caller).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from dataclasses import dataclass
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as _L
+from .layout import GridDims, MaterialGrid, MaterialTable, PmlContext
+
+_BOUNDARY = {"zero": 0, "periodic": 1}
+_ARITH = {"exact": 0, "fma": 1}
+_KERNEL = {"auto": 0, "fused": 1, "split": 2}
+
+# PmlAux array order of src/layout.rs:545-558
+PSI_NAMES = ["psi_ez_dx", "psi_ey_dx", "psi_ez_dy", "psi_ex_dy", "psi_ey_dz", "psi_ex_dz",
+             "psi_hz_dx", "psi_hy_dx", "psi_hx_dy", "psi_hz_dy", "psi_hy_dz", "psi_hx_dz"]
+
+
+class DeviceFieldGrid:
+    def __init__(self, dims: GridDims, boundary=("zero", "zero", "zero"), arith: str = "exact",
+                 kernel: str = "auto", device: int = 0, stream: Optional[int] = None):
+        self.dims = dims
+        d = _L.GridDesc()
+        d.nx, d.ny, d.nz = dims.nx, dims.ny, dims.nz
+        for i, b in enumerate(boundary):
+            d.boundary[i] = _BOUNDARY[b]
+        d.arith = _ARITH[arith]
+        d.kernel = _KERNEL[kernel]
+        d.precision = 0
+        d.device = device
+        d.stream = stream
+        h = C.c_void_p()
+        _L.check(_L.lib().wf_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.n_sources = 0
+        self.n_probes = 0
+
+    # -- lifetime ----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            _L.lib().wf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _chk(self, st):
+        _L.check(st, self._h)
+
+    # -- scene ---------------------------------------------------------------
+    def set_materials(self, grid: MaterialGrid, table: MaterialTable):
+        ids = np.ascontiguousarray(grid.ids, np.uint8)
+        q = np.ascontiguousarray(table.q16, np.int32)
+        self._chk(_L.lib().wf_set_materials(self._h, _L.ptr(ids, _L.u8p), _L.ptr(q, _L.i32p)))
+
+    def set_pml(self, ctx: PmlContext):
+        for axis in range(3):
+            p = ctx.profiles[axis]
+            t = ctx.thickness_voxels[axis]
+            self._chk(_L.lib().wf_set_pml(self._h, axis, t, _L.ptr(p.b, _L.f32p),
+                                          _L.ptr(p.a, _L.f32p), _L.ptr(p.inv_kappa, _L.f32p)))
+
+    def set_pml_axis(self, axis: int, thickness: int, b, a, inv_kappa):
+        b, a, k = (np.ascontiguousarray(v, np.float32) for v in (b, a, inv_kappa))
+        self._chk(_L.lib().wf_set_pml(self._h, axis, thickness, _L.ptr(b, _L.f32p),
+                                      _L.ptr(a, _L.f32p), _L.ptr(k, _L.f32p)))
+
+    def add_source_values(self, x, y, z, comp, values, mode=0) -> int:
+        v = np.ascontiguousarray(values, np.float32)
+        idx = C.c_int()
+        self._chk(_L.lib().wf_add_source(self._h, x, y, z, int(comp), mode, _L.ptr(v, _L.f32p),
+                                         len(v), C.byref(idx)))
+        self.n_sources += 1
+        return idx.value
+
+    def add_probe_tables(self, x, y, z, comp, cos_tab, sin_tab, first_step=0,
+                         record_trace=False) -> int:
+        c = np.ascontiguousarray(cos_tab, np.float64)
+        s = np.ascontiguousarray(sin_tab, np.float64)
+        nsteps = c.shape[0]
+        nfreq = c.shape[1] if c.ndim == 2 else 0
+        idx = C.c_int()
+        self._chk(_L.lib().wf_add_probe(self._h, x, y, z, int(comp), nfreq, _L.ptr(c, _L.f64p),
+                                        _L.ptr(s, _L.f64p), nsteps, first_step, int(record_trace),
+                                        C.byref(idx)))
+        self.n_probes += 1
+        return idx.value
+
+    # -- stepping -------------------------------------------------------------
+    def step(self, n: int = 1):
+        self._chk(_L.lib().wf_step(self._h, n))
+
+    def sync(self):
+        self._chk(_L.lib().wf_sync(self._h))
+
+    @property
+    def steps_done(self) -> int:
+        return int(_L.lib().wf_steps_done(self._h))
+
+    # -- timing -------------------------------------------------------------
+    def stream(self) -> int:
+        v = C.c_void_p()
+        self._chk(_L.lib().wf_get_stream(self._h, C.byref(v)))
+        return int(v.value or 0)
+
+    def set_timing(self, enable: bool):
+        self._chk(_L.lib().wf_set_timing(self._h, int(enable)))
+
+    def timing(self):
+        """(summed step-kernel milliseconds, launches) since set_timing(True)."""
+        ms = C.c_double()
+        n = C.c_int64()
+        self._chk(_L.lib().wf_get_timing(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    # -- tiling -------------------------------------------------------------
+    def tiling(self):
+        t = _L.Tiling()
+        self._chk(_L.lib().wf_get_tiling(self._h, C.byref(t)))
+        return t.tile_rows, t.z_chunk, t.stages
+
+    def set_tiling(self, tile_rows, z_chunk, stages):
+        t = _L.Tiling(tile_rows, z_chunk, stages)
+        self._chk(_L.lib().wf_set_tiling(self._h, C.byref(t)))
+
+    def autotune(self, steps: int = 5):
+        t = _L.Tiling()
+        ms = C.c_float()
+        self._chk(_L.lib().wf_autotune(self._h, steps, C.byref(t), C.byref(ms)))
+        return (t.tile_rows, t.z_chunk, t.stages), ms.value
+
+    # -- read-back ------------------------------------------------------------
+    def fields(self) -> np.ndarray:
+        d = self.dims
+        out = np.empty((6, d.nz, d.ny, d.nx), np.float32)
+        self._chk(_L.lib().wf_get_fields(self._h, _L.ptr(out, _L.f32p)))
+        return out
+
+    def set_fields(self, f6):
+        a = np.ascontiguousarray(f6, np.float32)
+        self._chk(_L.lib().wf_set_fields(self._h, _L.ptr(a, _L.f32p)))
+
+    def download_blocks(self) -> np.ndarray:
+        out = np.empty(self.dims.voxel_count() * 6, np.float32)
+        self._chk(_L.lib().wf_download_blocks(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def upload_blocks(self, blocks):
+        a = np.ascontiguousarray(blocks, np.float32)
+        self._chk(_L.lib().wf_upload_blocks(self._h, a.ctypes.data_as(C.c_void_p)))
+
+    def psi(self, which: int) -> np.ndarray:
+        d = self.dims
+        out = np.empty((d.nz, d.ny, d.nx), np.float32)
+        self._chk(_L.lib().wf_get_psi(self._h, which, _L.ptr(out, _L.f32p)))
+        return out
+
+    def probe_sums(self, p: int, nfreq: int):
+        c = np.zeros(max(nfreq, 1), np.float64)
+        s = np.zeros(max(nfreq, 1), np.float64)
+        n = C.c_uint64()
+        self._chk(_L.lib().wf_probe_sums(self._h, p, _L.ptr(c, _L.f64p), _L.ptr(s, _L.f64p),
+                                         C.byref(n)))
+        return c[:nfreq], s[:nfreq], int(n.value)
+
+    def probe_trace(self, p: int, n: int) -> np.ndarray:
+        out = np.empty(n, np.float32)
+        self._chk(_L.lib().wf_probe_trace(self._h, p, _L.ptr(out, _L.f32p), n))
+        return out
+
+    def device_field_ptrs(self):
+        arr = (C.c_void_p * 6)()
+        self._chk(_L.lib().wf_device_fields(self._h, arr))
+        return [int(v) for v in arr]
+
+
+@dataclass
+class EngineConfig:
+    """src/engine.rs:608-615 (output_path is the caller's snapshot sink)."""
+    num_steps: int
+    dt: float
+    snapshot_every: int = 0
+    snapshot_sink: Optional[Callable[[int, np.ndarray], None]] = None
+
+
+def run(grid: DeviceFieldGrid, sources: Sequence, probes: Sequence, config: EngineConfig,
+        quiet: bool = True) -> float:
+    """engine::run (src/engine.rs:653-819) on the device.  Returns wall seconds of
+    the step loop.  Probe objects receive their sums, count and optional trace."""
+    n = config.num_steps
+    base_src, base_prb = grid.n_sources, grid.n_probes
+    for s in sources:
+        grid.add_source_values(s.x, s.y, s.z, s.component, s.values(config.dt, n), s.mode)
+    for p in probes:
+        c, si = p.tables(config.dt, n)
+        grid.add_probe_tables(p.x, p.y, p.z, p.component, c, si, p.first_step(config.dt),
+                              p.record_trace)
+    grid.sync()
+    t0 = time.perf_counter()
+    every = max(config.snapshot_every, 1) if config.snapshot_sink else 0
+    done = 0
+    while done < n:
+        if every:
+            # next step index with step % every == 0 (taken after that step)
+            nxt = ((done + every - 1) // every) * every
+            chunk = nxt - done + 1 if nxt < n else n - done
+        else:
+            chunk = n - done
+        grid.step(chunk)
+        done += chunk
+        if every and (done - 1) % every == 0:
+            config.snapshot_sink(done - 1, grid.download_blocks())
+    grid.sync()
+    wall = time.perf_counter() - t0
+    for i, p in enumerate(probes):
+        sc, ss, cnt = grid.probe_sums(base_prb + i, len(p.frequencies_hz))
+        p.sum_cos, p.sum_sin, p.samples_recorded = sc, ss, cnt
+        if p.record_trace:
+            p.trace = grid.probe_trace(base_prb + i, n)
+    if not quiet:
+        d = grid.dims
+        print(f"wavefront_b200: {n} steps in {wall:.3f}s ({n / max(wall, 1e-9):.1f} steps/s, "
+              f"{d.voxel_count() * n / max(wall, 1e-9) / 1e6:.1f} Mcell/s)")
+    return wall
