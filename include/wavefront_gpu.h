@@ -192,6 +192,32 @@ wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t);
 /* Times each candidate tiling for `steps` steps and keeps the fastest. */
 wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms);
 
+/* ---- allocation-free stepping of caller-owned fields --------------------- */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * -- an application whose device memory belongs entirely to its own pool
+ * allocator, or a latency-critical loop in which an allocation (which can
+ * synchronise the device) is not allowed.  Advances the caller's device
+ * fields in place by nsteps Yee steps with no CPML, sources or probes:
+ *   fields6   device pointer, 6*nx*ny*nz floats, component-major ex..hz,
+ *             x fastest (the layout wf_device_fields reports);
+ *   ids       device pointer, nz*ny*nx material ids (MaterialGrid order);
+ *   table_q16 host pointer, the 256-entry Q16.16 table {ca, cb, da, db};
+ *   boundary  wf_boundary per axis; arith wf_arith; stream cudaStream_t.
+ * Allocates nothing: the next-state buffer is a static device array of at
+ * most 262144 cells (6 MiB, held by every GPU that loads the library until
+ * the process exits); larger grids are rejected with WF_ERR_ARG.  The first
+ * call on a device looks up that array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  Every call shares the array,
+ * so calls that overlap on the GPU (other streams, other threads) race.
+ * Results are bit-identical to wf_step on a handle with the same inputs.
+ * Errors are described by wf_noalloc_last_error(). */
+wf_status wf_step_fields_noalloc(float *fields6, const uint8_t *ids,
+                                 const int32_t (*table_q16)[4], int nx, int ny,
+                                 int nz, const int32_t boundary[3], int arith,
+                                 int nsteps, void *stream);
+const char *wf_noalloc_last_error(void);
+
 /* ---- host helpers: the reference's setup math ---------------------------- */
 
 int32_t wf_q16_from_f32(float v);   /* FixedQ16_16::from_f32, src/layout.rs:114-116 */

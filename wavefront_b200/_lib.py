@@ -24,6 +24,7 @@ EXPORTS = [
     "wf_material_coeffs", "wf_effective_pml_thickness_blocks", "wf_pml_profile",
     "wf_waveform_eval", "wf_source_values", "wf_probe_first_step", "wf_probe_tables",
     "wf_spectrum", "wf_scene_voxelize", "wf_demo_sphere",
+    "wf_step_fields_noalloc", "wf_noalloc_last_error",
 ]
 
 
@@ -133,6 +134,12 @@ def lib() -> C.CDLL:
                                         _u8p, _i32p, C.POINTER(C.c_int), C.c_char_p, C.c_int]
         L.wf_scene_voxelize.restype = S
         L.wf_demo_sphere.argtypes = [C.c_int, C.c_int, C.c_int, _u8p]
+        L.wf_step_fields_noalloc.argtypes = [C.c_void_p, C.c_void_p, _i32p, C.c_int, C.c_int,
+                                             C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int,
+                                             C.c_void_p]
+        L.wf_step_fields_noalloc.restype = S
+        L.wf_noalloc_last_error.argtypes = []
+        L.wf_noalloc_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
