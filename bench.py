@@ -34,9 +34,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_CELLS = 512 ** 3
 METRIC = "Mcell-updates/s"
-WORKLOAD = "two_spheres_512^3_fp32_cpml16_gaussian_8probes"
+GRID = 512  # set by --grid (smaller grids are for profiling captures only)
+N_CELLS = GRID ** 3
+WORKLOAD = f"two_spheres_{GRID}^3_fp32_cpml16_gaussian_8probes"
 
 
 def algorithmic_bytes(sc) -> int:
@@ -124,14 +125,14 @@ def cpu_baseline(sc, seconds=15.0):
     el = time.perf_counter() - t0
     sim.close()
     return {"value": round(sc.dims.voxel_count() * n / el / 1e6, 2), "unit": METRIC, "cores": nt,
-            "kind": "port", "sample": f"{n} full 512^3 steps after 1 warm-up step, {el:.1f} s"}
+            "kind": "port", "sample": f"{n} full {GRID}^3 steps after 1 warm-up step, {el:.1f} s"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     from wavefront_b200 import configs
-    sc = configs.two_spheres(n=512, steps=args.warmup + args.steps)
+    sc = configs.two_spheres(n=GRID, steps=args.warmup + args.steps)
     from oracle import oracle as O
     nt = os.cpu_count() or 1
     sim = O.sim_from_scenario(sc, steps=args.warmup + args.steps)
@@ -152,7 +153,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": METRIC,
         "n_gpus": world, "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": round(el / n * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "grid": [512, 512, 512],
+        "data": "synthetic", "config": {"workload": WORKLOAD, "grid": [GRID] * 3,
                                         "l2": "inputs larger than L2 (3.2 GB of fields)"},
         "cpu_baseline": {"value": round(v, 2), "unit": METRIC, "cores": nt, "kind": "port",
                          "sample": f"{n} of {args.steps} requested 512^3 steps in {el:.1f} s "
@@ -172,7 +173,7 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     total = args.warmup + args.steps
-    sc = configs.two_spheres(n=512, steps=total)
+    sc = configs.two_spheres(n=GRID, steps=total)
 
     def build(kernel="fused"):
         g = configs.device_grid(sc, kernel=kernel, device=local_rank)
@@ -256,7 +257,7 @@ def run_ours(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [512, 512, 512], "cpml_cells": 16,
+            "config": {"workload": WORKLOAD, "grid": [GRID] * 3, "cpml_cells": 16,
                        "probes": 8, "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
                        "tiling": list(build_tiling(args)),
                        "l2": "inputs larger than L2 (3.2 GB of fields per state buffer)",
@@ -294,7 +295,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tiling", default="", help="tile_rows,z_chunk,stages")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--grid", type=int, default=512, help="cube edge (profiling captures only)")
     args = ap.parse_args()
+    global GRID, N_CELLS, WORKLOAD
+    GRID = args.grid
+    N_CELLS = GRID ** 3
+    WORKLOAD = f"two_spheres_{GRID}^3_fp32_cpml16_gaussian_8probes"
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))
