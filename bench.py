@@ -188,6 +188,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- device-resident throughput (value) + fused-kernel roofline -------
     g = build()
+    tiling = list(g.tiling())
     g.step(args.warmup)
     g.sync()
     g.set_timing(True)
@@ -259,7 +260,8 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": [GRID] * 3, "cpml_cells": 16,
                        "probes": 8, "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
-                       "tiling": list(build_tiling(args)),
+                       "tiling": {"tile_rows": tiling[0], "z_chunk": tiling[1],
+                                  "stages": tiling[2]},
                        "l2": "inputs larger than L2 (3.2 GB of fields per state buffer)",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": round(e2e, 1), "unit": METRIC,
@@ -279,12 +281,6 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
-
-
-def build_tiling(args):
-    if args.tiling:
-        return tuple(int(v) for v in args.tiling.split(","))
-    return (8, 64, 3)
 
 
 def main():

@@ -39,7 +39,7 @@ struct ProbeRec {
 };
 
 struct AxisState {
-  int T = 0, W = 0;
+  int T = 0, W = 0, pitch = 0;
   float *prof = nullptr;       // [3][W]
   float *psi[2] = {nullptr, nullptr};
   long long cells = 0;
@@ -70,8 +70,9 @@ struct wf_handle {
   long long *d_step = nullptr;
   int *d_err = nullptr;
   long long steps_done = 0;
-  FusedConfig cfg{8, 64, 3};
-  CUtensorMap tmE[2], tmH[2], tmM;
+  FusedConfig cfg{4, 32, 3};
+  bool cfg_user_set = false;  // otherwise chosen from the grid at first use
+  wf::FusedMaps maps[2];      // per state buffer (the one read by the step)
   bool maps_ok = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_steps = 0;
@@ -140,37 +141,42 @@ bool use_fused(const wf_handle *h) {
   return fused_allowed(h) && encode_fn() != nullptr;
 }
 
-// TMA descriptors: fields as a 4D tensor {nx, ny, nz, 6} per buffer, ids as
-// {nx, ny, nz} with a 16-byte-multiple row pitch.
+bool has_pml(const wf_handle *h) { return h->ax[0].T > 0 || h->ax[1].T > 0 || h->ax[2].T > 0; }
+
+// One tiled TMA descriptor (no swizzle, no interleave, zero out-of-bounds fill).
+bool encode(CUtensorMap *m, CUtensorMapDataType t, int rank, void *base, const cuuint64_t *dims,
+            const cuuint64_t *strides, const cuuint32_t *box) {
+  static const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+  return encode_fn()(m, t, rank, base, dims, strides, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TMA descriptors per state buffer: fields as a 4D tensor {nx, ny, nz, 6},
+// ids as {nx, ny, nz} with a 16-byte-multiple row pitch, and each CPML
+// axis's psi slab as a 4D tensor {.., .., .., 4 terms}.
 wf_status build_maps(wf_handle *h) {
   h->maps_ok = false;
-  auto enc = encode_fn();
-  if (!enc) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  if (!encode_fn()) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  if (!h->cfg_user_set) h->cfg = FusedConfig{4, 32, 3};
   unsigned eb[4], hb[4], mb[3];
   wf::fused_boxes(h->cfg.ty, eb, hb, mb);
   const cuuint64_t fdim[4] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz, 6};
   const cuuint64_t fstr[3] = {(cuuint64_t)h->nx * 4, (cuuint64_t)h->nx * h->ny * 4,
                               (cuuint64_t)h->N * 4};
-  const cuuint32_t ones[4] = {1, 1, 1, 1};
-  for (int b = 0; b < 2; ++b) {
-    const cuuint32_t ebox[4] = {eb[0], eb[1], eb[2], eb[3]};
-    const cuuint32_t hbox[4] = {hb[0], hb[1], hb[2], hb[3]};
-    CUresult r1 = enc(&h->tmE[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, ebox,
-                      ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    CUresult r2 = enc(&h->tmH[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, hbox,
-                      ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS)
-      return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(fields) failed");
-  }
   const cuuint64_t mdim[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz};
   const cuuint64_t mstr[2] = {(cuuint64_t)h->mat_pitch, (cuuint64_t)h->mat_pitch * h->ny};
+  const cuuint32_t ebox[4] = {eb[0], eb[1], eb[2], eb[3]};
+  const cuuint32_t hbox[4] = {hb[0], hb[1], hb[2], hb[3]};
   const cuuint32_t mbox[3] = {mb[0], mb[1], mb[2]};
-  CUresult r3 = enc(&h->tmM, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->mat, mdim, mstr, mbox, ones,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r3 != CUDA_SUCCESS) return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(ids) failed");
+  for (int b = 0; b < 2; ++b) {
+    wf::FusedMaps &m = h->maps[b];
+    std::memset(&m, 0, sizeof(m));
+    if (!encode(&m.e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, ebox) ||
+        !encode(&m.h, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, hbox) ||
+        !encode(&m.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->mat, mdim, mstr, mbox))
+      return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(fields/ids) failed");
+  }
   WF_CUDA(h, wf::fused_prepare(h->cfg));
   h->maps_ok = true;
   return WF_OK;
@@ -192,6 +198,7 @@ GridArgs grid_args(const wf_handle *h) {
     const AxisState &A = h->ax[a];
     g.pml[a].T = A.T;
     g.pml[a].W = A.W;
+    g.pml[a].pitch = A.pitch;
     g.pml[a].prof = A.prof;
     g.pml[a].psi_cur = A.psi[h->cur];
     g.pml[a].psi_nxt = A.psi[h->cur ^ 1];
@@ -200,8 +207,6 @@ GridArgs grid_args(const wf_handle *h) {
   g.err = h->d_err;
   return g;
 }
-
-bool has_pml(const wf_handle *h) { return h->ax[0].T > 0 || h->ax[1].T > 0 || h->ax[2].T > 0; }
 
 // One full step on h->stream: step kernel(s) cur -> nxt, then the tail.
 cudaEvent_t timing_event(wf_handle *h) {
@@ -233,7 +238,7 @@ wf_status enqueue_one(wf_handle *h) {
     a.tiles_y = (h->ny + h->cfg.ty - 1) / h->cfg.ty;
     a.zchunk = h->cfg.zchunk;
     a.has_pml = has_pml(h) ? 1 : 0;
-    e = wf::launch_fused(h->cfg, h->tmE[h->cur], h->tmH[h->cur], h->tmM, a, fma, h->stream);
+    e = wf::launch_fused(h->cfg, h->maps[h->cur], a, fma, h->stream);
   } else {
     e = wf::launch_split(g, fma, h->stream);
   }
@@ -461,10 +466,12 @@ wf_status wf_set_pml(wf_handle *h, int axis, int T, const float *b, const float 
   if (T == 0) return WF_OK;
   A.T = T;
   A.W = std::min(2 * T, n);
+  // x rows are padded to a multiple of 4 positions (16 bytes) for TMA
+  A.pitch = axis == 0 ? (A.W + 3) / 4 * 4 : A.W;
   const long long cross = axis == 0 ? static_cast<long long>(h->ny) * h->nz
                         : axis == 1 ? static_cast<long long>(h->nx) * h->nz
                                     : static_cast<long long>(h->nx) * h->ny;
-  A.cells = cross * A.W;
+  A.cells = cross * A.pitch;
   std::vector<float> prof(3 * A.W);
   for (int s = 0; s < A.W; ++s) {
     const int c = s < T ? s : s + (n - A.W);  // slab position -> axis coordinate
@@ -693,7 +700,7 @@ wf_status wf_get_psi(wf_handle *h, int which, float *out) {
         else if (c >= n - A.T) s = c - (n - A.W);
         if (s < 0) continue;
         long long idx;
-        if (axis == 0) idx = (static_cast<long long>(z) * h->ny + y) * A.W + s;
+        if (axis == 0) idx = (static_cast<long long>(z) * h->ny + y) * A.pitch + s;
         else if (axis == 1) idx = (static_cast<long long>(z) * A.W + s) * h->nx + x;
         else idx = (static_cast<long long>(s) * h->ny + y) * h->nx + x;
         out[(static_cast<long long>(z) * h->ny + y) * h->nx + x] = buf[idx];
@@ -753,6 +760,7 @@ wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t) {
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   drop_graphs(h);
   h->cfg = c;
+  h->cfg_user_set = true;
   h->maps_ok = false;
   return WF_OK;
 }
@@ -769,8 +777,9 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) 
   if (st != WF_OK) return st;
   const FusedConfig orig = h->cfg;
   const int orig_cur = h->cur;
+  h->cfg_user_set = true;  // trials and the result are explicit tilings
   std::vector<FusedConfig> cands;
-  const int tys[] = {4, 8, 12, 16};
+  const int tys[] = {4, 6, 8, 12, 16};
   const int stg[] = {2, 3, 4};
   const int zcs[] = {16, 32, 64, 128, 1 << 20};
   for (int ty : tys)

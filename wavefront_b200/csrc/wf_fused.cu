@@ -18,8 +18,13 @@
 //    the -z neighbour H(p-1) rides along in registers (register-rotated z);
 //  * the state is double-buffered: the kernel reads buffer `cur` and writes
 //    buffer `nxt`, so halo recomputation never races a neighbour's writes;
-//  * CPML psi is read/written only by CTAs whose tile or z chunk meets a
-//    graded slab; interior CTAs run a body with no CPML code at all.
+//  * CPML: interior CTAs run a body with no CPML code.  CTAs whose tile,
+//    halo or z chunk meets a graded slab treat each lane's 4 cells as one
+//    vector: the y and z slab flags are uniform per warp and per plane, the
+//    x slab flag per lane, psi moves as float4, and each phase's psi loads
+//    are issued before the work that precedes their use (the H terms before
+//    the stage wait, the E terms before the barrier) so their latency
+//    overlaps it.
 //
 // All per-cell arithmetic goes through wf_internal.cuh, so results are
 // bit-identical to the split kernels and to the reference.
@@ -52,131 +57,111 @@ struct Layout {
   static_assert(TY + 1 <= 32, "x-halo column is handled by one warp");
 };
 
-struct HIn {
-  float ex, ey, ez, ex_py, ez_py, ex_pz, ey_pz, ez_px, ey_px, hx, hy, hz;
-};
-
-// update_h_field[_pml] for one cell (src/fdtd.rs:194-345)
-template <bool FMA, bool PML>
-__device__ __forceinline__ void h_cell(const HIn &c, float da, float db, const GridArgs &g, int x,
-                                       int y, int p, bool pml_ok, bool write_psi, float &hxo,
-                                       float &hyo, float &hzo) {
-  float d_ez_dy = sub(c.ez_py, c.ez), d_ex_dy = sub(c.ex_py, c.ex);
-  float d_ey_dz = sub(c.ey_pz, c.ey), d_ex_dz = sub(c.ex_pz, c.ex);
-  float d_ez_dx = sub(c.ez_px, c.ez), d_ey_dx = sub(c.ey_px, c.ey);
-  if (PML && pml_ok) {
-    {
-      const PmlAxis &P = g.pml[0];
-      const int s = slab_pos(x, g.nx, P.T, P.W);
-      if (s >= 0) {
-        const long long idx = (static_cast<long long>(p) * g.ny + y) * P.W + s;
-        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
-        float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
-        d_ez_dx = pml_corr<FMA>(d_ez_dx, b, a, ik, p0);
-        d_ey_dx = pml_corr<FMA>(d_ey_dx, b, a, ik, p1);
-        if (write_psi) {
-          P.psi_nxt[idx] = p0;
-          P.psi_nxt[P.cells + idx] = p1;
-        }
-      }
-    }
-    {
-      const PmlAxis &P = g.pml[1];
-      const int s = slab_pos(y, g.ny, P.T, P.W);
-      if (s >= 0) {
-        const long long idx = (static_cast<long long>(p) * P.W + s) * g.nx + x;
-        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
-        float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
-        d_ez_dy = pml_corr<FMA>(d_ez_dy, b, a, ik, p0);
-        d_ex_dy = pml_corr<FMA>(d_ex_dy, b, a, ik, p1);
-        if (write_psi) {
-          P.psi_nxt[idx] = p0;
-          P.psi_nxt[P.cells + idx] = p1;
-        }
-      }
-    }
-    {
-      const PmlAxis &P = g.pml[2];
-      const int s = slab_pos(p, g.nz, P.T, P.W);
-      if (s >= 0) {
-        const long long idx = (static_cast<long long>(s) * g.ny + y) * g.nx + x;
-        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
-        float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
-        d_ey_dz = pml_corr<FMA>(d_ey_dz, b, a, ik, p0);
-        d_ex_dz = pml_corr<FMA>(d_ex_dz, b, a, ik, p1);
-        if (write_psi) {
-          P.psi_nxt[idx] = p0;
-          P.psi_nxt[P.cells + idx] = p1;
-        }
-      }
-    }
-  }
-  hxo = h_new<FMA>(da, c.hx, db, sub(d_ez_dy, d_ey_dz));
-  hyo = h_new<FMA>(da, c.hy, db, sub(d_ex_dz, d_ez_dx));
-  hzo = h_new<FMA>(da, c.hz, db, sub(d_ey_dx, d_ex_dy));
-}
-
-struct EIn {
-  float hx, hy, hz, hz_my, hx_my, hy_mz, hx_mz, hz_mx, hy_mx, ex, ey, ez;
-};
-
-// update_e_field[_pml] for one cell (src/fdtd.rs:369-509)
-template <bool FMA, bool PML>
-__device__ __forceinline__ void e_cell(const EIn &c, float ca, float cb, const GridArgs &g, int x,
-                                       int y, int p, bool pml_ok, float &exo, float &eyo,
-                                       float &ezo) {
-  float d_hz_dy = sub(c.hz, c.hz_my), d_hx_dy = sub(c.hx, c.hx_my);
-  float d_hy_dz = sub(c.hy, c.hy_mz), d_hx_dz = sub(c.hx, c.hx_mz);
-  float d_hz_dx = sub(c.hz, c.hz_mx), d_hy_dx = sub(c.hy, c.hy_mx);
-  if (PML && pml_ok) {
-    {
-      const PmlAxis &P = g.pml[0];
-      const int s = slab_pos(x, g.nx, P.T, P.W);
-      if (s >= 0) {
-        const long long idx = (static_cast<long long>(p) * g.ny + y) * P.W + s;
-        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
-        float p2 = __ldg(P.psi_cur + 2 * P.cells + idx), p3 = __ldg(P.psi_cur + 3 * P.cells + idx);
-        d_hz_dx = pml_corr<FMA>(d_hz_dx, b, a, ik, p2);
-        d_hy_dx = pml_corr<FMA>(d_hy_dx, b, a, ik, p3);
-        P.psi_nxt[2 * P.cells + idx] = p2;
-        P.psi_nxt[3 * P.cells + idx] = p3;
-      }
-    }
-    {
-      const PmlAxis &P = g.pml[1];
-      const int s = slab_pos(y, g.ny, P.T, P.W);
-      if (s >= 0) {
-        const long long idx = (static_cast<long long>(p) * P.W + s) * g.nx + x;
-        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
-        float p2 = __ldg(P.psi_cur + 2 * P.cells + idx), p3 = __ldg(P.psi_cur + 3 * P.cells + idx);
-        d_hz_dy = pml_corr<FMA>(d_hz_dy, b, a, ik, p2);
-        d_hx_dy = pml_corr<FMA>(d_hx_dy, b, a, ik, p3);
-        P.psi_nxt[2 * P.cells + idx] = p2;
-        P.psi_nxt[3 * P.cells + idx] = p3;
-      }
-    }
-    {
-      const PmlAxis &P = g.pml[2];
-      const int s = slab_pos(p, g.nz, P.T, P.W);
-      if (s >= 0) {
-        const long long idx = (static_cast<long long>(s) * g.ny + y) * g.nx + x;
-        const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
-        float p2 = __ldg(P.psi_cur + 2 * P.cells + idx), p3 = __ldg(P.psi_cur + 3 * P.cells + idx);
-        d_hy_dz = pml_corr<FMA>(d_hy_dz, b, a, ik, p2);
-        d_hx_dz = pml_corr<FMA>(d_hx_dz, b, a, ik, p3);
-        P.psi_nxt[2 * P.cells + idx] = p2;
-        P.psi_nxt[3 * P.cells + idx] = p3;
-      }
-    }
-  }
-  exo = e_new<FMA>(ca, c.ex, cb, sub(d_hz_dy, d_hy_dz));
-  eyo = e_new<FMA>(ca, c.ey, cb, sub(d_hx_dz, d_hz_dx));
-  ezo = e_new<FMA>(ca, c.ez, cb, sub(d_hy_dx, d_hx_dy));
-}
-
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void stg4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ float &el(float4 &v, int q) {
+  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
 __device__ __forceinline__ float comp(const float4 &v, int q) {
   return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+
+// CPML geometry of one lane's 4 cells at one plane.
+struct LanePml {
+  bool y, z;        // row in the y slab / plane in the z slab (warp / CTA uniform)
+  int xmode;        // 0: no cell in the x slab; 1: all 4, aligned (vector); 2: per cell
+  long long iy, iz, ix;  // psi index of the lane's first cell (y, z, x-vector)
+  int sy, sz, sx;        // slab positions (x: of the first cell)
+};
+
+__device__ __forceinline__ LanePml lane_pml(const GridArgs &g, int xg, int y, int p) {
+  LanePml L{};
+  const PmlAxis &X = g.pml[0], &Y = g.pml[1], &Z = g.pml[2];
+  L.sy = slab_pos(y, g.ny, Y.T, Y.W);
+  L.sz = slab_pos(p, g.nz, Z.T, Z.W);
+  L.y = L.sy >= 0;
+  L.z = L.sz >= 0;
+  if (L.y) L.iy = (static_cast<long long>(p) * Y.W + L.sy) * g.nx + xg;
+  if (L.z) L.iz = (static_cast<long long>(L.sz) * g.ny + y) * g.nx + xg;
+  L.xmode = 0;
+  if (X.T > 0) {
+    const int s0 = slab_pos(xg, g.nx, X.T, X.W), s3 = slab_pos(xg + 3, g.nx, X.T, X.W);
+    const int s1 = slab_pos(xg + 1, g.nx, X.T, X.W), s2 = slab_pos(xg + 2, g.nx, X.T, X.W);
+    if (s0 >= 0 && s3 == s0 + 3 && (s0 & 3) == 0) {
+      L.xmode = 1;
+      L.sx = s0;
+      L.ix = (static_cast<long long>(p) * g.ny + y) * X.pitch + s0;
+    } else if (s0 >= 0 || s1 >= 0 || s2 >= 0 || s3 >= 0) {
+      L.xmode = 2;
+    }
+  }
+  return L;
+}
+
+// The two psi terms of one axis for a lane's 4 cells (float4 each).
+struct Psi2 {
+  float4 p0, p1;
+};
+
+__device__ __forceinline__ Psi2 load_psi2(const PmlAxis &P, int comp0, long long idx) {
+  return Psi2{ldg4(P.psi_cur + comp0 * P.cells + idx), ldg4(P.psi_cur + (comp0 + 1) * P.cells + idx)};
+}
+
+// psi recursion of one axis over 4 cells with one coefficient set (y, z).
+template <bool FMA>
+__device__ __forceinline__ void corr4_uniform(float d0[4], float d1[4], Psi2 &q, float b, float a,
+                                              float ik) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    d0[i] = pml_corr<FMA>(d0[i], b, a, ik, el(q.p0, i));
+    d1[i] = pml_corr<FMA>(d1[i], b, a, ik, el(q.p1, i));
+  }
+}
+
+// x axis: per-cell coefficients at slab positions s0..s0+3.
+template <bool FMA>
+__device__ __forceinline__ void corr4_x(float d0[4], float d1[4], Psi2 &q, const PmlAxis &P, int s0) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float b = __ldg(P.prof + s0 + i), a = __ldg(P.prof + P.W + s0 + i),
+                ik = __ldg(P.prof + 2 * P.W + s0 + i);
+    d0[i] = pml_corr<FMA>(d0[i], b, a, ik, el(q.p0, i));
+    d1[i] = pml_corr<FMA>(d1[i], b, a, ik, el(q.p1, i));
+  }
+}
+
+// x axis, one cell at a time (lanes straddling a slab edge, the x-halo cell).
+template <bool FMA>
+__device__ __forceinline__ void corr_x_cell(const GridArgs &g, int comp0, int x, int y, int p,
+                                            float &d0, float &d1, bool store) {
+  const PmlAxis &P = g.pml[0];
+  const int s = slab_pos(x, g.nx, P.T, P.W);
+  if (s < 0) return;
+  const long long idx = (static_cast<long long>(p) * g.ny + y) * P.pitch + s;
+  float p0 = __ldg(P.psi_cur + comp0 * P.cells + idx), p1 = __ldg(P.psi_cur + (comp0 + 1) * P.cells + idx);
+  const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+  d0 = pml_corr<FMA>(d0, b, a, ik, p0);
+  d1 = pml_corr<FMA>(d1, b, a, ik, p1);
+  if (store) {
+    P.psi_nxt[comp0 * P.cells + idx] = p0;
+    P.psi_nxt[(comp0 + 1) * P.cells + idx] = p1;
+  }
+}
+
+// y or z axis, one cell (the x-halo cell).
+template <bool FMA>
+__device__ __forceinline__ void corr_yz_cell(const GridArgs &g, int axis, int x, int y, int p,
+                                             float &d0, float &d1) {
+  const PmlAxis &P = g.pml[axis];
+  const int s = axis == 1 ? slab_pos(y, g.ny, P.T, P.W) : slab_pos(p, g.nz, P.T, P.W);
+  if (s < 0) return;
+  const long long idx = axis == 1 ? (static_cast<long long>(p) * P.W + s) * g.nx + x
+                                  : (static_cast<long long>(s) * g.ny + y) * g.nx + x;
+  float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
+  const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+  d0 = pml_corr<FMA>(d0, b, a, ik, p0);
+  d1 = pml_corr<FMA>(d1, b, a, ik, p1);
 }
 
 template <int TY, int S, bool FMA, bool PML>
@@ -225,12 +210,25 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   const int xg = x0 + 4 * lane;
   const bool row_in = (y >= 0) && (y < ny);
   const bool x_in = xg < nx;  // nx % 8 == 0: a lane's 4 cells are all in or all out
+  const bool cell_ok = row_in && x_in;
   const int cE = 4 + 4 * lane;
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;  // H(p-1), own cells
 
   for (int j = 0; j < np - 1; ++j) {
     const int p = kfirst + j;
     const bool warm = p < k0;
+    const bool active = tile_warp || !warm;  // the halo warp idles on the warm-up plane
+
+    // CPML: this plane's H-term psi loads go out before the stage wait
+    LanePml lp{};
+    Psi2 qx{}, qy{}, qz{};
+    if (PML && active && cell_ok) {
+      lp = lane_pml(g, xg, y, p);
+      if (lp.y) qy = load_psi2(g.pml[1], 0, lp.iy);
+      if (lp.z) qz = load_psi2(g.pml[2], 0, lp.iz);
+      if (lp.xmode == 1) qx = load_psi2(g.pml[0], 0, lp.ix);
+    }
+
     const bool arrived = mbar_wait(smem_u32(&s_bar[(j + 1) % S]), ((j + 1) / S) & 1);
     if (arrived && done == j + 1) done = j + 2;
     ok = arrived && ok;
@@ -243,11 +241,12 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     float *pl_hz = pl, *pl_hx = pl + L::PROWS * kTileX;
     float *pl_hzh = pl + 2 * L::PROWS * kTileX, *pl_hyh = pl_hzh + 32;
 
-    // ---------------- H phase ----------------
+    // ---------------- H phase (update_h_field[_pml], src/fdtd.rs:194-345) ----
     float ha[4], hb[4], hc[4];  // new hx, hy, hz of this lane's 4 cells
     float4 ex4, ey4, ez4;
     uchar4 m4;
-    if (tile_warp || !warm) {
+    Psi2 ex_{}, ey_{}, ez_{};  // E-term psi (x, y, z axes), loaded before the barrier
+    if (active) {
       auto E4 = [&](const float *B, int c, int row) { return lds4(B + (c * L::EH + row) * L::EW + cE); };
       ex4 = E4(Ec, 0, r);
       ey4 = E4(Ec, 1, r);
@@ -264,33 +263,74 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       const float4 hy4 = lds4(Hc + (1 * L::HH + r) * L::HW + cE);
       const float4 hz4 = lds4(Hc + (2 * L::HH + r) * L::HW + cE);
       m4 = *reinterpret_cast<const uchar4 *>(Mc + r * L::MW + 16 + 4 * lane);
-      const bool cell_ok = row_in && x_in;
-      const bool wpsi = tile_warp && !warm && cell_ok;
+
+      float d_ez_dy[4], d_ex_dy[4], d_ey_dz[4], d_ex_dz[4], d_ez_dx[4], d_ey_dx[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        HIn c;
-        c.ex = comp(ex4, q); c.ey = comp(ey4, q); c.ez = comp(ez4, q);
-        c.ex_py = comp(ex_py, q); c.ez_py = comp(ez_py, q);
-        c.ex_pz = comp(ex_pz, q); c.ey_pz = comp(ey_pz, q);
-        c.ez_px = q < 3 ? comp(ez4, q + 1) : ez_n;
-        c.ey_px = q < 3 ? comp(ey4, q + 1) : ey_n;
-        c.hx = comp(hx4, q); c.hy = comp(hy4, q); c.hz = comp(hz4, q);
+        d_ez_dy[q] = sub(comp(ez_py, q), comp(ez4, q));
+        d_ex_dy[q] = sub(comp(ex_py, q), comp(ex4, q));
+        d_ey_dz[q] = sub(comp(ey_pz, q), comp(ey4, q));
+        d_ex_dz[q] = sub(comp(ex_pz, q), comp(ex4, q));
+        d_ez_dx[q] = sub(q < 3 ? comp(ez4, q + 1) : ez_n, comp(ez4, q));
+        d_ey_dx[q] = sub(q < 3 ? comp(ey4, q + 1) : ey_n, comp(ey4, q));
+      }
+      if (PML && cell_ok) {  // CPML on the H terms (pml_correct_*, src/fdtd.rs:136-163)
+        const bool wpsi = tile_warp && !warm;
+        if (lp.xmode == 1) {
+          corr4_x<FMA>(d_ez_dx, d_ey_dx, qx, g.pml[0], lp.sx);
+          if (wpsi) {
+            const PmlAxis &P = g.pml[0];
+            stg4(P.psi_nxt + lp.ix, qx.p0);
+            stg4(P.psi_nxt + P.cells + lp.ix, qx.p1);
+          }
+        } else if (lp.xmode == 2) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) corr_x_cell<FMA>(g, 0, xg + q, y, p, d_ez_dx[q], d_ey_dx[q], wpsi);
+        }
+        if (lp.y) {
+          const PmlAxis &P = g.pml[1];
+          corr4_uniform<FMA>(d_ez_dy, d_ex_dy, qy, __ldg(P.prof + lp.sy), __ldg(P.prof + P.W + lp.sy),
+                             __ldg(P.prof + 2 * P.W + lp.sy));
+          if (wpsi) {
+            stg4(P.psi_nxt + lp.iy, qy.p0);
+            stg4(P.psi_nxt + P.cells + lp.iy, qy.p1);
+          }
+        }
+        if (lp.z) {
+          const PmlAxis &P = g.pml[2];
+          corr4_uniform<FMA>(d_ey_dz, d_ex_dz, qz, __ldg(P.prof + lp.sz), __ldg(P.prof + P.W + lp.sz),
+                             __ldg(P.prof + 2 * P.W + lp.sz));
+          if (wpsi) {
+            stg4(P.psi_nxt + lp.iz, qz.p0);
+            stg4(P.psi_nxt + P.cells + lp.iz, qz.p1);
+          }
+        }
+        if (wpsi) {  // the E terms' psi: in flight across the barrier
+          if (lp.xmode == 1) ex_ = load_psi2(g.pml[0], 2, lp.ix);
+          if (lp.y) ey_ = load_psi2(g.pml[1], 2, lp.iy);
+          if (lp.z) ez_ = load_psi2(g.pml[2], 2, lp.iz);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
         const unsigned char id = q == 0 ? m4.x : (q == 1 ? m4.y : (q == 2 ? m4.z : m4.w));
         const float4 cf = s_coef[id];
-        h_cell<FMA, PML>(c, cf.z, cf.w, g, xg + q, y, p, cell_ok, wpsi, ha[q], hb[q], hc[q]);
+        ha[q] = h_new<FMA>(cf.z, comp(hx4, q), cf.w, sub(d_ez_dy[q], d_ey_dz[q]));
+        hb[q] = h_new<FMA>(cf.z, comp(hy4, q), cf.w, sub(d_ex_dz[q], d_ez_dx[q]));
+        hc[q] = h_new<FMA>(cf.z, comp(hz4, q), cf.w, sub(d_ey_dx[q], d_ex_dy[q]));
       }
       if (!row_in) {  // outside the domain in y: zero field (OUTER_ZERO_BLOCK)
 #pragma unroll
         for (int q = 0; q < 4; ++q) ha[q] = hb[q] = hc[q] = 0.0f;
       }
       if (!warm) {
-        *reinterpret_cast<float4 *>(pl_hz + r * kTileX + 4 * lane) = make_float4(hc[0], hc[1], hc[2], hc[3]);
-        *reinterpret_cast<float4 *>(pl_hx + r * kTileX + 4 * lane) = make_float4(ha[0], ha[1], ha[2], ha[3]);
+        stg4(pl_hz + r * kTileX + 4 * lane, make_float4(hc[0], hc[1], hc[2], hc[3]));
+        stg4(pl_hx + r * kTileX + 4 * lane, make_float4(ha[0], ha[1], ha[2], ha[3]));
         if (tile_warp && cell_ok) {
           float *Hn = g.nxt + 3 * N + (static_cast<long long>(p) * ny + y) * nx + xg;
-          *reinterpret_cast<float4 *>(Hn) = make_float4(ha[0], ha[1], ha[2], ha[3]);
-          *reinterpret_cast<float4 *>(Hn + N) = make_float4(hb[0], hb[1], hb[2], hb[3]);
-          *reinterpret_cast<float4 *>(Hn + 2 * N) = make_float4(hc[0], hc[1], hc[2], hc[3]);
+          stg4(Hn, make_float4(ha[0], ha[1], ha[2], ha[3]));
+          stg4(Hn + N, make_float4(hb[0], hb[1], hb[2], hb[3]));
+          stg4(Hn + 2 * N, make_float4(hc[0], hc[1], hc[2], hc[3]));
         }
       }
       // -x halo column (x0-1, y0..y0+TY-1): Hz and Hy for the E update at x0
@@ -298,22 +338,23 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         const int rh = lane + 1, yh = y0 + lane, xh = x0 - 1;
         float hzv = 0.0f, hyv = 0.0f;
         if (x0 > 0 && yh < ny) {
-          HIn c;
-          c.ex = Ec[(0 * L::EH + rh) * L::EW + 3];
-          c.ey = Ec[(1 * L::EH + rh) * L::EW + 3];
-          c.ez = Ec[(2 * L::EH + rh) * L::EW + 3];
-          c.ex_py = Ec[(0 * L::EH + rh + 1) * L::EW + 3];
-          c.ez_py = Ec[(2 * L::EH + rh + 1) * L::EW + 3];
-          c.ex_pz = En[(0 * L::EH + rh) * L::EW + 3];
-          c.ey_pz = En[(1 * L::EH + rh) * L::EW + 3];
-          c.ez_px = Ec[(2 * L::EH + rh) * L::EW + 4];
-          c.ey_px = Ec[(1 * L::EH + rh) * L::EW + 4];
-          c.hx = Hc[(0 * L::HH + rh) * L::HW + 3];
-          c.hy = Hc[(1 * L::HH + rh) * L::HW + 3];
-          c.hz = Hc[(2 * L::HH + rh) * L::HW + 3];
+          const float ex = Ec[(0 * L::EH + rh) * L::EW + 3];
+          const float ey = Ec[(1 * L::EH + rh) * L::EW + 3];
+          const float ez = Ec[(2 * L::EH + rh) * L::EW + 3];
+          float d_ez_dx1 = sub(Ec[(2 * L::EH + rh) * L::EW + 4], ez);
+          float d_ey_dx1 = sub(Ec[(1 * L::EH + rh) * L::EW + 4], ey);
+          float d_ex_dz1 = sub(En[(0 * L::EH + rh) * L::EW + 3], ex);
+          float d_ey_dz1 = sub(En[(1 * L::EH + rh) * L::EW + 3], ey);
+          float d_ex_dy1 = sub(Ec[(0 * L::EH + rh + 1) * L::EW + 3], ex);
+          float d_ez_dy1 = sub(Ec[(2 * L::EH + rh + 1) * L::EW + 3], ez);
+          if (PML) {
+            corr_x_cell<FMA>(g, 0, xh, yh, p, d_ez_dx1, d_ey_dx1, false);
+            corr_yz_cell<FMA>(g, 1, xh, yh, p, d_ez_dy1, d_ex_dy1);
+            corr_yz_cell<FMA>(g, 2, xh, yh, p, d_ey_dz1, d_ex_dz1);
+          }
           const float4 cf = s_coef[Mc[rh * L::MW + 15]];
-          float hxv;
-          h_cell<FMA, PML>(c, cf.z, cf.w, g, xh, yh, p, true, false, hxv, hyv, hzv);
+          hyv = h_new<FMA>(cf.z, Hc[(1 * L::HH + rh) * L::HW + 3], cf.w, sub(d_ex_dz1, d_ez_dx1));
+          hzv = h_new<FMA>(cf.z, Hc[(2 * L::HH + rh) * L::HW + 3], cf.w, sub(d_ey_dx1, d_ex_dy1));
         }
         pl_hzh[rh] = hzv;
         pl_hyh[rh] = hyv;
@@ -328,7 +369,7 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       ++issued;
     }
 
-    // ---------------- E phase ----------------
+    // ---------------- E phase (update_e_field[_pml], src/fdtd.rs:369-509) ----
     if (tile_warp) {
       if (!warm) {
         const float4 hz_my = lds4(pl_hz + (r - 1) * kTileX + 4 * lane);
@@ -339,26 +380,55 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
           hz_w = pl_hzh[r];
           hy_w = pl_hyh[r];
         }
-        const bool cell_ok = row_in && x_in;
-        float eo[3][4];
+        float d_hz_dy[4], d_hx_dy[4], d_hy_dz[4], d_hx_dz[4], d_hz_dx[4], d_hy_dx[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          EIn c;
-          c.hx = ha[q]; c.hy = hb[q]; c.hz = hc[q];
-          c.hz_my = comp(hz_my, q); c.hx_my = comp(hx_my, q);
-          c.hy_mz = comp(hyp, q); c.hx_mz = comp(hxp, q);
-          c.hz_mx = q == 0 ? hz_w : hc[q - 1];
-          c.hy_mx = q == 0 ? hy_w : hb[q - 1];
-          c.ex = comp(ex4, q); c.ey = comp(ey4, q); c.ez = comp(ez4, q);
-          const unsigned char id = q == 0 ? m4.x : (q == 1 ? m4.y : (q == 2 ? m4.z : m4.w));
-          const float4 cf = s_coef[id];
-          e_cell<FMA, PML>(c, cf.x, cf.y, g, xg + q, y, p, cell_ok, eo[0][q], eo[1][q], eo[2][q]);
+          d_hz_dy[q] = sub(hc[q], comp(hz_my, q));
+          d_hx_dy[q] = sub(ha[q], comp(hx_my, q));
+          d_hy_dz[q] = sub(hb[q], comp(hyp, q));
+          d_hx_dz[q] = sub(ha[q], comp(hxp, q));
+          d_hz_dx[q] = sub(hc[q], q == 0 ? hz_w : hc[q - 1]);
+          d_hy_dx[q] = sub(hb[q], q == 0 ? hy_w : hb[q - 1]);
+        }
+        if (PML && cell_ok) {
+          if (lp.xmode == 1) {
+            const PmlAxis &P = g.pml[0];
+            corr4_x<FMA>(d_hz_dx, d_hy_dx, ex_, P, lp.sx);
+            stg4(P.psi_nxt + 2 * P.cells + lp.ix, ex_.p0);
+            stg4(P.psi_nxt + 3 * P.cells + lp.ix, ex_.p1);
+          } else if (lp.xmode == 2) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) corr_x_cell<FMA>(g, 2, xg + q, y, p, d_hz_dx[q], d_hy_dx[q], true);
+          }
+          if (lp.y) {
+            const PmlAxis &P = g.pml[1];
+            corr4_uniform<FMA>(d_hz_dy, d_hx_dy, ey_, __ldg(P.prof + lp.sy), __ldg(P.prof + P.W + lp.sy),
+                               __ldg(P.prof + 2 * P.W + lp.sy));
+            stg4(P.psi_nxt + 2 * P.cells + lp.iy, ey_.p0);
+            stg4(P.psi_nxt + 3 * P.cells + lp.iy, ey_.p1);
+          }
+          if (lp.z) {
+            const PmlAxis &P = g.pml[2];
+            corr4_uniform<FMA>(d_hy_dz, d_hx_dz, ez_, __ldg(P.prof + lp.sz), __ldg(P.prof + P.W + lp.sz),
+                               __ldg(P.prof + 2 * P.W + lp.sz));
+            stg4(P.psi_nxt + 2 * P.cells + lp.iz, ez_.p0);
+            stg4(P.psi_nxt + 3 * P.cells + lp.iz, ez_.p1);
+          }
         }
         if (cell_ok) {
+          float eo[3][4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const unsigned char id = q == 0 ? m4.x : (q == 1 ? m4.y : (q == 2 ? m4.z : m4.w));
+            const float4 cf = s_coef[id];
+            eo[0][q] = e_new<FMA>(cf.x, comp(ex4, q), cf.y, sub(d_hz_dy[q], d_hy_dz[q]));
+            eo[1][q] = e_new<FMA>(cf.x, comp(ey4, q), cf.y, sub(d_hx_dz[q], d_hz_dx[q]));
+            eo[2][q] = e_new<FMA>(cf.x, comp(ez4, q), cf.y, sub(d_hy_dx[q], d_hx_dy[q]));
+          }
           float *Ep = g.nxt + (static_cast<long long>(p) * ny + y) * nx + xg;
-          *reinterpret_cast<float4 *>(Ep) = make_float4(eo[0][0], eo[0][1], eo[0][2], eo[0][3]);
-          *reinterpret_cast<float4 *>(Ep + N) = make_float4(eo[1][0], eo[1][1], eo[1][2], eo[1][3]);
-          *reinterpret_cast<float4 *>(Ep + 2 * N) = make_float4(eo[2][0], eo[2][1], eo[2][2], eo[2][3]);
+          stg4(Ep, make_float4(eo[0][0], eo[0][1], eo[0][2], eo[0][3]));
+          stg4(Ep + N, make_float4(eo[1][0], eo[1][1], eo[1][2], eo[1][3]));
+          stg4(Ep + 2 * N, make_float4(eo[2][0], eo[2][1], eo[2][2], eo[2][3]));
         }
       }
       hxp = make_float4(ha[0], ha[1], ha[2], ha[3]);
@@ -429,12 +499,11 @@ cudaError_t prepare_t() {
 }
 
 template <int TY, int S, bool FMA>
-cudaError_t launch_t(const CUtensorMap &tmE, const CUtensorMap &tmH, const CUtensorMap &tmM,
-                     const FusedArgs &a, cudaStream_t s) {
+cudaError_t launch_t(const FusedMaps &m, const FusedArgs &a, cudaStream_t s) {
   using L = Layout<TY, S>;
   const long long nz_chunks = (a.g.nz + a.zchunk - 1) / a.zchunk;
   const long long items = static_cast<long long>(a.tiles_x) * a.tiles_y * nz_chunks;
-  k_fused<TY, S, FMA><<<static_cast<unsigned>(items), L::THREADS, L::BYTES, s>>>(tmE, tmH, tmM, a);
+  k_fused<TY, S, FMA><<<static_cast<unsigned>(items), L::THREADS, L::BYTES, s>>>(m.e, m.h, m.m, a);
   return cudaGetLastError();
 }
 
@@ -446,8 +515,9 @@ void fused_boxes(int ty, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]
   m_box[0] = kTileX + 16; m_box[1] = ty + 1; m_box[2] = 1;
 }
 
+// (tile rows, stages) combinations that are instantiated
 #define WF_FUSED_CONFIGS(X) \
-  X(4, 3) X(4, 4) X(8, 3) X(8, 4) X(12, 3) X(16, 2) X(16, 3)
+  X(4, 3) X(4, 4) X(6, 3) X(8, 3) X(8, 4) X(12, 3) X(16, 2) X(16, 3)
 
 bool fused_supported(const FusedConfig &c) {
 #define X(T, S_) if (c.ty == T && c.stages == S_) return c.zchunk >= 1;
@@ -470,12 +540,11 @@ cudaError_t fused_prepare(const FusedConfig &c) {
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_fused(const FusedConfig &c, const CUtensorMap &tmE, const CUtensorMap &tmH,
-                         const CUtensorMap &tmM, const FusedArgs &a, bool fma, cudaStream_t s) {
+cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a, bool fma,
+                         cudaStream_t s) {
 #define X(T, S_)                                                         \
   if (c.ty == T && c.stages == S_)                                      \
-    return fma ? launch_t<T, S_, true>(tmE, tmH, tmM, a, s)             \
-               : launch_t<T, S_, false>(tmE, tmH, tmM, a, s);
+    return fma ? launch_t<T, S_, true>(m, a, s) : launch_t<T, S_, false>(m, a, s);
   WF_FUSED_CONFIGS(X)
 #undef X
   return cudaErrorInvalidValue;

@@ -28,6 +28,8 @@ enum : int { kErrTimeout = 1, kErrBounds = 2 };
 struct PmlAxis {
   int T;                 // graded thickness in voxels (0: no CPML on axis)
   int W;                 // slab width
+  int pitch;             // x axis: row pitch of the slab array (W rounded up to 4,
+                         // so each row starts 16-byte aligned for TMA); y, z: W
   const float *prof;     // [3][W]: b, a, 1/kappa at slab positions
   const float *psi_cur;  // [4][cells]: H term 0, H term 1, E term 0, E term 1
   float *psi_nxt;

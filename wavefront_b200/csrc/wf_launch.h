@@ -24,10 +24,15 @@ struct FusedArgs {
   int has_pml;
 };
 
-// Tiling of the fused kernel: TY rows per CTA (x width kTileX), z chunk, and
+// Tiling of the fused kernel: TY rows per CTA (x width kTileX), z chunk and
 // pipeline depth.  Only the instantiated combinations are accepted.
 struct FusedConfig {
   int ty, zchunk, stages;
+};
+
+// TMA descriptors of one launch: E box, H box, ids box.
+struct FusedMaps {
+  CUtensorMap e, h, m;
 };
 
 cudaError_t launch_split(const GridArgs &g, bool fma, cudaStream_t s);
@@ -43,7 +48,7 @@ bool fused_supported(const FusedConfig &c);
 int fused_smem_bytes(const FusedConfig &c);
 // Sets the kernels' dynamic shared-memory limit (call outside graph capture).
 cudaError_t fused_prepare(const FusedConfig &c);
-cudaError_t launch_fused(const FusedConfig &c, const CUtensorMap &tmE, const CUtensorMap &tmH,
-                         const CUtensorMap &tmM, const FusedArgs &a, bool fma, cudaStream_t s);
+cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a, bool fma,
+                         cudaStream_t s);
 
 }  // namespace wf

@@ -28,7 +28,7 @@ __device__ __forceinline__ bool pml_slot(const PmlAxis &P, int axis, int x, int 
   const int c = axis == 0 ? x : (axis == 1 ? y : z);
   const int s = slab_pos(c, n, P.T, P.W);
   if (s < 0) return false;
-  if (axis == 0) idx = (static_cast<long long>(z) * ny + y) * P.W + s;
+  if (axis == 0) idx = (static_cast<long long>(z) * ny + y) * P.pitch + s;
   else if (axis == 1) idx = (static_cast<long long>(z) * P.W + s) * nx + x;
   else idx = (static_cast<long long>(s) * ny + y) * nx + x;
   b = P.prof[s];

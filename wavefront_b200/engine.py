@@ -136,6 +136,7 @@ class DeviceFieldGrid:
 
     # -- tiling -------------------------------------------------------------
     def tiling(self):
+        """(tile_rows, z_chunk, stages) of the fused kernel."""
         t = _L.Tiling()
         self._chk(_L.lib().wf_get_tiling(self._h, C.byref(t)))
         return t.tile_rows, t.z_chunk, t.stages
