@@ -75,8 +75,8 @@ def test_plain_cube_64_bit_exact(cube64, kernel):
         g.close()
 
 
-@pytest.mark.parametrize("tiling", [(4, 16, 3), (8, 64, 4), (12, 7, 3), (16, 1000, 2),
-                                    (16, 5, 3), (4, 32, 4), (6, 7, 3), (6, 1000, 3)])
+@pytest.mark.parametrize("tiling", [(4, 16, 3), (8, 64, 4), (8, 7, 3), (16, 1000, 3),
+                                    (16, 5, 3), (4, 32, 4), (4, 1000, 3), (8, 1, 4)])
 def test_fused_tilings_bit_identical(cube64, tiling):
     """Tiling is a scheduling detail (the GPU analogue of the reference's 1-slab
     vs 4-slab test, src/engine.rs:1008-1099): every tiling gives the oracle's bits."""
@@ -162,8 +162,8 @@ def test_ragged_grid_materials_h_probes_and_late_start(oracle):
     sc = configs.Scenario("ragged", dims, dx, dt, grid, table, pml, srcs, prbs, 200)
     sim = oracle.sim_from_scenario(sc)
     sim.step(sc.steps, NT)
-    for kernel, tiling in (("fused", (8, 64, 3)), ("fused", (12, 10, 3)),
-                           ("fused", (4, 10, 4)), ("fused", (6, 24, 3)), ("split", None)):
+    for kernel, tiling in (("fused", (8, 64, 3)), ("fused", (16, 10, 3)),
+                           ("fused", (4, 10, 4)), ("fused", (8, 24, 4)), ("split", None)):
         g = configs.device_grid(sc, kernel=kernel)
         try:
             if tiling:

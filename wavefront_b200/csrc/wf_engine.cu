@@ -70,9 +70,15 @@ struct wf_handle {
   long long *d_step = nullptr;
   int *d_err = nullptr;
   long long steps_done = 0;
-  FusedConfig cfg{4, 32, 3};
+  FusedConfig cfg{4, 12, 3};
   bool cfg_user_set = false;  // otherwise chosen from the grid at first use
   wf::FusedMaps maps[2];      // per state buffer (the one read by the step)
+  int *d_items = nullptr;     // work items grouped by kernel class
+  int class_off[5] = {0, 0, 0, 0, 0}, class_n[5] = {0, 0, 0, 0, 0};
+  // the class launches of one step run concurrently: forked from the main
+  // stream onto these streams and joined back before the step tail
+  cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr, join_ev[4] = {nullptr, nullptr, nullptr, nullptr};
   bool maps_ok = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_steps = 0;
@@ -138,10 +144,15 @@ bool fused_allowed(const wf_handle *h) {
 
 bool use_fused(const wf_handle *h) {
   if (h->kernel_pref == WF_KERNEL_SPLIT) return false;
+  // the fused kernel stages CPML profiles of up to 64 slab positions per axis
+  // in shared memory; thicker layers take the split kernels
+  for (const AxisState &A : h->ax)
+    if (A.T > 0 && A.W > 64) return false;
   return fused_allowed(h) && encode_fn() != nullptr;
 }
 
 bool has_pml(const wf_handle *h) { return h->ax[0].T > 0 || h->ax[1].T > 0 || h->ax[2].T > 0; }
+FusedArgs fused_args(const wf_handle *h);
 
 // One tiled TMA descriptor (no swizzle, no interleave, zero out-of-bounds fill).
 bool encode(CUtensorMap *m, CUtensorMapDataType t, int rank, void *base, const cuuint64_t *dims,
@@ -158,7 +169,7 @@ bool encode(CUtensorMap *m, CUtensorMapDataType t, int rank, void *base, const c
 wf_status build_maps(wf_handle *h) {
   h->maps_ok = false;
   if (!encode_fn()) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
-  if (!h->cfg_user_set) h->cfg = FusedConfig{4, 32, 3};
+  if (!h->cfg_user_set) h->cfg = FusedConfig{4, 12, 3};  // best measured at 512^3 on B200
   unsigned eb[4], hb[4], mb[3];
   wf::fused_boxes(h->cfg.ty, eb, hb, mb);
   const cuuint64_t fdim[4] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz, 6};
@@ -178,6 +189,26 @@ wf_status build_maps(wf_handle *h) {
       return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(fields/ids) failed");
   }
   WF_CUDA(h, wf::fused_prepare(h->cfg));
+  // Work lists, one per kernel class (interior first): each class runs the
+  // kernel instantiation that carries only the CPML code it needs.
+  const FusedArgs a = fused_args(h);
+  const int n_items = a.tiles_x * a.tiles_y * ((h->nz + a.zchunk - 1) / a.zchunk);
+  std::vector<int> lists[5];
+  for (int i = 0; i < n_items; ++i) {
+    const int c = wf::fused_item_class(a, h->cfg.ty, i);
+    for (int k = 0; k < 5; ++k)
+      if (wf::kFusedClasses[k] == c) lists[k].push_back(i);
+  }
+  std::vector<int> all;
+  for (int k = 0; k < 5; ++k) {
+    h->class_off[k] = static_cast<int>(all.size());
+    h->class_n[k] = static_cast<int>(lists[k].size());
+    all.insert(all.end(), lists[k].begin(), lists[k].end());
+  }
+  cudaFree(h->d_items);
+  h->d_items = nullptr;
+  WF_CUDA(h, cudaMalloc(&h->d_items, sizeof(int) * std::max<size_t>(all.size(), 1)));
+  WF_CUDA(h, cudaMemcpy(h->d_items, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
   h->maps_ok = true;
   return WF_OK;
 }
@@ -208,6 +239,17 @@ GridArgs grid_args(const wf_handle *h) {
   return g;
 }
 
+FusedArgs fused_args(const wf_handle *h) {
+  FusedArgs a{};
+  a.g = grid_args(h);
+  a.tiles_x = (h->nx + wf::kTileX - 1) / wf::kTileX;
+  a.tiles_y = (h->ny + h->cfg.ty - 1) / h->cfg.ty;
+  a.zchunk = h->cfg.zchunk;
+  a.has_pml = has_pml(h) ? 1 : 0;
+  a.prof_in_smem = (h->ax[0].W <= 64 && h->ax[1].W <= 64 && h->ax[2].W <= 64) ? 1 : 0;
+  return a;
+}
+
 // One full step on h->stream: step kernel(s) cur -> nxt, then the tail.
 cudaEvent_t timing_event(wf_handle *h) {
   if (h->ev_used == h->ev_pool.size()) {
@@ -232,13 +274,22 @@ wf_status enqueue_one(wf_handle *h) {
       wf_status s = build_maps(h);
       if (s != WF_OK) return s;
     }
-    FusedArgs a{};
-    a.g = g;
-    a.tiles_x = (h->nx + wf::kTileX - 1) / wf::kTileX;
-    a.tiles_y = (h->ny + h->cfg.ty - 1) / h->cfg.ty;
-    a.zchunk = h->cfg.zchunk;
-    a.has_pml = has_pml(h) ? 1 : 0;
-    e = wf::launch_fused(h->cfg, h->maps[h->cur], a, fma, h->stream);
+    const FusedArgs a = fused_args(h);
+    // class 0 (interior) on the main stream, the CPML classes on side
+    // streams forked from it; they touch disjoint cells of the next state
+    WF_CUDA(h, cudaEventRecord(h->fork_ev, h->stream));
+    e = cudaSuccess;
+    for (int k = 0; k < 5 && e == cudaSuccess; ++k) {
+      if (h->class_n[k] == 0) continue;
+      cudaStream_t s = k == 0 ? h->stream : h->side[k - 1];
+      if (k > 0) WF_CUDA(h, cudaStreamWaitEvent(s, h->fork_ev, 0));
+      e = wf::launch_fused(h->cfg, h->maps[h->cur], a, h->d_items + h->class_off[k],
+                           h->class_n[k], wf::kFusedClasses[k], fma, s);
+      if (e == cudaSuccess && k > 0) {
+        WF_CUDA(h, cudaEventRecord(h->join_ev[k - 1], s));
+        WF_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_ev[k - 1], 0));
+      }
+    }
   } else {
     e = wf::launch_split(g, fma, h->stream);
   }
@@ -382,6 +433,13 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaStreamCreate"));
     h->own_stream = true;
   }
+  for (int k = 0; k < 4; ++k) {
+    if ((e = cudaStreamCreateWithFlags(&h->side[k], cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->join_ev[k], cudaEventDisableTiming)) != cudaSuccess)
+      return cleanup_fail(cuda_fail(nullptr, e, "side stream setup"));
+  }
+  if ((e = cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming)) != cudaSuccess)
+    return cleanup_fail(cuda_fail(nullptr, e, "cudaEventCreate"));
   for (int b = 0; b < 2; ++b) {
     e = cudaMalloc(&h->fld[b], sizeof(float) * 6 * h->N);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(fields)"));
@@ -410,6 +468,14 @@ wf_status wf_destroy(wf_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   for (auto ev : h->ev_pool) cudaEventDestroy(ev);
+  for (int k = 0; k < 4; ++k) {
+    if (h->side[k]) {
+      cudaStreamSynchronize(h->side[k]);
+      cudaStreamDestroy(h->side[k]);
+    }
+    if (h->join_ev[k]) cudaEventDestroy(h->join_ev[k]);
+  }
+  if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   for (auto &f : h->fld) cudaFree(f);
   cudaFree(h->mat);
   cudaFree(h->coef);
@@ -417,6 +483,7 @@ wf_status wf_destroy(wf_handle *h) {
   cudaFree(h->d_err);
   cudaFree(h->d_src);
   cudaFree(h->d_probe);
+  cudaFree(h->d_items);
   for (auto &a : h->ax) {
     cudaFree(a.prof);
     cudaFree(a.psi[0]);
@@ -458,6 +525,7 @@ wf_status wf_set_pml(wf_handle *h, int axis, int T, const float *b, const float 
   DeviceGuard guard(h->dev);
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   drop_graphs(h);
+  h->maps_ok = false;  // the work lists depend on the CPML slabs
   AxisState &A = h->ax[axis];
   cudaFree(A.prof);
   cudaFree(A.psi[0]);
@@ -779,8 +847,8 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) 
   const int orig_cur = h->cur;
   h->cfg_user_set = true;  // trials and the result are explicit tilings
   std::vector<FusedConfig> cands;
-  const int tys[] = {4, 6, 8, 12, 16};
-  const int stg[] = {2, 3, 4};
+  const int tys[] = {4, 8, 16};
+  const int stg[] = {3, 4};
   const int zcs[] = {16, 32, 64, 128, 1 << 20};
   for (int ty : tys)
     for (int s : stg)

@@ -28,12 +28,16 @@
 //
 // All per-cell arithmetic goes through wf_internal.cuh, so results are
 // bit-identical to the split kernels and to the reference.
+#include <algorithm>
+
 #include "wf_internal.cuh"
 #include "wf_launch.h"
 
 namespace wf {
 
 namespace {
+
+constexpr int kProfSmem = 3 * 3 * 64;  // floats: 3 axes x {b, a, 1/kappa} x 64 positions
 
 template <int TY, int S>
 struct Layout {
@@ -51,7 +55,8 @@ struct Layout {
   static constexpr int PROWS = TY + 1;    // plane rows: 0 = y0-1, 1..TY = tile rows
   static constexpr int PLANE_FLOATS = 2 * PROWS * kTileX + 64;  // hz, hx rows; x-halo hz, hy
   static constexpr int PLANE_OFF = STAGE_OFF + S * STAGE;
-  static constexpr int BAR_OFF = PLANE_OFF + 2 * PLANE_FLOATS * 4;
+  static constexpr int PROF_OFF = PLANE_OFF + 2 * PLANE_FLOATS * 4;  // CPML profiles
+  static constexpr int BAR_OFF = PROF_OFF + kProfSmem * 4;
   static constexpr int BYTES = BAR_OFF + S * 8 + 128;  // +128: base alignment slack
   static constexpr int THREADS = 32 * (TY + 1);
   static_assert(TY + 1 <= 32, "x-halo column is handled by one warp");
@@ -75,26 +80,51 @@ struct LanePml {
   int sy, sz, sx;        // slab positions (x: of the first cell)
 };
 
-__device__ __forceinline__ LanePml lane_pml(const GridArgs &g, int xg, int y, int p) {
-  LanePml L{};
-  const PmlAxis &X = g.pml[0], &Y = g.pml[1], &Z = g.pml[2];
-  L.sy = slab_pos(y, g.ny, Y.T, Y.W);
-  L.sz = slab_pos(p, g.nz, Z.T, Z.W);
-  L.y = L.sy >= 0;
-  L.z = L.sz >= 0;
-  if (L.y) L.iy = (static_cast<long long>(p) * Y.W + L.sy) * g.nx + xg;
-  if (L.z) L.iz = (static_cast<long long>(L.sz) * g.ny + y) * g.nx + xg;
-  L.xmode = 0;
-  if (X.T > 0) {
+// The plane-independent part of a lane's CPML geometry (computed once per
+// CTA): its x-slab mode and position, and its row's y-slab position.
+struct LaneConst {
+  int xmode, sx, sy;
+};
+
+// AX: bit mask of the CPML axes (1 x, 2 y, 4 z) the calling kernel handles.
+template <int AX>
+__device__ __forceinline__ LaneConst lane_const(const GridArgs &g, int xg, int y, bool cell_ok) {
+  LaneConst c{0, -1, -1};
+  if (!cell_ok) return c;
+  const PmlAxis &X = g.pml[0], &Y = g.pml[1];
+  if (AX & 2) c.sy = slab_pos(y, g.ny, Y.T, Y.W);
+  if ((AX & 1) && X.T > 0) {
     const int s0 = slab_pos(xg, g.nx, X.T, X.W), s3 = slab_pos(xg + 3, g.nx, X.T, X.W);
     const int s1 = slab_pos(xg + 1, g.nx, X.T, X.W), s2 = slab_pos(xg + 2, g.nx, X.T, X.W);
     if (s0 >= 0 && s3 == s0 + 3 && (s0 & 3) == 0) {
-      L.xmode = 1;
-      L.sx = s0;
-      L.ix = (static_cast<long long>(p) * g.ny + y) * X.pitch + s0;
+      c.xmode = 1;
+      c.sx = s0;
     } else if (s0 >= 0 || s1 >= 0 || s2 >= 0 || s3 >= 0) {
-      L.xmode = 2;
+      c.xmode = 2;
     }
+  }
+  return c;
+}
+
+template <int AX>
+__device__ __forceinline__ LanePml lane_pml(const GridArgs &g, const LaneConst &c, int xg, int y,
+                                            int p) {
+  LanePml L{};
+  if (AX & 2) {
+    L.sy = c.sy;
+    L.y = c.sy >= 0;
+    if (L.y) L.iy = (static_cast<long long>(p) * g.pml[1].W + c.sy) * g.nx + xg;
+  }
+  if (AX & 4) {
+    const PmlAxis &Z = g.pml[2];
+    L.sz = slab_pos(p, g.nz, Z.T, Z.W);
+    L.z = L.sz >= 0;
+    if (L.z) L.iz = (static_cast<long long>(L.sz) * g.ny + y) * g.nx + xg;
+  }
+  if (AX & 1) {
+    L.xmode = c.xmode;
+    L.sx = c.sx;
+    if (c.xmode == 1) L.ix = (static_cast<long long>(p) * g.ny + y) * g.pml[0].pitch + c.sx;
   }
   return L;
 }
@@ -102,6 +132,12 @@ __device__ __forceinline__ LanePml lane_pml(const GridArgs &g, int xg, int y, in
 // The two psi terms of one axis for a lane's 4 cells (float4 each).
 struct Psi2 {
   float4 p0, p1;
+};
+
+// The H-term psi of the -x halo cell on each axis (slab position, or -1).
+struct HaloPsi {
+  int sx, sy, sz;
+  float x0, x1, y0, y1, z0, z1;
 };
 
 __device__ __forceinline__ Psi2 load_psi2(const PmlAxis &P, int comp0, long long idx) {
@@ -119,13 +155,23 @@ __device__ __forceinline__ void corr4_uniform(float d0[4], float d1[4], Psi2 &q,
   }
 }
 
+// CPML profiles (b, a, 1/kappa at slab positions) as the body reads them:
+// a shared-memory copy when every axis's slab fits kProfCap positions,
+// otherwise the global arrays.
+constexpr int kProfCap = kProfSmem / 9;
+struct Prof {
+  const float *p;  // shared memory: [3 axes][b, a, 1/kappa][kProfCap]
+  __device__ __forceinline__ float b(int ax, int s) const { return p[ax * 3 * kProfCap + s]; }
+  __device__ __forceinline__ float a(int ax, int s) const { return p[(ax * 3 + 1) * kProfCap + s]; }
+  __device__ __forceinline__ float ik(int ax, int s) const { return p[(ax * 3 + 2) * kProfCap + s]; }
+};
+
 // x axis: per-cell coefficients at slab positions s0..s0+3.
 template <bool FMA>
-__device__ __forceinline__ void corr4_x(float d0[4], float d1[4], Psi2 &q, const PmlAxis &P, int s0) {
+__device__ __forceinline__ void corr4_x(float d0[4], float d1[4], Psi2 &q, const Prof &pf, int s0) {
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const float b = __ldg(P.prof + s0 + i), a = __ldg(P.prof + P.W + s0 + i),
-                ik = __ldg(P.prof + 2 * P.W + s0 + i);
+    const float b = pf.b(0, s0 + i), a = pf.a(0, s0 + i), ik = pf.ik(0, s0 + i);
     d0[i] = pml_corr<FMA>(d0[i], b, a, ik, el(q.p0, i));
     d1[i] = pml_corr<FMA>(d1[i], b, a, ik, el(q.p1, i));
   }
@@ -133,14 +179,14 @@ __device__ __forceinline__ void corr4_x(float d0[4], float d1[4], Psi2 &q, const
 
 // x axis, one cell at a time (lanes straddling a slab edge, the x-halo cell).
 template <bool FMA>
-__device__ __forceinline__ void corr_x_cell(const GridArgs &g, int comp0, int x, int y, int p,
-                                            float &d0, float &d1, bool store) {
+__device__ __forceinline__ void corr_x_cell(const GridArgs &g, const Prof &pf, int comp0, int x,
+                                            int y, int p, float &d0, float &d1, bool store) {
   const PmlAxis &P = g.pml[0];
   const int s = slab_pos(x, g.nx, P.T, P.W);
   if (s < 0) return;
   const long long idx = (static_cast<long long>(p) * g.ny + y) * P.pitch + s;
   float p0 = __ldg(P.psi_cur + comp0 * P.cells + idx), p1 = __ldg(P.psi_cur + (comp0 + 1) * P.cells + idx);
-  const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+  const float b = pf.b(0, s), a = pf.a(0, s), ik = pf.ik(0, s);
   d0 = pml_corr<FMA>(d0, b, a, ik, p0);
   d1 = pml_corr<FMA>(d1, b, a, ik, p1);
   if (store) {
@@ -151,24 +197,27 @@ __device__ __forceinline__ void corr_x_cell(const GridArgs &g, int comp0, int x,
 
 // y or z axis, one cell (the x-halo cell).
 template <bool FMA>
-__device__ __forceinline__ void corr_yz_cell(const GridArgs &g, int axis, int x, int y, int p,
-                                             float &d0, float &d1) {
+__device__ __forceinline__ void corr_yz_cell(const GridArgs &g, const Prof &pf, int axis, int x,
+                                             int y, int p, float &d0, float &d1) {
   const PmlAxis &P = g.pml[axis];
   const int s = axis == 1 ? slab_pos(y, g.ny, P.T, P.W) : slab_pos(p, g.nz, P.T, P.W);
   if (s < 0) return;
   const long long idx = axis == 1 ? (static_cast<long long>(p) * P.W + s) * g.nx + x
                                   : (static_cast<long long>(s) * g.ny + y) * g.nx + x;
   float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
-  const float b = __ldg(P.prof + s), a = __ldg(P.prof + P.W + s), ik = __ldg(P.prof + 2 * P.W + s);
+  const float b = pf.b(axis, s), a = pf.a(axis, s), ik = pf.ik(axis, s);
   d0 = pml_corr<FMA>(d0, b, a, ik, p0);
   d1 = pml_corr<FMA>(d1, b, a, ik, p1);
 }
 
-template <int TY, int S, bool FMA, bool PML>
+// AX: the CPML axes this body handles (bit 1 x, 2 y, 4 z; 0 = interior).
+template <int TY, int S, bool FMA, int AX>
 __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtensorMap *tmH,
                                            const CUtensorMap *tmM, const FusedArgs &a,
                                            unsigned char *smem, int x0, int y0, int k0, int k1) {
   using L = Layout<TY, S>;
+  constexpr bool PML = AX != 0;
+  constexpr bool AXX = (AX & 1) != 0, AXY = (AX & 2) != 0, AXZ = (AX & 4) != 0;
   const GridArgs &g = a.g;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const float4 *s_coef = reinterpret_cast<const float4 *>(smem);
@@ -214,20 +263,62 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   const int cE = 4 + 4 * lane;
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;  // H(p-1), own cells
 
+  const Prof pf{reinterpret_cast<const float *>(smem + L::PROF_OFF)};
+  const LaneConst lc = lane_const<AX>(g, xg, y, cell_ok);
+  // CPML: each plane's H-term psi is loaded one plane ahead (the first plane's
+  // here), so its latency hides behind a whole plane of work.
+  LanePml lp_n{};
+  Psi2 qx_n{}, qy_n{}, qz_n{};
+  auto prefetch = [&](int pp) {
+    lp_n = lane_pml<AX>(g, lc, xg, y, pp);
+    if (AXY && lp_n.y) qy_n = load_psi2(g.pml[1], 0, lp_n.iy);
+    if (AXZ && lp_n.z) qz_n = load_psi2(g.pml[2], 0, lp_n.iz);
+    if (AXX && lp_n.xmode == 1) qx_n = load_psi2(g.pml[0], 0, lp_n.ix);
+  };
+  // ... and so is the H-term psi of the -x halo cell (x0-1, y0+lane) that
+  // lanes 0..TY-1 of the halo warp update.
+  const bool xhalo = PML && !tile_warp && lane < TY && x0 > 0 && y0 + lane < ny;
+  HaloPsi hh_n{-1, -1, -1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  auto prefetch_halo = [&](int pp) {
+    const int xh = x0 - 1, yh = y0 + lane;
+    if (AXX) {
+      const PmlAxis &P = g.pml[0];
+      hh_n.sx = slab_pos(xh, nx, P.T, P.W);
+      if (hh_n.sx >= 0) {
+        const long long i = (static_cast<long long>(pp) * ny + yh) * P.pitch + hh_n.sx;
+        hh_n.x0 = __ldg(P.psi_cur + i);
+        hh_n.x1 = __ldg(P.psi_cur + P.cells + i);
+      }
+    }
+    if (AXY) {
+      const PmlAxis &P = g.pml[1];
+      hh_n.sy = slab_pos(yh, ny, P.T, P.W);
+      if (hh_n.sy >= 0) {
+        const long long i = (static_cast<long long>(pp) * P.W + hh_n.sy) * nx + xh;
+        hh_n.y0 = __ldg(P.psi_cur + i);
+        hh_n.y1 = __ldg(P.psi_cur + P.cells + i);
+      }
+    }
+    if (AXZ) {
+      const PmlAxis &P = g.pml[2];
+      hh_n.sz = slab_pos(pp, g.nz, P.T, P.W);
+      if (hh_n.sz >= 0) {
+        const long long i = (static_cast<long long>(hh_n.sz) * ny + yh) * nx + xh;
+        hh_n.z0 = __ldg(P.psi_cur + i);
+        hh_n.z1 = __ldg(P.psi_cur + P.cells + i);
+      }
+    }
+  };
+  if (PML && cell_ok) prefetch(kfirst);
+  if (xhalo) prefetch_halo(kfirst);
+
   for (int j = 0; j < np - 1; ++j) {
     const int p = kfirst + j;
     const bool warm = p < k0;
     const bool active = tile_warp || !warm;  // the halo warp idles on the warm-up plane
-
-    // CPML: this plane's H-term psi loads go out before the stage wait
-    LanePml lp{};
-    Psi2 qx{}, qy{}, qz{};
-    if (PML && active && cell_ok) {
-      lp = lane_pml(g, xg, y, p);
-      if (lp.y) qy = load_psi2(g.pml[1], 0, lp.iy);
-      if (lp.z) qz = load_psi2(g.pml[2], 0, lp.iz);
-      if (lp.xmode == 1) qx = load_psi2(g.pml[0], 0, lp.ix);
-    }
+    const LanePml lp = lp_n;
+    Psi2 qx = qx_n, qy = qy_n, qz = qz_n;
+    HaloPsi hh = hh_n;  // (pml_corr updates its psi argument in place)
 
     const bool arrived = mbar_wait(smem_u32(&s_bar[(j + 1) % S]), ((j + 1) / S) & 1);
     if (arrived && done == j + 1) done = j + 2;
@@ -276,39 +367,38 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       }
       if (PML && cell_ok) {  // CPML on the H terms (pml_correct_*, src/fdtd.rs:136-163)
         const bool wpsi = tile_warp && !warm;
-        if (lp.xmode == 1) {
-          corr4_x<FMA>(d_ez_dx, d_ey_dx, qx, g.pml[0], lp.sx);
+        if (AXX && lp.xmode == 1) {
+          corr4_x<FMA>(d_ez_dx, d_ey_dx, qx, pf, lp.sx);
           if (wpsi) {
             const PmlAxis &P = g.pml[0];
             stg4(P.psi_nxt + lp.ix, qx.p0);
             stg4(P.psi_nxt + P.cells + lp.ix, qx.p1);
           }
-        } else if (lp.xmode == 2) {
+        } else if (AXX && lp.xmode == 2) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) corr_x_cell<FMA>(g, 0, xg + q, y, p, d_ez_dx[q], d_ey_dx[q], wpsi);
+          for (int q = 0; q < 4; ++q)
+            corr_x_cell<FMA>(g, pf, 0, xg + q, y, p, d_ez_dx[q], d_ey_dx[q], wpsi);
         }
-        if (lp.y) {
-          const PmlAxis &P = g.pml[1];
-          corr4_uniform<FMA>(d_ez_dy, d_ex_dy, qy, __ldg(P.prof + lp.sy), __ldg(P.prof + P.W + lp.sy),
-                             __ldg(P.prof + 2 * P.W + lp.sy));
+        if (AXY && lp.y) {
+          corr4_uniform<FMA>(d_ez_dy, d_ex_dy, qy, pf.b(1, lp.sy), pf.a(1, lp.sy), pf.ik(1, lp.sy));
           if (wpsi) {
+            const PmlAxis &P = g.pml[1];
             stg4(P.psi_nxt + lp.iy, qy.p0);
             stg4(P.psi_nxt + P.cells + lp.iy, qy.p1);
           }
         }
-        if (lp.z) {
-          const PmlAxis &P = g.pml[2];
-          corr4_uniform<FMA>(d_ey_dz, d_ex_dz, qz, __ldg(P.prof + lp.sz), __ldg(P.prof + P.W + lp.sz),
-                             __ldg(P.prof + 2 * P.W + lp.sz));
+        if (AXZ && lp.z) {
+          corr4_uniform<FMA>(d_ey_dz, d_ex_dz, qz, pf.b(2, lp.sz), pf.a(2, lp.sz), pf.ik(2, lp.sz));
           if (wpsi) {
+            const PmlAxis &P = g.pml[2];
             stg4(P.psi_nxt + lp.iz, qz.p0);
             stg4(P.psi_nxt + P.cells + lp.iz, qz.p1);
           }
         }
         if (wpsi) {  // the E terms' psi: in flight across the barrier
-          if (lp.xmode == 1) ex_ = load_psi2(g.pml[0], 2, lp.ix);
-          if (lp.y) ey_ = load_psi2(g.pml[1], 2, lp.iy);
-          if (lp.z) ez_ = load_psi2(g.pml[2], 2, lp.iz);
+          if (AXX && lp.xmode == 1) ex_ = load_psi2(g.pml[0], 2, lp.ix);
+          if (AXY && lp.y) ey_ = load_psi2(g.pml[1], 2, lp.iy);
+          if (AXZ && lp.z) ez_ = load_psi2(g.pml[2], 2, lp.iz);
         }
       }
 #pragma unroll
@@ -347,10 +437,17 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
           float d_ey_dz1 = sub(En[(1 * L::EH + rh) * L::EW + 3], ey);
           float d_ex_dy1 = sub(Ec[(0 * L::EH + rh + 1) * L::EW + 3], ex);
           float d_ez_dy1 = sub(Ec[(2 * L::EH + rh + 1) * L::EW + 3], ez);
-          if (PML) {
-            corr_x_cell<FMA>(g, 0, xh, yh, p, d_ez_dx1, d_ey_dx1, false);
-            corr_yz_cell<FMA>(g, 1, xh, yh, p, d_ez_dy1, d_ex_dy1);
-            corr_yz_cell<FMA>(g, 2, xh, yh, p, d_ey_dz1, d_ex_dz1);
+          if (AXX && hh.sx >= 0) {
+            d_ez_dx1 = pml_corr<FMA>(d_ez_dx1, pf.b(0, hh.sx), pf.a(0, hh.sx), pf.ik(0, hh.sx), hh.x0);
+            d_ey_dx1 = pml_corr<FMA>(d_ey_dx1, pf.b(0, hh.sx), pf.a(0, hh.sx), pf.ik(0, hh.sx), hh.x1);
+          }
+          if (AXY && hh.sy >= 0) {
+            d_ez_dy1 = pml_corr<FMA>(d_ez_dy1, pf.b(1, hh.sy), pf.a(1, hh.sy), pf.ik(1, hh.sy), hh.y0);
+            d_ex_dy1 = pml_corr<FMA>(d_ex_dy1, pf.b(1, hh.sy), pf.a(1, hh.sy), pf.ik(1, hh.sy), hh.y1);
+          }
+          if (AXZ && hh.sz >= 0) {
+            d_ey_dz1 = pml_corr<FMA>(d_ey_dz1, pf.b(2, hh.sz), pf.a(2, hh.sz), pf.ik(2, hh.sz), hh.z0);
+            d_ex_dz1 = pml_corr<FMA>(d_ex_dz1, pf.b(2, hh.sz), pf.a(2, hh.sz), pf.ik(2, hh.sz), hh.z1);
           }
           const float4 cf = s_coef[Mc[rh * L::MW + 15]];
           hyv = h_new<FMA>(cf.z, Hc[(1 * L::HH + rh) * L::HW + 3], cf.w, sub(d_ex_dz1, d_ez_dx1));
@@ -360,6 +457,8 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         pl_hyh[rh] = hyv;
       }
     }
+    if (PML && cell_ok && j + 1 < np - 1) prefetch(p + 1);  // next plane's H terms
+    if (xhalo && j + 1 < np - 1) prefetch_halo(p + 1);
 
     ok = __syncthreads_or(ok ? 0 : 1) == 0;
     if (!ok) break;
@@ -391,26 +490,25 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
           d_hy_dx[q] = sub(hb[q], q == 0 ? hy_w : hb[q - 1]);
         }
         if (PML && cell_ok) {
-          if (lp.xmode == 1) {
+          if (AXX && lp.xmode == 1) {
             const PmlAxis &P = g.pml[0];
-            corr4_x<FMA>(d_hz_dx, d_hy_dx, ex_, P, lp.sx);
+            corr4_x<FMA>(d_hz_dx, d_hy_dx, ex_, pf, lp.sx);
             stg4(P.psi_nxt + 2 * P.cells + lp.ix, ex_.p0);
             stg4(P.psi_nxt + 3 * P.cells + lp.ix, ex_.p1);
-          } else if (lp.xmode == 2) {
+          } else if (AXX && lp.xmode == 2) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) corr_x_cell<FMA>(g, 2, xg + q, y, p, d_hz_dx[q], d_hy_dx[q], true);
+            for (int q = 0; q < 4; ++q)
+              corr_x_cell<FMA>(g, pf, 2, xg + q, y, p, d_hz_dx[q], d_hy_dx[q], true);
           }
-          if (lp.y) {
+          if (AXY && lp.y) {
             const PmlAxis &P = g.pml[1];
-            corr4_uniform<FMA>(d_hz_dy, d_hx_dy, ey_, __ldg(P.prof + lp.sy), __ldg(P.prof + P.W + lp.sy),
-                               __ldg(P.prof + 2 * P.W + lp.sy));
+            corr4_uniform<FMA>(d_hz_dy, d_hx_dy, ey_, pf.b(1, lp.sy), pf.a(1, lp.sy), pf.ik(1, lp.sy));
             stg4(P.psi_nxt + 2 * P.cells + lp.iy, ey_.p0);
             stg4(P.psi_nxt + 3 * P.cells + lp.iy, ey_.p1);
           }
-          if (lp.z) {
+          if (AXZ && lp.z) {
             const PmlAxis &P = g.pml[2];
-            corr4_uniform<FMA>(d_hy_dz, d_hx_dz, ez_, __ldg(P.prof + lp.sz), __ldg(P.prof + P.W + lp.sz),
-                               __ldg(P.prof + 2 * P.W + lp.sz));
+            corr4_uniform<FMA>(d_hy_dz, d_hx_dz, ez_, pf.b(2, lp.sz), pf.a(2, lp.sz), pf.ik(2, lp.sz));
             stg4(P.psi_nxt + 2 * P.cells + lp.iz, ez_.p0);
             stg4(P.psi_nxt + 3 * P.cells + lp.iz, ez_.p1);
           }
@@ -447,15 +545,20 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   }
 }
 
-template <int TY, int S, bool FMA>
-__global__ void __launch_bounds__(32 * (TY + 1))
+// One launch handles one class of work items: interior items (AX = 0: no
+// CPML code, lean registers), items meeting only the x, only the y or only
+// the z slab (AX = 1, 2, 4), or items meeting several (AX = 7).  The host
+// lists each class's items (tile x, tile y, z chunk); the launches
+// partition the grid.
+template <int TY, int S, bool FMA, int AX>
+__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 3 : 1)
     k_fused(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
-            const __grid_constant__ CUtensorMap tmM, const FusedArgs a) {
+            const __grid_constant__ CUtensorMap tmM, const FusedArgs a, const int *items) {
   using L = Layout<TY, S>;
   extern __shared__ unsigned char smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
-  int item = blockIdx.x;
+  int item = items[blockIdx.x];
   const int txi = item % a.tiles_x;
   item /= a.tiles_x;
   const int tyi = item % a.tiles_y;
@@ -466,44 +569,56 @@ __global__ void __launch_bounds__(32 * (TY + 1))
 
   float4 *s_coef = reinterpret_cast<float4 *>(smem);
   for (int i = threadIdx.x; i < 256; i += blockDim.x) s_coef[i] = a.g.coef[i];
+  if (AX != 0) {  // CPML profiles at slab positions (every W <= kProfCap here)
+    float *s_prof = reinterpret_cast<float *>(smem + L::PROF_OFF);
+    for (int i = threadIdx.x; i < kProfSmem; i += blockDim.x) {
+      const int cap = kProfSmem / 9;
+      const int ax = i / (3 * cap), k = (i / cap) % 3, s = i % cap;
+      const PmlAxis &P = a.g.pml[ax];
+      s_prof[i] = (P.T > 0 && s < P.W) ? P.prof[k * P.W + s] : 0.0f;
+    }
+  }
   if (threadIdx.x == 0) {
     uint64_t *s_bar = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
     for (int s = 0; s < S; ++s) mbar_init(smem_u32(&s_bar[s]), 1);
     mbar_fence_init();
   }
   __syncthreads();
-
-  // Does this CTA meet a graded CPML slab?  Interior CTAs skip all psi code.
-  bool pml = false;
-  if (a.has_pml) {
-    const PmlAxis &X = a.g.pml[0], &Y = a.g.pml[1], &Z = a.g.pml[2];
-    const int xh = min(x0 + kTileX, a.g.nx) - 1, yh = min(y0 + TY, a.g.ny) - 1;
-    if (X.T > 0 && (x0 - 1 < X.T || xh >= a.g.nx - X.T)) pml = true;
-    if (Y.T > 0 && (y0 - 1 < Y.T || yh >= a.g.ny - Y.T)) pml = true;
-    if (Z.T > 0 && (k0 - 1 < Z.T || k1 - 1 >= a.g.nz - Z.T)) pml = true;
-  }
-  if (pml)
-    fused_body<TY, S, FMA, true>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
-  else
-    fused_body<TY, S, FMA, false>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
+  fused_body<TY, S, FMA, AX>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
 }
+
+#define WF_AX_CLASSES(X) X(0) X(1) X(2) X(4) X(7)
 
 template <int TY, int S>
 cudaError_t prepare_t() {
   using L = Layout<TY, S>;
-  cudaError_t e = cudaFuncSetAttribute(k_fused<TY, S, false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_fused<TY, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              L::BYTES);
+  const void *fns[] = {
+#define X(A) (const void *)k_fused<TY, S, false, A>, (const void *)k_fused<TY, S, true, A>,
+      WF_AX_CLASSES(X)
+#undef X
+  };
+  for (const void *f : fns) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 template <int TY, int S, bool FMA>
-cudaError_t launch_t(const FusedMaps &m, const FusedArgs &a, cudaStream_t s) {
+cudaError_t launch_t(const FusedMaps &m, const FusedArgs &a, const int *items, int n_items,
+                     int ax, cudaStream_t s) {
   using L = Layout<TY, S>;
-  const long long nz_chunks = (a.g.nz + a.zchunk - 1) / a.zchunk;
-  const long long items = static_cast<long long>(a.tiles_x) * a.tiles_y * nz_chunks;
-  k_fused<TY, S, FMA><<<static_cast<unsigned>(items), L::THREADS, L::BYTES, s>>>(m.e, m.h, m.m, a);
+  if (n_items <= 0) return cudaSuccess;
+  switch (ax) {
+#define X(A)                                                                                 \
+  case A:                                                                                   \
+    k_fused<TY, S, FMA, A><<<n_items, L::THREADS, L::BYTES, s>>>(m.e, m.h, m.m, a, items); \
+    break;
+    WF_AX_CLASSES(X)
+#undef X
+    default:
+      return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -515,9 +630,26 @@ void fused_boxes(int ty, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]
   m_box[0] = kTileX + 16; m_box[1] = ty + 1; m_box[2] = 1;
 }
 
+int fused_item_class(const FusedArgs &a, int ty, int item) {
+  if (!a.has_pml) return 0;
+  const int txi = item % a.tiles_x;
+  const int tyi = (item / a.tiles_x) % a.tiles_y;
+  const int zc = item / (a.tiles_x * a.tiles_y);
+  const int x0 = txi * kTileX, y0 = tyi * ty;
+  const int k0 = zc * a.zchunk, k1 = std::min(k0 + a.zchunk, a.g.nz);
+  const PmlAxis &X = a.g.pml[0], &Y = a.g.pml[1], &Z = a.g.pml[2];
+  const int xh = std::min(x0 + kTileX, a.g.nx) - 1, yh = std::min(y0 + ty, a.g.ny) - 1;
+  // an axis's CPML code is needed if the CTA's cells, its -x/-y halo or its
+  // warm-up plane (k0-1) meet that axis's graded slab
+  int mask = 0;
+  if (X.T > 0 && (x0 - 1 < X.T || xh >= a.g.nx - X.T)) mask |= 1;
+  if (Y.T > 0 && (y0 - 1 < Y.T || yh >= a.g.ny - Y.T)) mask |= 2;
+  if (Z.T > 0 && (k0 - 1 < Z.T || k1 - 1 >= a.g.nz - Z.T)) mask |= 4;
+  return (mask == 0 || mask == 1 || mask == 2 || mask == 4) ? mask : 7;
+}
+
 // (tile rows, stages) combinations that are instantiated
-#define WF_FUSED_CONFIGS(X) \
-  X(4, 3) X(4, 4) X(6, 3) X(8, 3) X(8, 4) X(12, 3) X(16, 2) X(16, 3)
+#define WF_FUSED_CONFIGS(X) X(4, 3) X(4, 4) X(8, 3) X(8, 4) X(16, 3)
 
 bool fused_supported(const FusedConfig &c) {
 #define X(T, S_) if (c.ty == T && c.stages == S_) return c.zchunk >= 1;
@@ -540,11 +672,12 @@ cudaError_t fused_prepare(const FusedConfig &c) {
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a, bool fma,
-                         cudaStream_t s) {
-#define X(T, S_)                                                         \
-  if (c.ty == T && c.stages == S_)                                      \
-    return fma ? launch_t<T, S_, true>(m, a, s) : launch_t<T, S_, false>(m, a, s);
+cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
+                         const int *items, int n_items, int ax, bool fma, cudaStream_t s) {
+#define X(T, S_)                                                                        \
+  if (c.ty == T && c.stages == S_)                                                     \
+    return fma ? launch_t<T, S_, true>(m, a, items, n_items, ax, s)                    \
+               : launch_t<T, S_, false>(m, a, items, n_items, ax, s);
   WF_FUSED_CONFIGS(X)
 #undef X
   return cudaErrorInvalidValue;

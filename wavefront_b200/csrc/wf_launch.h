@@ -22,6 +22,7 @@ struct FusedArgs {
   GridArgs g;
   int tiles_x, tiles_y, zchunk;
   int has_pml;
+  int prof_in_smem;  // every CPML axis has at most 64 slab positions
 };
 
 // Tiling of the fused kernel: TY rows per CTA (x width kTileX), z chunk and
@@ -48,7 +49,12 @@ bool fused_supported(const FusedConfig &c);
 int fused_smem_bytes(const FusedConfig &c);
 // Sets the kernels' dynamic shared-memory limit (call outside graph capture).
 cudaError_t fused_prepare(const FusedConfig &c);
-cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a, bool fma,
-                         cudaStream_t s);
+// Kernel class of work item `item` (tile x, tile y, z chunk): 0 interior,
+// 1 / 2 / 4 meets only the x / y / z CPML slab, 7 meets several.
+int fused_item_class(const FusedArgs &a, int ty, int item);
+constexpr int kFusedClasses[5] = {0, 1, 2, 4, 7};
+// Launches the kernel of class `ax` over a device list of n_items items.
+cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
+                         const int *items, int n_items, int ax, bool fma, cudaStream_t s);
 
 }  // namespace wf
