@@ -197,6 +197,7 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    k_before = g.kernel_launches
     with ClockSampler(local_rank) as clk:
         e0.record(stream)
         g.step(args.steps)
@@ -206,6 +207,7 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1)
+    gpu_launches = g.kernel_launches - k_before
     kern_ms, launches = g.timing()
     g.set_timing(False)
     g.close()
@@ -273,7 +275,7 @@ def run_ours(args, rank, world, local_rank):
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
                          "kernel_ms_per_launch": round(per_launch_ms, 4)},
-            "gpu_launches": int(launches) + args.steps,
+            "gpu_launches": int(gpu_launches),
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu:

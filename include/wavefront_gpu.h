@@ -178,6 +178,9 @@ wf_status wf_get_stream(wf_handle *h, void **out_stream);
  * since timing was enabled. */
 wf_status wf_set_timing(wf_handle *h, int enable);
 wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches);
+/* Device kernels this handle has launched for steps so far (step kernels of
+ * every work class plus the source/probe tail), graph replays included. */
+int64_t wf_kernel_launches(const wf_handle *h);
 
 /* ---- fused-kernel tiling (autotuner surface) --------------------------- */
 

@@ -70,6 +70,8 @@ struct wf_handle {
   long long *d_step = nullptr;
   int *d_err = nullptr;
   long long steps_done = 0;
+  long long kernel_launches = 0;       // step + tail kernels issued so far
+  long long graph_kernels[2] = {0, 0};  // kernels in one replay of graph[parity]
   FusedConfig cfg{4, 12, 3};
   bool cfg_user_set = false;  // otherwise chosen from the grid at first use
   wf::FusedMaps maps[2];      // per state buffer (the one read by the step)
@@ -285,6 +287,7 @@ wf_status enqueue_one(wf_handle *h) {
       if (k > 0) WF_CUDA(h, cudaStreamWaitEvent(s, h->fork_ev, 0));
       e = wf::launch_fused(h->cfg, h->maps[h->cur], a, h->d_items + h->class_off[k],
                            h->class_n[k], wf::kFusedClasses[k], fma, s);
+      if (e == cudaSuccess) h->kernel_launches += 1;
       if (e == cudaSuccess && k > 0) {
         WF_CUDA(h, cudaEventRecord(h->join_ev[k - 1], s));
         WF_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_ev[k - 1], 0));
@@ -292,6 +295,7 @@ wf_status enqueue_one(wf_handle *h) {
     }
   } else {
     e = wf::launch_split(g, fma, h->stream);
+    if (e == cudaSuccess) h->kernel_launches += 2;  // H pass, E pass
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
   if (h->timing) {
@@ -312,6 +316,7 @@ wf_status enqueue_one(wf_handle *h) {
     t.step = h->d_step;
     e = wf::launch_tail(t, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "tail kernel launch");
+    h->kernel_launches += 1;
   }
   h->cur ^= 1;
   return WF_OK;
@@ -648,12 +653,16 @@ wf_status wf_step(wf_handle *h, int nsteps) {
     cudaGraphExec_t &ge = h->graph[h->cur];
     if (!ge) {
       const int cur0 = h->cur;
+      const long long k0 = h->kernel_launches;
       cudaGraph_t graph;
       WF_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       wf_status st = WF_OK;
       for (int i = 0; i < G && st == WF_OK; ++i) st = enqueue_one(h);
       cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
       h->cur = cur0;
+      // captured launches run at each replay, not now
+      h->graph_kernels[cur0] = h->kernel_launches - k0;
+      h->kernel_launches = k0;
       if (st != WF_OK) return st;
       if (ec != cudaSuccess) return cuda_fail(h, ec, "cudaStreamEndCapture");
       ec = cudaGraphInstantiate(&ge, graph, 0);
@@ -661,6 +670,7 @@ wf_status wf_step(wf_handle *h, int nsteps) {
       if (ec != cudaSuccess) return cuda_fail(h, ec, "cudaGraphInstantiate");
     }
     WF_CUDA(h, cudaGraphLaunch(ge, h->stream));
+    h->kernel_launches += h->graph_kernels[h->cur];
     left -= G;
     h->steps_done += G;
     if (G % 2) h->cur ^= 1;
@@ -681,6 +691,8 @@ wf_status wf_sync(wf_handle *h) {
 }
 
 int64_t wf_steps_done(const wf_handle *h) { return h ? h->steps_done : -1; }
+
+int64_t wf_kernel_launches(const wf_handle *h) { return h ? h->kernel_launches : -1; }
 
 wf_status wf_probe_sums(wf_handle *h, int p, double *c, double *s, uint64_t *n) {
   if (!h || p < 0 || p >= static_cast<int>(h->probes.size())) return fail(h, WF_ERR_ARG, "bad probe index");

@@ -118,6 +118,11 @@ class DeviceFieldGrid:
     def steps_done(self) -> int:
         return int(_L.lib().wf_steps_done(self._h))
 
+    @property
+    def kernel_launches(self) -> int:
+        """Device kernels launched for steps so far (all work classes + tail)."""
+        return int(_L.lib().wf_kernel_launches(self._h))
+
     # -- timing -------------------------------------------------------------
     def stream(self) -> int:
         v = C.c_void_p()
