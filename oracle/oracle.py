@@ -89,6 +89,15 @@ def _declare(L: C.CDLL) -> None:
         getattr(L, p + "get_psi").argtypes = [C.c_void_p, C.c_int, rp]
         getattr(L, p + "probe_sums").argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, C.POINTER(C.c_uint64)]
         getattr(L, p + "probe_trace").argtypes = [C.c_void_p, C.c_int, _f64p]
+        getattr(L, p + "set_storage").argtypes = [C.c_void_p, C.c_int]
+        getattr(L, p + "set_storage").restype = C.c_int
+        getattr(L, p + "storage_overflows").argtypes = [C.c_void_p]
+        getattr(L, p + "storage_overflows").restype = C.c_longlong
+        getattr(L, p + "get_shifts").argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.or_store_shift.argtypes = [C.c_float]
+    L.or_store_shift.restype = C.c_int
+    L.or_store16.argtypes = [C.c_float, C.c_int, C.c_int, C.POINTER(C.c_longlong)]
+    L.or_store16.restype = C.c_float
 
 
 def _ptr(a: np.ndarray, t):
@@ -285,11 +294,42 @@ class Sim:
         self._f("probe_trace")(self._h, p, _ptr(out, _f64p))
         return out
 
+    def set_storage(self, kind: str):
+        """16-bit field storage emulation: "f32" (off), "f16" or "bf16" (both
+        round to nearest even).  Call after the sources are added (their
+        amplitudes enter the shifts)."""
+        if self._f("set_storage")(self._h, STORAGE_KINDS[kind]) != 0:
+            raise ValueError("storage emulation needs the f32 oracle")
 
-def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None):
+    @property
+    def storage_overflows(self) -> int:
+        return int(self._f("storage_overflows")(self._h))
+
+    def shifts(self):
+        nbz = self.nz // 8
+        e = (C.c_int * nbz)()
+        h = (C.c_int * nbz)()
+        self._f("get_shifts")(self._h, e, h)
+        return np.array(e[:], np.int32), np.array(h[:], np.int32)
+
+
+STORAGE_KINDS = {"f32": 0, "f16": 1, "bf16": 2}
+
+
+def store_shift(bound: float) -> int:
+    return int(lib().or_store_shift(bound))
+
+
+def store16(v: float, kind: str, shift: int) -> float:
+    ov = C.c_longlong(0)
+    return float(lib().or_store16(v, STORAGE_KINDS[kind], shift, C.byref(ov)))
+
+
+def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None, storage="f32"):
     """Builds an oracle Sim for a wavefront_b200.configs.Scenario, computing every
     table (CPML profiles, source values, probe twiddles) with the oracle's own
-    C code; only the scenario's description and its material ids are shared."""
+    C code; only the scenario's description and its material ids are shared.
+    storage "f16"/"bf16" turns on the 16-bit storage emulation (f32 only)."""
     steps = sc.steps if steps is None else steps
     d = sc.dims
     sim = Sim(d.nx, d.ny, d.nz, sc.grid.ids, sc.table.q16, periodic, dtype)
@@ -309,4 +349,6 @@ def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None):
         c, si = probe_tables(p.frequencies_hz, sc.dt, steps)
         sim.add_probe(p.x, p.y, p.z, int(p.component), c, si, steps,
                       probe_first_step(p.start_recording_at_s, sc.dt), p.record_trace)
+    if storage != "f32":
+        sim.set_storage(storage)
     return sim

@@ -297,6 +297,55 @@ static void or_parallel_blocks(int nb, int nthreads, or_range_fn fn, void *ctx) 
   for (int i = 1; i < nj; i++) pthread_join(th[i], NULL);
 }
 
+/* ------------------------------------------------------------------------ */
+/* 16-bit field storage (no reference counterpart): the mixed-precision      */
+/* form's storage rounding, emulated exactly so the CUDA kernels that store   */
+/* f16/bf16 can be checked bit for bit.                                       */
+/* ------------------------------------------------------------------------ */
+
+static inline uint32_t or_f2u(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline float or_u2f(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+/* |v| as its bit pattern: non-negative floats order like their bits. */
+static inline uint32_t or_abs_bits(float v) { return or_f2u(v) & 0x7fffffffu; }
+
+/* Power-of-two shift that maps a bound b into [2^13, 2^14): the biased
+ * exponent field of b minus 140, clamped to [-60, 60] (zero or subnormal
+ * bounds take -60). */
+int or_store_shift(float bound) {
+  int e8 = (int)((or_f2u(bound) >> 23) & 0xffu);
+  int sh = e8 == 0 ? -60 : e8 - 127 - 13;
+  return sh < -60 ? -60 : (sh > 60 ? 60 : sh);
+}
+
+/* bf16 from f32, round to nearest even on the dropped 16 bits (NaN and
+ * infinities pass unchanged). */
+static inline float or_round_bf16(float v) {
+  uint32_t u = or_f2u(v);
+  if ((u & 0x7f800000u) == 0x7f800000u) return v;
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return or_u2f(u & 0xffff0000u);
+}
+
+/* Stores v as a 16-bit value of v * 2^-shift and returns the decoded f32
+ * value: kind 1 = IEEE binary16, round to nearest even, finite values
+ * saturating at +-65504 (counted in *overflow); kind 2 = bf16, round to
+ * nearest even.  Scaling by a power of two is exact, so the decoded value is
+ * exactly what a device kernel storing the same format reads back. */
+float or_store16(float v, int kind, int shift, long long *overflow) {
+  float u = v * ldexpf(1.0f, -shift);
+  if (kind == 1) {
+    if (u > 65504.0f || u < -65504.0f) {
+      __atomic_fetch_add(overflow, 1, __ATOMIC_RELAXED);
+      u = u > 0 ? 65504.0f : -65504.0f;
+    }
+    u = (float)(_Float16)u;
+  } else {
+    u = or_round_bf16(u);
+  }
+  return u * ldexpf(1.0f, shift);
+}
+
 #define REAL float
 #define SIM or_sim_f32
 #define FN(n) or_sim_f32_##n

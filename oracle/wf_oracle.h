@@ -59,6 +59,14 @@ int or_scene_voxelize(const char *text, int nx, int ny, int nz, float dt,
 /* src/main.rs:403-425: material id 1 sphere at the domain centre. */
 void or_demo_sphere(int nx, int ny, int nz, uint8_t *grid);
 
+/* ---- 16-bit field storage (mixed-precision form; no reference code) ----- */
+/* Shift mapping a bound into [2^13, 2^14) (biased exponent - 140, clamped
+ * to [-60, 60]). */
+int   or_store_shift(float bound);
+/* Decoded value of v stored as kind (1 f16 saturating, 2 bf16; both round to
+ * nearest even) of v * 2^-shift; counts f16 saturations. */
+float or_store16(float v, int kind, int shift, long long *overflow);
+
 /* ---- the timestep engine (src/engine.rs, src/fdtd.rs) ------------------ */
 typedef struct or_sim_f32 or_sim_f32;
 typedef struct or_sim_f64 or_sim_f64;
@@ -93,7 +101,13 @@ typedef struct or_sim_f64 or_sim_f64;
   void S##_get_psi(const S *s, int which, R *out);                              \
   void S##_probe_sums(const S *s, int p, double *cos_out, double *sin_out,      \
                       uint64_t *n);                                             \
-  void S##_probe_trace(const S *s, int p, double *out);
+  void S##_probe_trace(const S *s, int p, double *out);                         \
+  /* 16-bit field storage (f32 sim only): 0 plain, 1 f16, 2 bf16.  Re-encodes  \
+   * the current state; -1 for a bad kind or on the f64 sim. */                \
+  int S##_set_storage(S *s, int kind);                                          \
+  long long S##_storage_overflows(const S *s);                                  \
+  /* write shifts (per 8-plane z slab) of the next step, E and H kinds */      \
+  void S##_get_shifts(const S *s, int *shift_e, int *shift_h);
 
 OR_DECLARE_SIM(or_sim_f32, float)
 OR_DECLARE_SIM(or_sim_f64, double)

@@ -89,6 +89,43 @@ def two_spheres(n: int = 512, steps: int = 1000, pml_cells: int = 16) -> Scenari
                     {"f": f})
 
 
+def random_spheres_text(n: int, count: int = 32, seed: int = 1234) -> str:
+    """`count` spheres drawn from numpy's PCG64 stream `seed`, in file order:
+    centre U[0,n) per axis, radius U[20,120]*(n/1024) cells, eps_r U[1,8],
+    sigma U[0,0.01] S/m, mu_r 1 (a later sphere overwrites an earlier one)."""
+    rng = np.random.default_rng(seed)
+    lines = []
+    for _ in range(count):
+        cx, cy, cz = rng.uniform(0.0, n, 3)
+        r = rng.uniform(20.0, 120.0) * (n / 1024.0)
+        eps = rng.uniform(1.0, 8.0)
+        sig = rng.uniform(0.0, 0.01)
+        lines.append(f"sphere {eps:.6f} 1.0 {sig:.6f} {cx:.4f} {cy:.4f} {cz:.4f} {r:.4f}")
+    return "\n".join(lines) + "\n"
+
+
+def random_spheres(n: int = 1024, steps: int = 2000, pml_cells: int = 16,
+                   seed: int = 1234) -> Scenario:
+    """Mixed-precision workload: 32 seeded random dielectric spheres, 16-cell
+    CPML, sinusoid Ez at the centre with 15 cells per wavelength, 8 Ez probes
+    on a line at z = 7n/8 (x = n/16 + k*n/8, y = n/2), 2000 steps.  The same
+    scene at n = 128 is small enough for the FP64 oracle."""
+    dims = GridDims(n, n, n)
+    dx = 1.0e-3
+    dt = courant_dt(dx)
+    f = float(np.float32(C0 / (15.0 * dx)))
+    grid = MaterialGrid(dims)
+    table = MaterialTable.vacuum_filled(dt, dx)
+    Scene.parse(random_spheres_text(n, seed=seed)).voxelize(grid, table, dt, dx)
+    pml = PmlContext.build(dims, PmlConfig(thickness=pml_cells), dt, dx) if pml_cells else None
+    c = n // 2
+    src = Source(c, c, c, FieldComponent.Ez, 1.0, default_waveform("sinusoid", f))
+    zp = (7 * n) // 8
+    probes = [Probe(n // 16 + (n // 8) * k, c, zp, PC.Ez, [f], 0.0) for k in range(8)]
+    return Scenario(f"random_spheres_{n}", dims, dx, dt, grid, table, pml, [src], probes, steps,
+                    {"f": f, "seed": seed})
+
+
 def demo_sphere_cube(n: int = 256, steps: int = 150, pml_cells: int = 8) -> Scenario:
     dims = GridDims(n, n, n)
     dx, dt = 1.0e-3, 1.5e-12
