@@ -7,6 +7,13 @@ A step is one full Yee timestep of the whole grid (H, E, CPML psi, source,
 probes).  Metric: Mcell-updates/s = cells * steps / seconds / 1e6.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload two_spheres|random_spheres] [--grid N]
+                  [--precision f32|f16|bf16]
+
+--workload random_spheres --precision f16|bf16 measures the mixed-precision
+form (32 seeded random spheres, sinusoid source, 16-cell CPML; fields stored
+as 16-bit values with per-slab power-of-two scales, FP32 arithmetic) against
+the same scene in FP32 (--precision f32).
 
 Our arm prints one JSON line with `value` (device-resident, CUDA events on
 the handle's stream), `e2e` (through the C ABI from host buffers: upload of
@@ -40,13 +47,18 @@ N_CELLS = GRID ** 3
 WORKLOAD = f"two_spheres_{GRID}^3_fp32_cpml16_gaussian_8probes"
 
 
+PRECISION = "f32"
+ELEM = {"f32": 4, "f16": 2, "bf16": 2}
+
+
 def algorithmic_bytes(sc) -> int:
-    """Per fused-kernel launch: 49 B per cell (6 f32 fields read + written, 1 B
-    material id) plus 32 B per (cell, axis) inside that axis's graded slab
-    (4 psi values read + written)."""
+    """Per step (one launch of each fused work class): 6 fields read + written
+    at the storage width plus 1 B material id per cell (49 B in FP32, 25 B in
+    16-bit storage), plus 32 B per (cell, axis) inside that axis's graded
+    slab (4 FP32 psi values read + written)."""
     n = (sc.dims.nx, sc.dims.ny, sc.dims.nz)
     cells = sc.dims.voxel_count()
-    b = 49 * cells
+    b = (12 * ELEM[PRECISION] + 1) * cells
     for ax in range(3):
         t = sc.pml.thickness_voxels[ax] if sc.pml else 0
         if t:
@@ -128,11 +140,17 @@ def cpu_baseline(sc, seconds=15.0):
             "kind": "port", "sample": f"{n} full {GRID}^3 steps after 1 warm-up step, {el:.1f} s"}
 
 
+def scenario(args, steps):
+    from wavefront_b200 import configs
+    if args.workload == "random_spheres":
+        return configs.random_spheres(n=GRID, steps=steps)
+    return configs.two_spheres(n=GRID, steps=steps)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    from wavefront_b200 import configs
-    sc = configs.two_spheres(n=GRID, steps=args.warmup + args.steps)
+    sc = scenario(args, args.warmup + args.steps)
     from oracle import oracle as O
     nt = os.cpu_count() or 1
     sim = O.sim_from_scenario(sc, steps=args.warmup + args.steps)
@@ -154,9 +172,10 @@ def run_reference(args, rank, world):
         "n_gpus": world, "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": round(el / n * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": {"workload": WORKLOAD, "grid": [GRID] * 3,
-                                        "l2": "inputs larger than L2 (3.2 GB of fields)"},
+                                        "l2": f"inputs larger than L2 ({N_CELLS * 24 / 1e9:.1f} GB "
+                                              "of fields)"},
         "cpu_baseline": {"value": round(v, 2), "unit": METRIC, "cores": nt, "kind": "port",
-                         "sample": f"{n} of {args.steps} requested 512^3 steps in {el:.1f} s "
+                         "sample": f"{n} of {args.steps} requested {GRID}^3 steps in {el:.1f} s "
                                    "(time-bounded); the Rust reference cannot be built here, so "
                                    "this is the oracle's C restatement of its f32 AVX2 path"},
         "e2e": {"value": round(v, 2), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -173,10 +192,10 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     total = args.warmup + args.steps
-    sc = configs.two_spheres(n=GRID, steps=total)
+    sc = scenario(args, total)
 
     def build(kernel="fused"):
-        g = configs.device_grid(sc, kernel=kernel, device=local_rank)
+        g = configs.device_grid(sc, kernel=kernel, device=local_rank, precision=PRECISION)
         if args.tiling:
             g.set_tiling(*[int(v) for v in args.tiling.split(",")])
         for s in sc.sources:
@@ -224,7 +243,7 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and args.workload == "two_spheres" and GRID == 512 and PRECISION == "f32":
         with open(tf) as f:
             traffic = json.load(f).get("fused_two_spheres_512_bytes_per_launch")
 
@@ -264,7 +283,9 @@ def run_ours(args, rank, world, local_rank):
                        "probes": 8, "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
                        "tiling": {"tile_rows": tiling[0], "z_chunk": tiling[1],
                                   "stages": tiling[2]},
-                       "l2": "inputs larger than L2 (3.2 GB of fields per state buffer)",
+                       "storage": PRECISION,
+                       "l2": f"inputs larger than L2 ({N_CELLS * 6 * ELEM[PRECISION] / 1e9:.1f} GB "
+                             "of fields per state buffer)",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": round(e2e, 1), "unit": METRIC,
                     "h2d_bytes_per_step": int(h2d / args.steps),
@@ -293,12 +314,22 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tiling", default="", help="tile_rows,z_chunk,stages")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--grid", type=int, default=512, help="cube edge (profiling captures only)")
+    ap.add_argument("--grid", type=int, default=0,
+                    help="cube edge (default 512 for two_spheres, 1024 for random_spheres)")
+    ap.add_argument("--workload", default="two_spheres", choices=["two_spheres", "random_spheres"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
+                    help="field storage (16-bit: per-slab power-of-two scales, FP32 math)")
     args = ap.parse_args()
-    global GRID, N_CELLS, WORKLOAD
-    GRID = args.grid
+    global GRID, N_CELLS, WORKLOAD, PRECISION
+    GRID = args.grid or (1024 if args.workload == "random_spheres" else 512)
     N_CELLS = GRID ** 3
-    WORKLOAD = f"two_spheres_{GRID}^3_fp32_cpml16_gaussian_8probes"
+    PRECISION = args.precision
+    if args.workload == "random_spheres":
+        WORKLOAD = f"random_spheres_{GRID}^3_{PRECISION}_storage_cpml16_sinusoid_8probes"
+    elif PRECISION == "f32":
+        WORKLOAD = f"two_spheres_{GRID}^3_fp32_cpml16_gaussian_8probes"
+    else:
+        WORKLOAD = f"two_spheres_{GRID}^3_{PRECISION}_storage_cpml16_gaussian_8probes"
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))

@@ -63,6 +63,13 @@ typedef enum {
   WF_KERNEL_SPLIT = 2  /* an H kernel then an E kernel (any boundaries)      */
 } wf_kernel;
 
+/* Field storage.  The 16-bit forms (no reference counterpart) store each
+ * field value v as a 16-bit number of v * 2^-shift, round to nearest even,
+ * with one power-of-two shift per z slab of 8 planes and per kind (E, H);
+ * arithmetic is FP32 in the reference's order, probe sums FP64, CPML psi
+ * FP32.  They need the exact arithmetic, the fused kernel (zero-field
+ * boundaries, CPML slabs of at most 64 cells) and nz <= 8192; the FP32 view
+ * (get/set fields, snapshots) converts at the boundary. */
 typedef enum {
   WF_PREC_F32 = 0,  /* FP32 field storage (reference parity)               */
   WF_PREC_BF16 = 1, /* BF16 storage, per-slab power-of-two scale, FP32 math */
@@ -168,6 +175,10 @@ wf_status wf_upload_blocks(wf_handle *h, const void *in);
 wf_status wf_get_psi(wf_handle *h, int which, float *out);
 /* Device pointers of the current six field arrays (FP32 precision only). */
 wf_status wf_device_fields(wf_handle *h, float **out6);
+/* 16-bit storage: the shifts the next step stores E and H with, per z slab
+ * (nz/8 entries each; either may be NULL), and the count of binary16 values
+ * saturated at +-65504 so far.  FP32 storage reports 0 overflows. */
+wf_status wf_storage_info(wf_handle *h, int *shift_e, int *shift_h, uint64_t *overflows);
 
 /* The handle's CUDA stream (cudaStream_t) for event timing and interop. */
 wf_status wf_get_stream(wf_handle *h, void **out_stream);

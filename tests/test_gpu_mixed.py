@@ -1,0 +1,166 @@
+"""GPU: the 16-bit storage forms (binary16 / bfloat16 fields with one
+power-of-two shift per 8-plane z slab and field kind, FP32 arithmetic, FP64
+probe sums) through the C ABI.
+
+Two bars.  Parity: against the oracle's emulation of the same storage
+rounding (oracle set_storage), bit-exact -- fields, psi, probe sums and the
+shifts the next step would store with.  Error: against the FP64 oracle on
+the mixed-precision workload (random spheres, sinusoid source, 2000 steps) at
+128^3, with the measured figures printed and bounded.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import wavefront_b200 as wf
+from wavefront_b200 import configs
+
+pytestmark = pytest.mark.gpu
+NT = min(os.cpu_count() or 1, 32)
+
+
+def _eq(got, want, what):
+    bad = got != want  # +0 == -0
+    if bad.any():
+        idx = np.argwhere(bad)[:5]
+        raise AssertionError(f"{what}: {bad.sum()} values differ, first {idx.tolist()}, "
+                             f"got {got[bad][:5]} want {want[bad][:5]}")
+
+
+def _run(sc, precision, steps=None, tiling=None):
+    steps = sc.steps if steps is None else steps
+    g = configs.device_grid(sc, kernel="fused", precision=precision)
+    if tiling:
+        g.set_tiling(*tiling)
+    for s in sc.sources:
+        g.add_source_values(s.x, s.y, s.z, s.component, s.values(sc.dt, steps), s.mode)
+    for p in sc.probes:
+        c, si = p.tables(sc.dt, steps)
+        g.add_probe_tables(p.x, p.y, p.z, p.component, c, si, p.first_step(sc.dt))
+    g.step(steps)
+    g.sync()
+    return g
+
+
+def _compare(g, sim, sc):
+    _eq(g.fields(), sim.fields(), "fields")
+    for i, p in enumerate(sc.probes):
+        nf = len(p.frequencies_hz)
+        gc, gs, gn = g.probe_sums(i, nf)
+        oc, os_, on = sim.probe_sums(i, nf)
+        assert gn == on
+        assert np.array_equal(gc, oc) and np.array_equal(gs, os_), (i, gc, oc)
+    if sc.pml is not None:
+        for w in range(12):
+            _eq(g.psi(w), sim.psi(w), wf.PSI_NAMES[w])
+    ge, gh, gov = g.storage_info()
+    oe, oh = sim.shifts()
+    assert np.array_equal(ge, oe) and np.array_equal(gh, oh), (ge, oe, gh, oh)
+    assert gov == sim.storage_overflows
+
+
+@pytest.mark.parametrize("prec", ["f16", "bf16"])
+def test_cube64_matches_storage_emulation(oracle, prec):
+    """64^3 vacuum, CPML 16, Ricker at the centre, 300 steps."""
+    sc = configs.plain_cube_64(steps=300)
+    sim = oracle.sim_from_scenario(sc, storage=prec)
+    sim.step(sc.steps, NT)
+    g = _run(sc, prec)
+    try:
+        _compare(g, sim, sc)
+        assert np.any(g.fields())
+    finally:
+        g.close()
+
+
+@pytest.mark.parametrize("prec", ["f16", "bf16"])
+def test_ragged_grid_tilings_match_storage_emulation(oracle, prec):
+    """A ragged grid with lossy materials, four sources and probes on all six
+    components, under several tilings (z chunks crossing slab boundaries)."""
+    dims = wf.GridDims(136, 40, 24)
+    dx = 1e-3
+    dt = configs.courant_dt(dx)
+    grid = wf.MaterialGrid(dims)
+    table = wf.MaterialTable.vacuum_filled(dt, dx)
+    wf.Scene.parse("sphere 4.0 1.0 0.02 60 20 12 9\nbox 2.5 1.5 0.0 100 3 2 130 30 20\n"
+                   "sphere 1.7 1.0 0.0 7 35 20 6\n").voxelize(grid, table, dt, dx)
+    pml = wf.PmlContext.build(dims, wf.PmlConfig(thickness=8), dt, dx)
+    f = float(np.float32(3e8 / (15 * dx)))
+    srcs = [wf.Source(70, 21, 11, wf.FieldComponent.Ez, 1.0, wf.default_waveform("ricker", f)),
+            wf.Source(70, 21, 11, wf.FieldComponent.Ez, 0.5, wf.default_waveform("gaussian", f)),
+            wf.Source(3, 38, 1, wf.FieldComponent.Ex, 2.0, wf.default_waveform("sinusoid", f)),
+            wf.Source(135, 0, 23, wf.FieldComponent.Ey, 1.0, wf.default_waveform("ricker", f))]
+    prbs = [wf.Probe(90, 20, 12, wf.ProbeComponent(c), [f, 2 * f], 40 * dt) for c in range(6)]
+    sc = configs.Scenario("ragged", dims, dx, dt, grid, table, pml, srcs, prbs, 200)
+    sim = oracle.sim_from_scenario(sc, storage=prec)
+    sim.step(sc.steps, NT)
+    for tiling in ((4, 12, 3), (8, 24, 4), (4, 5, 4), (8, 64, 3)):
+        g = _run(sc, prec, tiling=tiling)
+        try:
+            _compare(g, sim, sc)
+        finally:
+            g.close()
+
+
+def test_random_spheres_128_f16_matches_emulation_and_fields_round_trip(oracle):
+    """The mixed-precision scene at 128^3 for 300 steps; then the FP32 view
+    (get_fields / snapshot) re-encodes losslessly into a fresh handle."""
+    sc = configs.random_spheres(128, steps=300)
+    sim = oracle.sim_from_scenario(sc, storage="f16")
+    sim.step(sc.steps, NT)
+    g = _run(sc, "f16")
+    try:
+        _compare(g, sim, sc)
+        assert np.array_equal(g.download_blocks(), sim.blocks())
+        f = g.fields()
+        g2 = configs.device_grid(sc, kernel="fused", precision="f16")
+        try:
+            g2.set_fields(f)
+            _eq(g2.fields(), f, "set_fields round trip")
+        finally:
+            g2.close()
+    finally:
+        g.close()
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_mixed_precision_error_vs_fp64(oracle):
+    """Relative L2 error of every field, and probe amplitude / phase error, of
+    the FP32, binary16 and bfloat16 storage forms against the FP64 oracle on
+    random spheres at 128^3 after 2000 steps.  The printed table is the
+    measured statement; the bounds hold it (the oracle's emulation of the
+    same storage gave about 2e-2 for binary16 and 1e-1 for bfloat16)."""
+    sc = configs.random_spheres(128, steps=2000)
+    ref = oracle.sim_from_scenario(sc, dtype="f64")
+    ref.step(sc.steps, NT)
+    fr = ref.fields()
+    pr = [ref.probe_sums(i, 1) for i in range(len(sc.probes))]
+    bounds = {"f32": (1e-5, 1e-6), "f16": (5e-2, 1e-3), "bf16": (3e-1, 1e-2)}
+    rows = []
+    for prec, (fb, pb) in bounds.items():
+        g = _run(sc, prec)
+        try:
+            f = g.fields().astype(np.float64)
+            ps = [g.probe_sums(i, 1) for i in range(len(sc.probes))]
+            ov = g.storage_info()[2]
+        finally:
+            g.close()
+        fe = [_rel(f[c], fr[c]) for c in range(6)]
+        amp, ph = [], []
+        for (c, s, n), (c0, s0, n0) in zip(ps, pr):
+            z, z0 = complex(c[0], s[0]), complex(c0[0], s0[0])
+            amp.append(abs(abs(z) - abs(z0)) / abs(z0))
+            ph.append(abs(np.angle(z / z0)))
+        rows.append((prec, fe, max(amp), max(ph), ov))
+    print("\nstorage  ex        ey        ez        hx        hy        hz        "
+          "probe|amp|  probe phase(rad)")
+    for prec, fe, a, p, _ in rows:
+        print(f"{prec:7s} " + " ".join(f"{e:.2e}" for e in fe) + f"  {a:.2e}    {p:.2e}")
+    for (prec, fe, a, p, ov), (fb, pb) in zip(rows, bounds.values()):
+        assert ov == 0, prec
+        assert max(fe) < fb, (prec, fe)
+        assert a < pb, (prec, a)

@@ -7,6 +7,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -57,7 +58,16 @@ struct wf_handle {
   int arith = WF_ARITH_EXACT;
   int kernel_pref = WF_KERNEL_AUTO;
   int precision = WF_PREC_F32;
-  float *fld[2] = {nullptr, nullptr};
+  float *fld[2] = {nullptr, nullptr};  // 16-bit elements unless precision is F32
+  // 16-bit storage: per state buffer the [nslab][2] shifts it is stored with,
+  // the slab maxima of the state being written, binary16 saturations, and
+  // whether the next step's shifts must be derived from the current state
+  int *shift[2] = {nullptr, nullptr};
+  unsigned *slab_max = nullptr;
+  unsigned long long *d_ovf = nullptr;
+  int nslab = 0;
+  bool shifts_dirty = true;
+  float kh = 0.0f, ke = 0.0f;  // 8 * max |Db|, 8 * max |Cb|
   int cur = 0;
   uint8_t *mat = nullptr;
   int mat_pitch = 0;
@@ -141,8 +151,11 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 bool fused_allowed(const wf_handle *h) {
-  return h->precision == WF_PREC_F32 && !h->periodic[0] && !h->periodic[1] && !h->periodic[2];
+  return !h->periodic[0] && !h->periodic[1] && !h->periodic[2];
 }
+
+bool store16(const wf_handle *h) { return h->precision != WF_PREC_F32; }
+size_t elem_bytes(const wf_handle *h) { return store16(h) ? 2 : 4; }
 
 bool use_fused(const wf_handle *h) {
   if (h->kernel_pref == WF_KERNEL_SPLIT) return false;
@@ -172,11 +185,16 @@ wf_status build_maps(wf_handle *h) {
   h->maps_ok = false;
   if (!encode_fn()) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   if (!h->cfg_user_set) h->cfg = FusedConfig{4, 12, 3};  // best measured at 512^3 on B200
+  if (store16(h) && !h->cfg_user_set) h->cfg = FusedConfig{4, 12, 4};
   unsigned eb[4], hb[4], mb[3];
-  wf::fused_boxes(h->cfg.ty, eb, hb, mb);
+  wf::fused_boxes(h->cfg.ty, h->precision, eb, hb, mb);
+  const cuuint64_t es = elem_bytes(h);
   const cuuint64_t fdim[4] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz, 6};
-  const cuuint64_t fstr[3] = {(cuuint64_t)h->nx * 4, (cuuint64_t)h->nx * h->ny * 4,
-                              (cuuint64_t)h->N * 4};
+  const cuuint64_t fstr[3] = {(cuuint64_t)h->nx * es, (cuuint64_t)h->nx * h->ny * es,
+                              (cuuint64_t)h->N * es};
+  const CUtensorMapDataType ft = h->precision == WF_PREC_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                 : h->precision == WF_PREC_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                                : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   const cuuint64_t mdim[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz};
   const cuuint64_t mstr[2] = {(cuuint64_t)h->mat_pitch, (cuuint64_t)h->mat_pitch * h->ny};
   const cuuint32_t ebox[4] = {eb[0], eb[1], eb[2], eb[3]};
@@ -185,12 +203,12 @@ wf_status build_maps(wf_handle *h) {
   for (int b = 0; b < 2; ++b) {
     wf::FusedMaps &m = h->maps[b];
     std::memset(&m, 0, sizeof(m));
-    if (!encode(&m.e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, ebox) ||
-        !encode(&m.h, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[b], fdim, fstr, hbox) ||
+    if (!encode(&m.e, ft, 4, h->fld[b], fdim, fstr, ebox) ||
+        !encode(&m.h, ft, 4, h->fld[b], fdim, fstr, hbox) ||
         !encode(&m.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->mat, mdim, mstr, mbox))
       return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(fields/ids) failed");
   }
-  WF_CUDA(h, wf::fused_prepare(h->cfg));
+  WF_CUDA(h, wf::fused_prepare(h->cfg, h->precision));
   // Work lists, one per kernel class (interior first): each class runs the
   // kernel instantiation that carries only the CPML code it needs.
   const FusedArgs a = fused_args(h);
@@ -238,7 +256,37 @@ GridArgs grid_args(const wf_handle *h) {
     g.pml[a].cells = A.cells;
   }
   g.err = h->d_err;
+  g.prec = h->precision;
+  g.shift_rd = h->shift[h->cur];
+  g.shift_wr = h->shift[h->cur ^ 1];
+  g.slab_max = h->slab_max;
+  g.ovf = h->d_ovf;
+  g.nslab = h->nslab;
   return g;
+}
+
+// Tail arguments of a step that reads buffer h->cur (16-bit fields included).
+TailArgs tail_args(const wf_handle *h) {
+  TailArgs t{};
+  t.f = h->fld[h->cur ^ 1];
+  t.nx = h->nx;
+  t.ny = h->ny;
+  t.nz = h->nz;
+  t.src = h->d_src;
+  t.nsrc = static_cast<int>(h->srcs.size());
+  t.probe = h->d_probe;
+  t.nprobe = static_cast<int>(h->probes.size());
+  t.step = h->d_step;
+  t.prec = h->precision;
+  t.shift_f = h->shift[h->cur ^ 1];
+  t.slab_max = h->slab_max;
+  t.shift_next = h->shift[h->cur];  // the next step reads cur ^ 1 and writes cur
+  t.nslab = h->nslab;
+  t.periodic_z = h->periodic[2];
+  t.kh = h->kh;
+  t.ke = h->ke;
+  t.ovf = h->d_ovf;
+  return t;
 }
 
 FusedArgs fused_args(const wf_handle *h) {
@@ -303,18 +351,9 @@ wf_status enqueue_one(wf_handle *h) {
     if (!ev) return fail(h, WF_ERR_CUDA, "cudaEventCreate");
     WF_CUDA(h, cudaEventRecord(ev, h->stream));
   }
-  if (!h->srcs.empty() || !h->probes.empty()) {
-    TailArgs t{};
-    t.f = h->fld[h->cur ^ 1];
-    t.nx = h->nx;
-    t.ny = h->ny;
-    t.nz = h->nz;
-    t.src = h->d_src;
-    t.nsrc = static_cast<int>(h->srcs.size());
-    t.probe = h->d_probe;
-    t.nprobe = static_cast<int>(h->probes.size());
-    t.step = h->d_step;
-    e = wf::launch_tail(t, h->stream);
+  // 16-bit storage always runs the tail: it picks the next step's shifts
+  if (!h->srcs.empty() || !h->probes.empty() || store16(h)) {
+    e = wf::launch_tail(tail_args(h), h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "tail kernel launch");
     h->kernel_launches += 1;
   }
@@ -322,8 +361,21 @@ wf_status enqueue_one(wf_handle *h) {
   return WF_OK;
 }
 
+// 16-bit storage: the slab maxima of the current state (from its data) and
+// the shifts the next step writes with.
+wf_status refresh_shifts(wf_handle *h) {
+  WF_CUDA(h, wf::launch_state_max(h->fld[h->cur], h->precision, h->nx, h->ny, h->nz,
+                                  h->shift[h->cur], h->slab_max, h->stream));
+  TailArgs t = tail_args(h);
+  t.shift_next = h->shift[h->cur ^ 1];  // the next step reads cur, writes cur ^ 1
+  WF_CUDA(h, wf::launch_next_shifts(t, h->steps_done, h->stream));
+  h->shifts_dirty = false;
+  return WF_OK;
+}
+
 wf_status upload_src_probe_tables(wf_handle *h) {
   drop_graphs(h);
+  h->shifts_dirty = true;  // source amplitudes enter the 16-bit shifts
   if (h->d_src) cudaFree(h->d_src);
   if (h->d_probe) cudaFree(h->d_probe);
   h->d_src = nullptr;
@@ -398,8 +450,18 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
                 "grid dimensions must be positive multiples of BLOCK_DIM (8)");
   if (d->arith != WF_ARITH_EXACT && d->arith != WF_ARITH_FMA)
     return fail(nullptr, WF_ERR_ARG, "unknown arith mode");
-  if (d->precision != WF_PREC_F32)
-    return fail(nullptr, WF_ERR_UNSUPPORTED, "only FP32 storage is available in this handle type");
+  if (d->precision != WF_PREC_F32 && d->precision != WF_PREC_F16 && d->precision != WF_PREC_BF16)
+    return fail(nullptr, WF_ERR_ARG, "unknown precision");
+  if (d->precision != WF_PREC_F32) {
+    // 16-bit storage: the fused kernel with the exact arithmetic, zero-field
+    // boundaries, and at most 1024 scale slabs along z
+    if (d->arith != WF_ARITH_EXACT)
+      return fail(nullptr, WF_ERR_UNSUPPORTED, "16-bit storage uses the exact arithmetic");
+    if (d->kernel == WF_KERNEL_SPLIT || d->boundary[0] || d->boundary[1] || d->boundary[2])
+      return fail(nullptr, WF_ERR_UNSUPPORTED,
+                  "16-bit storage runs the fused kernel (zero-field boundaries)");
+    if (d->nz / 8 > 1024) return fail(nullptr, WF_ERR_UNSUPPORTED, "16-bit storage: nz <= 8192");
+  }
   for (int i = 0; i < 3; ++i)
     if (d->boundary[i] != WF_BOUNDARY_ZERO && d->boundary[i] != WF_BOUNDARY_PERIODIC)
       return fail(nullptr, WF_ERR_ARG, "unknown boundary kind");
@@ -446,10 +508,23 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
   if ((e = cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup_fail(cuda_fail(nullptr, e, "cudaEventCreate"));
   for (int b = 0; b < 2; ++b) {
-    e = cudaMalloc(&h->fld[b], sizeof(float) * 6 * h->N);
+    e = cudaMalloc(&h->fld[b], elem_bytes(h) * 6 * h->N);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(fields)"));
-    e = cudaMemsetAsync(h->fld[b], 0, sizeof(float) * 6 * h->N, h->stream);
+    e = cudaMemsetAsync(h->fld[b], 0, elem_bytes(h) * 6 * h->N, h->stream);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMemset(fields)"));
+  }
+  if (store16(h)) {
+    h->nslab = h->nz / 8;
+    const size_t sb = sizeof(int) * 2 * h->nslab;
+    if ((e = cudaMalloc(&h->shift[0], sb)) != cudaSuccess ||
+        (e = cudaMalloc(&h->shift[1], sb)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->shift[0], 0, sb, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->shift[1], 0, sb, h->stream)) != cudaSuccess ||
+        (e = cudaMalloc(&h->slab_max, sb)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->slab_max, 0, sb, h->stream)) != cudaSuccess ||
+        (e = cudaMalloc(&h->d_ovf, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->d_ovf, 0, sizeof(unsigned long long), h->stream)) != cudaSuccess)
+      return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(storage scales)"));
   }
   const size_t mbytes = static_cast<size_t>(h->mat_pitch) * d->ny * d->nz;
   if ((e = cudaMalloc(&h->mat, mbytes)) != cudaSuccess ||
@@ -482,6 +557,9 @@ wf_status wf_destroy(wf_handle *h) {
   }
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   for (auto &f : h->fld) cudaFree(f);
+  for (auto &s : h->shift) cudaFree(s);
+  cudaFree(h->slab_max);
+  cudaFree(h->d_ovf);
   cudaFree(h->mat);
   cudaFree(h->coef);
   cudaFree(h->d_step);
@@ -510,9 +588,16 @@ wf_status wf_set_materials(wf_handle *h, const uint8_t *ids, const int32_t (*tab
   DeviceGuard guard(h->dev);
   // FixedQ16_16::to_f32 (src/layout.rs:123-125): q as f32 * (1/65536)
   float4 coef[256];
-  for (int m = 0; m < 256; ++m)
+  float cbmax = 0.0f, dbmax = 0.0f;
+  for (int m = 0; m < 256; ++m) {
     coef[m] = make_float4(wf_q16_to_f32(table[m][0]), wf_q16_to_f32(table[m][1]),
                           wf_q16_to_f32(table[m][2]), wf_q16_to_f32(table[m][3]));
+    cbmax = std::max(cbmax, std::fabs(coef[m].y));
+    dbmax = std::max(dbmax, std::fabs(coef[m].w));
+  }
+  h->kh = 8.0f * dbmax;  // 16-bit storage: E/H coupling of the shift bounds
+  h->ke = 8.0f * cbmax;
+  h->shifts_dirty = true;
   WF_CUDA(h, cudaMemcpyAsync(h->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, h->stream));
   WF_CUDA(h, cudaMemcpy2DAsync(h->mat, h->mat_pitch, ids, h->nx, h->nx,
                                static_cast<size_t>(h->ny) * h->nz, cudaMemcpyHostToDevice,
@@ -641,8 +726,15 @@ wf_status wf_step(wf_handle *h, int nsteps) {
   std::string why;
   if (!tables_cover(h, h->steps_done + nsteps, &why)) return fail(h, WF_ERR_ARG, why);
   DeviceGuard guard(h->dev);
+  if (store16(h) && !use_fused(h))
+    return fail(h, WF_ERR_UNSUPPORTED,
+                "16-bit storage runs the fused kernel only: CPML slabs of at most 64 cells");
   if (use_fused(h) && !h->maps_ok) {  // descriptors + smem limit, outside any capture
     wf_status s = build_maps(h);
+    if (s != WF_OK) return s;
+  }
+  if (store16(h) && h->shifts_dirty) {
+    wf_status s = refresh_shifts(h);
     if (s != WF_OK) return s;
   }
   // Long runs replay a captured graph of an even number of steps (the
@@ -719,10 +811,41 @@ wf_status wf_probe_trace(wf_handle *h, int p, float *out, int n) {
   return WF_OK;
 }
 
+// Device scratch of 6*N floats for 16-bit conversions (freed on scope exit).
+struct Scratch {
+  float *p = nullptr;
+  ~Scratch() { cudaFree(p); }
+};
+
+// FP32 SoA copy of the current 16-bit state into `tmp`.
+wf_status decode_current(wf_handle *h, Scratch &tmp) {
+  WF_CUDA(h, cudaMalloc(&tmp.p, sizeof(float) * 6 * h->N));
+  WF_CUDA(h, wf::launch_decode_state(h->fld[h->cur], tmp.p, h->precision, h->nx, h->ny, h->nz,
+                                     h->shift[h->cur], h->stream));
+  return WF_OK;
+}
+
+// Encodes the FP32 SoA state at device pointer `src` as the current state.
+wf_status encode_current(wf_handle *h, const float *src) {
+  WF_CUDA(h, wf::launch_encode_state(src, h->fld[h->cur], h->precision, h->nx, h->ny, h->nz,
+                                     h->shift[h->cur], h->slab_max, h->d_ovf, h->stream));
+  h->shifts_dirty = true;
+  return WF_OK;
+}
+
 wf_status wf_get_fields(wf_handle *h, float *out6) {
   if (!h || !out6) return fail(h, WF_ERR_ARG, "null argument");
   DeviceGuard guard(h->dev);
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (store16(h)) {
+    Scratch tmp;
+    wf_status s = decode_current(h, tmp);
+    if (s != WF_OK) return s;
+    WF_CUDA(h, cudaMemcpyAsync(out6, tmp.p, sizeof(float) * 6 * h->N, cudaMemcpyDeviceToHost,
+                               h->stream));
+    WF_CUDA(h, cudaStreamSynchronize(h->stream));
+    return WF_OK;
+  }
   WF_CUDA(h, cudaMemcpy(out6, h->fld[h->cur], sizeof(float) * 6 * h->N, cudaMemcpyDeviceToHost));
   return WF_OK;
 }
@@ -731,6 +854,16 @@ wf_status wf_set_fields(wf_handle *h, const float *in6) {
   if (!h || !in6) return fail(h, WF_ERR_ARG, "null argument");
   DeviceGuard guard(h->dev);
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (store16(h)) {
+    Scratch tmp;
+    WF_CUDA(h, cudaMalloc(&tmp.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, cudaMemcpyAsync(tmp.p, in6, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice,
+                               h->stream));
+    wf_status s = encode_current(h, tmp.p);
+    if (s != WF_OK) return s;
+    WF_CUDA(h, cudaStreamSynchronize(h->stream));
+    return WF_OK;
+  }
   WF_CUDA(h, cudaMemcpy(h->fld[h->cur], in6, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice));
   return WF_OK;
 }
@@ -738,6 +871,17 @@ wf_status wf_set_fields(wf_handle *h, const float *in6) {
 wf_status wf_download_blocks(wf_handle *h, void *out) {
   if (!h || !out) return fail(h, WF_ERR_ARG, "null argument");
   DeviceGuard guard(h->dev);
+  if (store16(h)) {  // decode, then reorder into a second scratch buffer
+    Scratch soa, blk;
+    wf_status s = decode_current(h, soa);
+    if (s != WF_OK) return s;
+    WF_CUDA(h, cudaMalloc(&blk.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, wf::launch_soa_to_blocks(soa.p, blk.p, h->nx, h->ny, h->nz, h->stream));
+    WF_CUDA(h, cudaMemcpyAsync(out, blk.p, sizeof(float) * 6 * h->N, cudaMemcpyDeviceToHost,
+                               h->stream));
+    WF_CUDA(h, cudaStreamSynchronize(h->stream));
+    return WF_OK;
+  }
   // the next-state buffer is dead between steps: use it to reorder
   float *tmp = h->fld[h->cur ^ 1];
   WF_CUDA(h, wf::launch_soa_to_blocks(h->fld[h->cur], tmp, h->nx, h->ny, h->nz, h->stream));
@@ -749,6 +893,18 @@ wf_status wf_download_blocks(wf_handle *h, void *out) {
 wf_status wf_upload_blocks(wf_handle *h, const void *in) {
   if (!h || !in) return fail(h, WF_ERR_ARG, "null argument");
   DeviceGuard guard(h->dev);
+  if (store16(h)) {
+    Scratch blk, soa;
+    WF_CUDA(h, cudaMalloc(&blk.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, cudaMalloc(&soa.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, cudaMemcpyAsync(blk.p, in, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice,
+                               h->stream));
+    WF_CUDA(h, wf::launch_blocks_to_soa(blk.p, soa.p, h->nx, h->ny, h->nz, h->stream));
+    wf_status s = encode_current(h, soa.p);
+    if (s != WF_OK) return s;
+    WF_CUDA(h, cudaStreamSynchronize(h->stream));
+    return WF_OK;
+  }
   float *tmp = h->fld[h->cur ^ 1];
   WF_CUDA(h, cudaMemcpyAsync(tmp, in, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice, h->stream));
   WF_CUDA(h, wf::launch_blocks_to_soa(tmp, h->fld[h->cur], h->nx, h->ny, h->nz, h->stream));
@@ -788,8 +944,36 @@ wf_status wf_get_psi(wf_handle *h, int which, float *out) {
   return WF_OK;
 }
 
+wf_status wf_storage_info(wf_handle *h, int *shift_e, int *shift_h, uint64_t *overflows) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  if (!store16(h)) {
+    if (overflows) *overflows = 0;
+    return WF_OK;
+  }
+  DeviceGuard guard(h->dev);
+  if (h->shifts_dirty) {
+    wf_status s = refresh_shifts(h);
+    if (s != WF_OK) return s;
+  }
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::vector<int> sh(2 * h->nslab);
+  WF_CUDA(h, cudaMemcpy(sh.data(), h->shift[h->cur ^ 1], sizeof(int) * sh.size(),
+                        cudaMemcpyDeviceToHost));
+  for (int b = 0; b < h->nslab; ++b) {
+    if (shift_e) shift_e[b] = sh[2 * b];
+    if (shift_h) shift_h[b] = sh[2 * b + 1];
+  }
+  if (overflows) {
+    unsigned long long v = 0;
+    WF_CUDA(h, cudaMemcpy(&v, h->d_ovf, sizeof(v), cudaMemcpyDeviceToHost));
+    *overflows = v;
+  }
+  return WF_OK;
+}
+
 wf_status wf_device_fields(wf_handle *h, float **out6) {
   if (!h || !out6) return fail(h, WF_ERR_ARG, "null argument");
+  if (store16(h)) return fail(h, WF_ERR_UNSUPPORTED, "device FP32 fields need FP32 storage");
   for (int c = 0; c < 6; ++c) out6[c] = h->fld[h->cur] + c * h->N;
   return WF_OK;
 }
@@ -835,7 +1019,7 @@ wf_status wf_get_tiling(const wf_handle *h, wf_tiling *out) {
 wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t) {
   if (!h || !t) return fail(h, WF_ERR_ARG, "null argument");
   FusedConfig c{t->tile_rows, t->z_chunk, t->stages};
-  if (!wf::fused_supported(c)) return fail(h, WF_ERR_ARG, "tiling not instantiated");
+  if (!wf::fused_supported(c, h->precision)) return fail(h, WF_ERR_ARG, "tiling not instantiated");
   DeviceGuard guard(h->dev);
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   drop_graphs(h);
@@ -866,7 +1050,7 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) 
     for (int s : stg)
       for (int zc : zcs) {
         FusedConfig c{ty, std::min(zc, h->nz), s};
-        if (wf::fused_supported(c)) cands.push_back(c);
+        if (wf::fused_supported(c, h->precision)) cands.push_back(c);
       }
   cudaEvent_t e0, e1;
   WF_CUDA(h, cudaEventCreate(&e0));
@@ -910,6 +1094,10 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) 
     for (int k = 0; k < 2; ++k)
       if (A.psi[k]) WF_CUDA(h, cudaMemset(A.psi[k], 0, sizeof(float) * 4 * A.cells));
   WF_CUDA(h, cudaMemset(h->d_err, 0, sizeof(int)));
+  if (store16(h)) {  // the trial steps ran the 16-bit tail: rewind its counters
+    WF_CUDA(h, cudaMemset(h->d_step, 0, sizeof(long long)));
+    WF_CUDA(h, cudaMemset(h->d_ovf, 0, sizeof(unsigned long long)));
+  }
   if (best) {
     best->tile_rows = bc.ty;
     best->z_chunk = bc.zchunk;

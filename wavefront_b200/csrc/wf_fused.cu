@@ -1,632 +1,18 @@
-// wf_fused.cu -- one-pass fused H->E Yee step for sm_100a.
-//
-// Replaces, for zero-field boundaries, one whole step_all_slabs call of the
-// reference (src/engine.rs:291-422: an H phase over every 8^3 block with
-// update_h_field[_pml], a barrier, then an E phase with update_e_field[_pml])
-// with a single kernel in which every field value crosses HBM once:
-//
-//  * a CTA owns a 128 x TY column of cells and marches it through a chunk of
-//    z planes;
-//  * plane p's E box (tile + 1-cell halo), H box (tile + -x/-y halo) and the
-//    material-id box are staged into shared memory by TMA
-//    (cp.async.bulk.tensor, no multicast) through an S-deep mbarrier ring;
-//    out-of-domain box cells arrive as zeros, which is exactly the
-//    reference's OUTER_ZERO_BLOCK (src/engine.rs:83);
-//  * H of plane p is computed for the tile plus the -x column and -y row
-//    the E update needs (recomputed, never exchanged between CTAs), E of
-//    plane p follows at once from registers and a shared-memory H plane;
-//    the -z neighbour H(p-1) rides along in registers (register-rotated z);
-//  * the state is double-buffered: the kernel reads buffer `cur` and writes
-//    buffer `nxt`, so halo recomputation never races a neighbour's writes;
-//  * CPML: interior CTAs run a body with no CPML code.  CTAs whose tile,
-//    halo or z chunk meets a graded slab treat each lane's 4 cells as one
-//    vector: the y and z slab flags are uniform per warp and per plane, the
-//    x slab flag per lane, psi moves as float4, and each phase's psi loads
-//    are issued before the work that precedes their use (the H terms before
-//    the stage wait, the E terms before the barrier) so their latency
-//    overlaps it.
-//
-// All per-cell arithmetic goes through wf_internal.cuh, so results are
-// bit-identical to the split kernels and to the reference.
-#include <algorithm>
-
-#include "wf_internal.cuh"
-#include "wf_launch.h"
+// wf_fused.cu -- FP32-storage instantiations of the fused step kernel
+// (wf_fused_impl.cuh) and the host-side dispatch of every storage type:
+// work-item classes, TMA box shapes, tiling support and launches.  The 16-bit
+// instantiations live in wf_fused16.cu so the two compile in parallel.
+#include "wf_fused_impl.cuh"
 
 namespace wf {
 
-namespace {
+// (tile rows, stages) combinations instantiated for FP32 storage
+#define WF_FUSED_CONFIGS(X) X(4, 3) X(4, 4) X(8, 3) X(8, 4) X(16, 3)
 
-constexpr int kProfSmem = 3 * 3 * 64;  // floats: 3 axes x {b, a, 1/kappa} x 64 positions
-
-template <int TY, int S>
-struct Layout {
-  static constexpr int EW = kTileX + 8, EH = TY + 2;   // E box: x0-4..x0+131, y0-1..y0+TY
-  static constexpr int HW = kTileX + 4, HH = TY + 1;   // H box: x0-4..x0+127, y0-1..y0+TY-1
-  static constexpr int MW = kTileX + 16, MH = TY + 1;  // ids:   x0-16..x0+127
-  static constexpr int E_BYTES = 3 * EH * EW * 4;
-  static constexpr int H_BYTES = 3 * HH * HW * 4;
-  static constexpr int M_BYTES = MH * MW;
-  static constexpr int al(int v) { return (v + 127) / 128 * 128; }
-  static constexpr int H_OFF = al(E_BYTES);
-  static constexpr int M_OFF = H_OFF + al(H_BYTES);
-  static constexpr int STAGE = M_OFF + al(M_BYTES);
-  static constexpr int STAGE_OFF = 4096;  // after the 256-entry float4 coefficient table
-  static constexpr int PROWS = TY + 1;    // plane rows: 0 = y0-1, 1..TY = tile rows
-  static constexpr int PLANE_FLOATS = 2 * PROWS * kTileX + 64;  // hz, hx rows; x-halo hz, hy
-  static constexpr int PLANE_OFF = STAGE_OFF + S * STAGE;
-  static constexpr int PROF_OFF = PLANE_OFF + 2 * PLANE_FLOATS * 4;  // CPML profiles
-  static constexpr int BAR_OFF = PROF_OFF + kProfSmem * 4;
-  static constexpr int BYTES = BAR_OFF + S * 8 + 128;  // +128: base alignment slack
-  static constexpr int THREADS = 32 * (TY + 1);
-  static_assert(TY + 1 <= 32, "x-halo column is handled by one warp");
-};
-
-__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
-__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
-__device__ __forceinline__ void stg4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
-__device__ __forceinline__ float &el(float4 &v, int q) {
-  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
-}
-__device__ __forceinline__ float comp(const float4 &v, int q) {
-  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
-}
-
-// CPML geometry of one lane's 4 cells at one plane.
-struct LanePml {
-  bool y, z;        // row in the y slab / plane in the z slab (warp / CTA uniform)
-  int xmode;        // 0: no cell in the x slab; 1: all 4, aligned (vector); 2: per cell
-  long long iy, iz, ix;  // psi index of the lane's first cell (y, z, x-vector)
-  int sy, sz, sx;        // slab positions (x: of the first cell)
-};
-
-// The plane-independent part of a lane's CPML geometry (computed once per
-// CTA): its x-slab mode and position, and its row's y-slab position.
-struct LaneConst {
-  int xmode, sx, sy;
-};
-
-// AX: bit mask of the CPML axes (1 x, 2 y, 4 z) the calling kernel handles.
-template <int AX>
-__device__ __forceinline__ LaneConst lane_const(const GridArgs &g, int xg, int y, bool cell_ok) {
-  LaneConst c{0, -1, -1};
-  if (!cell_ok) return c;
-  const PmlAxis &X = g.pml[0], &Y = g.pml[1];
-  if (AX & 2) c.sy = slab_pos(y, g.ny, Y.T, Y.W);
-  if ((AX & 1) && X.T > 0) {
-    const int s0 = slab_pos(xg, g.nx, X.T, X.W), s3 = slab_pos(xg + 3, g.nx, X.T, X.W);
-    const int s1 = slab_pos(xg + 1, g.nx, X.T, X.W), s2 = slab_pos(xg + 2, g.nx, X.T, X.W);
-    if (s0 >= 0 && s3 == s0 + 3 && (s0 & 3) == 0) {
-      c.xmode = 1;
-      c.sx = s0;
-    } else if (s0 >= 0 || s1 >= 0 || s2 >= 0 || s3 >= 0) {
-      c.xmode = 2;
-    }
-  }
-  return c;
-}
-
-template <int AX>
-__device__ __forceinline__ LanePml lane_pml(const GridArgs &g, const LaneConst &c, int xg, int y,
-                                            int p) {
-  LanePml L{};
-  if (AX & 2) {
-    L.sy = c.sy;
-    L.y = c.sy >= 0;
-    if (L.y) L.iy = (static_cast<long long>(p) * g.pml[1].W + c.sy) * g.nx + xg;
-  }
-  if (AX & 4) {
-    const PmlAxis &Z = g.pml[2];
-    L.sz = slab_pos(p, g.nz, Z.T, Z.W);
-    L.z = L.sz >= 0;
-    if (L.z) L.iz = (static_cast<long long>(L.sz) * g.ny + y) * g.nx + xg;
-  }
-  if (AX & 1) {
-    L.xmode = c.xmode;
-    L.sx = c.sx;
-    if (c.xmode == 1) L.ix = (static_cast<long long>(p) * g.ny + y) * g.pml[0].pitch + c.sx;
-  }
-  return L;
-}
-
-// The two psi terms of one axis for a lane's 4 cells (float4 each).
-struct Psi2 {
-  float4 p0, p1;
-};
-
-// The H-term psi of the -x halo cell on each axis (slab position, or -1).
-struct HaloPsi {
-  int sx, sy, sz;
-  float x0, x1, y0, y1, z0, z1;
-};
-
-__device__ __forceinline__ Psi2 load_psi2(const PmlAxis &P, int comp0, long long idx) {
-  return Psi2{ldg4(P.psi_cur + comp0 * P.cells + idx), ldg4(P.psi_cur + (comp0 + 1) * P.cells + idx)};
-}
-
-// psi recursion of one axis over 4 cells with one coefficient set (y, z).
-template <bool FMA>
-__device__ __forceinline__ void corr4_uniform(float d0[4], float d1[4], Psi2 &q, float b, float a,
-                                              float ik) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    d0[i] = pml_corr<FMA>(d0[i], b, a, ik, el(q.p0, i));
-    d1[i] = pml_corr<FMA>(d1[i], b, a, ik, el(q.p1, i));
-  }
-}
-
-// CPML profiles (b, a, 1/kappa at slab positions) as the body reads them:
-// a shared-memory copy when every axis's slab fits kProfCap positions,
-// otherwise the global arrays.
-constexpr int kProfCap = kProfSmem / 9;
-struct Prof {
-  const float *p;  // shared memory: [3 axes][b, a, 1/kappa][kProfCap]
-  __device__ __forceinline__ float b(int ax, int s) const { return p[ax * 3 * kProfCap + s]; }
-  __device__ __forceinline__ float a(int ax, int s) const { return p[(ax * 3 + 1) * kProfCap + s]; }
-  __device__ __forceinline__ float ik(int ax, int s) const { return p[(ax * 3 + 2) * kProfCap + s]; }
-};
-
-// x axis: per-cell coefficients at slab positions s0..s0+3.
-template <bool FMA>
-__device__ __forceinline__ void corr4_x(float d0[4], float d1[4], Psi2 &q, const Prof &pf, int s0) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float b = pf.b(0, s0 + i), a = pf.a(0, s0 + i), ik = pf.ik(0, s0 + i);
-    d0[i] = pml_corr<FMA>(d0[i], b, a, ik, el(q.p0, i));
-    d1[i] = pml_corr<FMA>(d1[i], b, a, ik, el(q.p1, i));
-  }
-}
-
-// x axis, one cell at a time (lanes straddling a slab edge, the x-halo cell).
-template <bool FMA>
-__device__ __forceinline__ void corr_x_cell(const GridArgs &g, const Prof &pf, int comp0, int x,
-                                            int y, int p, float &d0, float &d1, bool store) {
-  const PmlAxis &P = g.pml[0];
-  const int s = slab_pos(x, g.nx, P.T, P.W);
-  if (s < 0) return;
-  const long long idx = (static_cast<long long>(p) * g.ny + y) * P.pitch + s;
-  float p0 = __ldg(P.psi_cur + comp0 * P.cells + idx), p1 = __ldg(P.psi_cur + (comp0 + 1) * P.cells + idx);
-  const float b = pf.b(0, s), a = pf.a(0, s), ik = pf.ik(0, s);
-  d0 = pml_corr<FMA>(d0, b, a, ik, p0);
-  d1 = pml_corr<FMA>(d1, b, a, ik, p1);
-  if (store) {
-    P.psi_nxt[comp0 * P.cells + idx] = p0;
-    P.psi_nxt[(comp0 + 1) * P.cells + idx] = p1;
-  }
-}
-
-// y or z axis, one cell (the x-halo cell).
-template <bool FMA>
-__device__ __forceinline__ void corr_yz_cell(const GridArgs &g, const Prof &pf, int axis, int x,
-                                             int y, int p, float &d0, float &d1) {
-  const PmlAxis &P = g.pml[axis];
-  const int s = axis == 1 ? slab_pos(y, g.ny, P.T, P.W) : slab_pos(p, g.nz, P.T, P.W);
-  if (s < 0) return;
-  const long long idx = axis == 1 ? (static_cast<long long>(p) * P.W + s) * g.nx + x
-                                  : (static_cast<long long>(s) * g.ny + y) * g.nx + x;
-  float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
-  const float b = pf.b(axis, s), a = pf.a(axis, s), ik = pf.ik(axis, s);
-  d0 = pml_corr<FMA>(d0, b, a, ik, p0);
-  d1 = pml_corr<FMA>(d1, b, a, ik, p1);
-}
-
-// AX: the CPML axes this body handles (bit 1 x, 2 y, 4 z; 0 = interior).
-template <int TY, int S, bool FMA, int AX>
-__device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtensorMap *tmH,
-                                           const CUtensorMap *tmM, const FusedArgs &a,
-                                           unsigned char *smem, int x0, int y0, int k0, int k1) {
-  using L = Layout<TY, S>;
-  constexpr bool PML = AX != 0;
-  constexpr bool AXX = (AX & 1) != 0, AXY = (AX & 2) != 0, AXZ = (AX & 4) != 0;
-  const GridArgs &g = a.g;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const float4 *s_coef = reinterpret_cast<const float4 *>(smem);
-  unsigned char *s_stage = smem + L::STAGE_OFF;
-  float *s_plane = reinterpret_cast<float *>(smem + L::PLANE_OFF);
-  uint64_t *s_bar = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
-
-  const int nx = g.nx, ny = g.ny;
-  const long long N = g.N;
-  const int kfirst = k0 > 0 ? k0 - 1 : 0;  // k0-1: warm-up plane for H(k0-1)
-  const int np = k1 - kfirst + 1;          // planes staged; plane k1 brings only E
-
-  auto issue = [&](int j) {
-    const int p = kfirst + j;
-    const int slot = j % S;
-    unsigned char *st = s_stage + slot * L::STAGE;
-    const uint32_t bar = smem_u32(&s_bar[slot]);
-    const bool e_only = (p == k1);
-    mbar_expect_tx(bar, e_only ? L::E_BYTES : (L::E_BYTES + L::H_BYTES + L::M_BYTES));
-    tma_load_4d(smem_u32(st), tmE, x0 - 4, y0 - 1, p, 0, bar);
-    if (!e_only) {
-      tma_load_4d(smem_u32(st + L::H_OFF), tmH, x0 - 4, y0 - 1, p, 3, bar);
-      tma_load_3d(smem_u32(st + L::M_OFF), tmM, x0 - 16, y0 - 1, p, bar);
-    }
-  };
-
-  int issued = 0;
-  if (tid == 0) {
-    const int pro = np < S ? np : S;
-    for (int j = 0; j < pro; ++j) issue(j);
-    issued = pro;
-  }
-  bool ok = mbar_wait(smem_u32(&s_bar[0]), 0);
-  int done = ok ? 1 : 0;  // stages [0, done) seen complete, in order
-
-  const bool tile_warp = warp < TY;
-  const int r = tile_warp ? warp + 1 : 0;  // smem row: 0 is the -y halo row y0-1
-  const int y = y0 - 1 + r;
-  const int xg = x0 + 4 * lane;
-  const bool row_in = (y >= 0) && (y < ny);
-  const bool x_in = xg < nx;  // nx % 8 == 0: a lane's 4 cells are all in or all out
-  const bool cell_ok = row_in && x_in;
-  const int cE = 4 + 4 * lane;
-  float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;  // H(p-1), own cells
-
-  const Prof pf{reinterpret_cast<const float *>(smem + L::PROF_OFF)};
-  const LaneConst lc = lane_const<AX>(g, xg, y, cell_ok);
-  // CPML: each plane's H-term psi is loaded one plane ahead (the first plane's
-  // here), so its latency hides behind a whole plane of work.
-  LanePml lp_n{};
-  Psi2 qx_n{}, qy_n{}, qz_n{};
-  auto prefetch = [&](int pp) {
-    lp_n = lane_pml<AX>(g, lc, xg, y, pp);
-    if (AXY && lp_n.y) qy_n = load_psi2(g.pml[1], 0, lp_n.iy);
-    if (AXZ && lp_n.z) qz_n = load_psi2(g.pml[2], 0, lp_n.iz);
-    if (AXX && lp_n.xmode == 1) qx_n = load_psi2(g.pml[0], 0, lp_n.ix);
-  };
-  // ... and so is the H-term psi of the -x halo cell (x0-1, y0+lane) that
-  // lanes 0..TY-1 of the halo warp update.
-  const bool xhalo = PML && !tile_warp && lane < TY && x0 > 0 && y0 + lane < ny;
-  HaloPsi hh_n{-1, -1, -1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  auto prefetch_halo = [&](int pp) {
-    const int xh = x0 - 1, yh = y0 + lane;
-    if (AXX) {
-      const PmlAxis &P = g.pml[0];
-      hh_n.sx = slab_pos(xh, nx, P.T, P.W);
-      if (hh_n.sx >= 0) {
-        const long long i = (static_cast<long long>(pp) * ny + yh) * P.pitch + hh_n.sx;
-        hh_n.x0 = __ldg(P.psi_cur + i);
-        hh_n.x1 = __ldg(P.psi_cur + P.cells + i);
-      }
-    }
-    if (AXY) {
-      const PmlAxis &P = g.pml[1];
-      hh_n.sy = slab_pos(yh, ny, P.T, P.W);
-      if (hh_n.sy >= 0) {
-        const long long i = (static_cast<long long>(pp) * P.W + hh_n.sy) * nx + xh;
-        hh_n.y0 = __ldg(P.psi_cur + i);
-        hh_n.y1 = __ldg(P.psi_cur + P.cells + i);
-      }
-    }
-    if (AXZ) {
-      const PmlAxis &P = g.pml[2];
-      hh_n.sz = slab_pos(pp, g.nz, P.T, P.W);
-      if (hh_n.sz >= 0) {
-        const long long i = (static_cast<long long>(hh_n.sz) * ny + yh) * nx + xh;
-        hh_n.z0 = __ldg(P.psi_cur + i);
-        hh_n.z1 = __ldg(P.psi_cur + P.cells + i);
-      }
-    }
-  };
-  if (PML && cell_ok) prefetch(kfirst);
-  if (xhalo) prefetch_halo(kfirst);
-
-  for (int j = 0; j < np - 1; ++j) {
-    const int p = kfirst + j;
-    const bool warm = p < k0;
-    const bool active = tile_warp || !warm;  // the halo warp idles on the warm-up plane
-    const LanePml lp = lp_n;
-    Psi2 qx = qx_n, qy = qy_n, qz = qz_n;
-    HaloPsi hh = hh_n;  // (pml_corr updates its psi argument in place)
-
-    const bool arrived = mbar_wait(smem_u32(&s_bar[(j + 1) % S]), ((j + 1) / S) & 1);
-    if (arrived && done == j + 1) done = j + 2;
-    ok = arrived && ok;
-    const unsigned char *stc = s_stage + (j % S) * L::STAGE;
-    const float *Ec = reinterpret_cast<const float *>(stc);
-    const float *En = reinterpret_cast<const float *>(s_stage + ((j + 1) % S) * L::STAGE);
-    const float *Hc = reinterpret_cast<const float *>(stc + L::H_OFF);
-    const uint8_t *Mc = stc + L::M_OFF;
-    float *pl = s_plane + (p & 1) * L::PLANE_FLOATS;
-    float *pl_hz = pl, *pl_hx = pl + L::PROWS * kTileX;
-    float *pl_hzh = pl + 2 * L::PROWS * kTileX, *pl_hyh = pl_hzh + 32;
-
-    // ---------------- H phase (update_h_field[_pml], src/fdtd.rs:194-345) ----
-    float ha[4], hb[4], hc[4];  // new hx, hy, hz of this lane's 4 cells
-    float4 ex4, ey4, ez4;
-    uchar4 m4;
-    Psi2 ex_{}, ey_{}, ez_{};  // E-term psi (x, y, z axes), loaded before the barrier
-    if (active) {
-      auto E4 = [&](const float *B, int c, int row) { return lds4(B + (c * L::EH + row) * L::EW + cE); };
-      ex4 = E4(Ec, 0, r);
-      ey4 = E4(Ec, 1, r);
-      ez4 = E4(Ec, 2, r);
-      const float4 ex_py = E4(Ec, 0, r + 1), ez_py = E4(Ec, 2, r + 1);
-      const float4 ex_pz = E4(En, 0, r), ey_pz = E4(En, 1, r);
-      float ez_n = __shfl_down_sync(0xffffffffu, ez4.x, 1);
-      float ey_n = __shfl_down_sync(0xffffffffu, ey4.x, 1);
-      if (lane == 31) {
-        ez_n = Ec[(2 * L::EH + r) * L::EW + 4 + kTileX];
-        ey_n = Ec[(1 * L::EH + r) * L::EW + 4 + kTileX];
-      }
-      const float4 hx4 = lds4(Hc + (0 * L::HH + r) * L::HW + cE);
-      const float4 hy4 = lds4(Hc + (1 * L::HH + r) * L::HW + cE);
-      const float4 hz4 = lds4(Hc + (2 * L::HH + r) * L::HW + cE);
-      m4 = *reinterpret_cast<const uchar4 *>(Mc + r * L::MW + 16 + 4 * lane);
-
-      float d_ez_dy[4], d_ex_dy[4], d_ey_dz[4], d_ex_dz[4], d_ez_dx[4], d_ey_dx[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        d_ez_dy[q] = sub(comp(ez_py, q), comp(ez4, q));
-        d_ex_dy[q] = sub(comp(ex_py, q), comp(ex4, q));
-        d_ey_dz[q] = sub(comp(ey_pz, q), comp(ey4, q));
-        d_ex_dz[q] = sub(comp(ex_pz, q), comp(ex4, q));
-        d_ez_dx[q] = sub(q < 3 ? comp(ez4, q + 1) : ez_n, comp(ez4, q));
-        d_ey_dx[q] = sub(q < 3 ? comp(ey4, q + 1) : ey_n, comp(ey4, q));
-      }
-      if (PML && cell_ok) {  // CPML on the H terms (pml_correct_*, src/fdtd.rs:136-163)
-        const bool wpsi = tile_warp && !warm;
-        if (AXX && lp.xmode == 1) {
-          corr4_x<FMA>(d_ez_dx, d_ey_dx, qx, pf, lp.sx);
-          if (wpsi) {
-            const PmlAxis &P = g.pml[0];
-            stg4(P.psi_nxt + lp.ix, qx.p0);
-            stg4(P.psi_nxt + P.cells + lp.ix, qx.p1);
-          }
-        } else if (AXX && lp.xmode == 2) {
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            corr_x_cell<FMA>(g, pf, 0, xg + q, y, p, d_ez_dx[q], d_ey_dx[q], wpsi);
-        }
-        if (AXY && lp.y) {
-          corr4_uniform<FMA>(d_ez_dy, d_ex_dy, qy, pf.b(1, lp.sy), pf.a(1, lp.sy), pf.ik(1, lp.sy));
-          if (wpsi) {
-            const PmlAxis &P = g.pml[1];
-            stg4(P.psi_nxt + lp.iy, qy.p0);
-            stg4(P.psi_nxt + P.cells + lp.iy, qy.p1);
-          }
-        }
-        if (AXZ && lp.z) {
-          corr4_uniform<FMA>(d_ey_dz, d_ex_dz, qz, pf.b(2, lp.sz), pf.a(2, lp.sz), pf.ik(2, lp.sz));
-          if (wpsi) {
-            const PmlAxis &P = g.pml[2];
-            stg4(P.psi_nxt + lp.iz, qz.p0);
-            stg4(P.psi_nxt + P.cells + lp.iz, qz.p1);
-          }
-        }
-        if (wpsi) {  // the E terms' psi: in flight across the barrier
-          if (AXX && lp.xmode == 1) ex_ = load_psi2(g.pml[0], 2, lp.ix);
-          if (AXY && lp.y) ey_ = load_psi2(g.pml[1], 2, lp.iy);
-          if (AXZ && lp.z) ez_ = load_psi2(g.pml[2], 2, lp.iz);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const unsigned char id = q == 0 ? m4.x : (q == 1 ? m4.y : (q == 2 ? m4.z : m4.w));
-        const float4 cf = s_coef[id];
-        ha[q] = h_new<FMA>(cf.z, comp(hx4, q), cf.w, sub(d_ez_dy[q], d_ey_dz[q]));
-        hb[q] = h_new<FMA>(cf.z, comp(hy4, q), cf.w, sub(d_ex_dz[q], d_ez_dx[q]));
-        hc[q] = h_new<FMA>(cf.z, comp(hz4, q), cf.w, sub(d_ey_dx[q], d_ex_dy[q]));
-      }
-      if (!row_in) {  // outside the domain in y: zero field (OUTER_ZERO_BLOCK)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) ha[q] = hb[q] = hc[q] = 0.0f;
-      }
-      if (!warm) {
-        stg4(pl_hz + r * kTileX + 4 * lane, make_float4(hc[0], hc[1], hc[2], hc[3]));
-        stg4(pl_hx + r * kTileX + 4 * lane, make_float4(ha[0], ha[1], ha[2], ha[3]));
-        if (tile_warp && cell_ok) {
-          float *Hn = g.nxt + 3 * N + (static_cast<long long>(p) * ny + y) * nx + xg;
-          stg4(Hn, make_float4(ha[0], ha[1], ha[2], ha[3]));
-          stg4(Hn + N, make_float4(hb[0], hb[1], hb[2], hb[3]));
-          stg4(Hn + 2 * N, make_float4(hc[0], hc[1], hc[2], hc[3]));
-        }
-      }
-      // -x halo column (x0-1, y0..y0+TY-1): Hz and Hy for the E update at x0
-      if (!tile_warp && !warm && lane < TY) {
-        const int rh = lane + 1, yh = y0 + lane, xh = x0 - 1;
-        float hzv = 0.0f, hyv = 0.0f;
-        if (x0 > 0 && yh < ny) {
-          const float ex = Ec[(0 * L::EH + rh) * L::EW + 3];
-          const float ey = Ec[(1 * L::EH + rh) * L::EW + 3];
-          const float ez = Ec[(2 * L::EH + rh) * L::EW + 3];
-          float d_ez_dx1 = sub(Ec[(2 * L::EH + rh) * L::EW + 4], ez);
-          float d_ey_dx1 = sub(Ec[(1 * L::EH + rh) * L::EW + 4], ey);
-          float d_ex_dz1 = sub(En[(0 * L::EH + rh) * L::EW + 3], ex);
-          float d_ey_dz1 = sub(En[(1 * L::EH + rh) * L::EW + 3], ey);
-          float d_ex_dy1 = sub(Ec[(0 * L::EH + rh + 1) * L::EW + 3], ex);
-          float d_ez_dy1 = sub(Ec[(2 * L::EH + rh + 1) * L::EW + 3], ez);
-          if (AXX && hh.sx >= 0) {
-            d_ez_dx1 = pml_corr<FMA>(d_ez_dx1, pf.b(0, hh.sx), pf.a(0, hh.sx), pf.ik(0, hh.sx), hh.x0);
-            d_ey_dx1 = pml_corr<FMA>(d_ey_dx1, pf.b(0, hh.sx), pf.a(0, hh.sx), pf.ik(0, hh.sx), hh.x1);
-          }
-          if (AXY && hh.sy >= 0) {
-            d_ez_dy1 = pml_corr<FMA>(d_ez_dy1, pf.b(1, hh.sy), pf.a(1, hh.sy), pf.ik(1, hh.sy), hh.y0);
-            d_ex_dy1 = pml_corr<FMA>(d_ex_dy1, pf.b(1, hh.sy), pf.a(1, hh.sy), pf.ik(1, hh.sy), hh.y1);
-          }
-          if (AXZ && hh.sz >= 0) {
-            d_ey_dz1 = pml_corr<FMA>(d_ey_dz1, pf.b(2, hh.sz), pf.a(2, hh.sz), pf.ik(2, hh.sz), hh.z0);
-            d_ex_dz1 = pml_corr<FMA>(d_ex_dz1, pf.b(2, hh.sz), pf.a(2, hh.sz), pf.ik(2, hh.sz), hh.z1);
-          }
-          const float4 cf = s_coef[Mc[rh * L::MW + 15]];
-          hyv = h_new<FMA>(cf.z, Hc[(1 * L::HH + rh) * L::HW + 3], cf.w, sub(d_ex_dz1, d_ez_dx1));
-          hzv = h_new<FMA>(cf.z, Hc[(2 * L::HH + rh) * L::HW + 3], cf.w, sub(d_ey_dx1, d_ex_dy1));
-        }
-        pl_hzh[rh] = hzv;
-        pl_hyh[rh] = hyv;
-      }
-    }
-    if (PML && cell_ok && j + 1 < np - 1) prefetch(p + 1);  // next plane's H terms
-    if (xhalo && j + 1 < np - 1) prefetch_halo(p + 1);
-
-    ok = __syncthreads_or(ok ? 0 : 1) == 0;
-    if (!ok) break;
-    if (tid == 0 && issued < np) {  // stage j is consumed: refill its slot
-      fence_proxy_async();
-      issue(issued);
-      ++issued;
-    }
-
-    // ---------------- E phase (update_e_field[_pml], src/fdtd.rs:369-509) ----
-    if (tile_warp) {
-      if (!warm) {
-        const float4 hz_my = lds4(pl_hz + (r - 1) * kTileX + 4 * lane);
-        const float4 hx_my = lds4(pl_hx + (r - 1) * kTileX + 4 * lane);
-        float hz_w = __shfl_up_sync(0xffffffffu, hc[3], 1);
-        float hy_w = __shfl_up_sync(0xffffffffu, hb[3], 1);
-        if (lane == 0) {
-          hz_w = pl_hzh[r];
-          hy_w = pl_hyh[r];
-        }
-        float d_hz_dy[4], d_hx_dy[4], d_hy_dz[4], d_hx_dz[4], d_hz_dx[4], d_hy_dx[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          d_hz_dy[q] = sub(hc[q], comp(hz_my, q));
-          d_hx_dy[q] = sub(ha[q], comp(hx_my, q));
-          d_hy_dz[q] = sub(hb[q], comp(hyp, q));
-          d_hx_dz[q] = sub(ha[q], comp(hxp, q));
-          d_hz_dx[q] = sub(hc[q], q == 0 ? hz_w : hc[q - 1]);
-          d_hy_dx[q] = sub(hb[q], q == 0 ? hy_w : hb[q - 1]);
-        }
-        if (PML && cell_ok) {
-          if (AXX && lp.xmode == 1) {
-            const PmlAxis &P = g.pml[0];
-            corr4_x<FMA>(d_hz_dx, d_hy_dx, ex_, pf, lp.sx);
-            stg4(P.psi_nxt + 2 * P.cells + lp.ix, ex_.p0);
-            stg4(P.psi_nxt + 3 * P.cells + lp.ix, ex_.p1);
-          } else if (AXX && lp.xmode == 2) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              corr_x_cell<FMA>(g, pf, 2, xg + q, y, p, d_hz_dx[q], d_hy_dx[q], true);
-          }
-          if (AXY && lp.y) {
-            const PmlAxis &P = g.pml[1];
-            corr4_uniform<FMA>(d_hz_dy, d_hx_dy, ey_, pf.b(1, lp.sy), pf.a(1, lp.sy), pf.ik(1, lp.sy));
-            stg4(P.psi_nxt + 2 * P.cells + lp.iy, ey_.p0);
-            stg4(P.psi_nxt + 3 * P.cells + lp.iy, ey_.p1);
-          }
-          if (AXZ && lp.z) {
-            const PmlAxis &P = g.pml[2];
-            corr4_uniform<FMA>(d_hy_dz, d_hx_dz, ez_, pf.b(2, lp.sz), pf.a(2, lp.sz), pf.ik(2, lp.sz));
-            stg4(P.psi_nxt + 2 * P.cells + lp.iz, ez_.p0);
-            stg4(P.psi_nxt + 3 * P.cells + lp.iz, ez_.p1);
-          }
-        }
-        if (cell_ok) {
-          float eo[3][4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const unsigned char id = q == 0 ? m4.x : (q == 1 ? m4.y : (q == 2 ? m4.z : m4.w));
-            const float4 cf = s_coef[id];
-            eo[0][q] = e_new<FMA>(cf.x, comp(ex4, q), cf.y, sub(d_hz_dy[q], d_hy_dz[q]));
-            eo[1][q] = e_new<FMA>(cf.x, comp(ey4, q), cf.y, sub(d_hx_dz[q], d_hz_dx[q]));
-            eo[2][q] = e_new<FMA>(cf.x, comp(ez4, q), cf.y, sub(d_hy_dx[q], d_hx_dy[q]));
-          }
-          float *Ep = g.nxt + (static_cast<long long>(p) * ny + y) * nx + xg;
-          stg4(Ep, make_float4(eo[0][0], eo[0][1], eo[0][2], eo[0][3]));
-          stg4(Ep + N, make_float4(eo[1][0], eo[1][1], eo[1][2], eo[1][3]));
-          stg4(Ep + 2 * N, make_float4(eo[2][0], eo[2][1], eo[2][2], eo[2][3]));
-        }
-      }
-      hxp = make_float4(ha[0], ha[1], ha[2], ha[3]);
-      hyp = make_float4(hb[0], hb[1], hb[2], hb[3]);
-    }
-  }
-
-  if (!ok) {
-    // A staged plane never arrived within the wait limit: latch the error and
-    // wait (again bounded) for this CTA's copies still in flight before its
-    // shared memory is released.
-    if (tid == 0) {
-      atomicOr(g.err, kErrTimeout);
-      for (int jj = done; jj < issued; ++jj) mbar_wait(smem_u32(&s_bar[jj % S]), (jj / S) & 1);
-    }
-  }
-}
-
-// One launch handles one class of work items: interior items (AX = 0: no
-// CPML code, lean registers), items meeting only the x, only the y or only
-// the z slab (AX = 1, 2, 4), or items meeting several (AX = 7).  The host
-// lists each class's items (tile x, tile y, z chunk); the launches
-// partition the grid.
-template <int TY, int S, bool FMA, int AX>
-__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 3 : 1)
-    k_fused(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
-            const __grid_constant__ CUtensorMap tmM, const FusedArgs a, const int *items) {
-  using L = Layout<TY, S>;
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char *smem = reinterpret_cast<unsigned char *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
-  int item = items[blockIdx.x];
-  const int txi = item % a.tiles_x;
-  item /= a.tiles_x;
-  const int tyi = item % a.tiles_y;
-  const int zc = item / a.tiles_y;
-  const int x0 = txi * kTileX, y0 = tyi * TY;
-  const int k0 = zc * a.zchunk;
-  const int k1 = min(k0 + a.zchunk, a.g.nz);
-
-  float4 *s_coef = reinterpret_cast<float4 *>(smem);
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) s_coef[i] = a.g.coef[i];
-  if (AX != 0) {  // CPML profiles at slab positions (every W <= kProfCap here)
-    float *s_prof = reinterpret_cast<float *>(smem + L::PROF_OFF);
-    for (int i = threadIdx.x; i < kProfSmem; i += blockDim.x) {
-      const int cap = kProfSmem / 9;
-      const int ax = i / (3 * cap), k = (i / cap) % 3, s = i % cap;
-      const PmlAxis &P = a.g.pml[ax];
-      s_prof[i] = (P.T > 0 && s < P.W) ? P.prof[k * P.W + s] : 0.0f;
-    }
-  }
-  if (threadIdx.x == 0) {
-    uint64_t *s_bar = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
-    for (int s = 0; s < S; ++s) mbar_init(smem_u32(&s_bar[s]), 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  fused_body<TY, S, FMA, AX>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
-}
-
-#define WF_AX_CLASSES(X) X(0) X(1) X(2) X(4) X(7)
-
-template <int TY, int S>
-cudaError_t prepare_t() {
-  using L = Layout<TY, S>;
-  const void *fns[] = {
-#define X(A) (const void *)k_fused<TY, S, false, A>, (const void *)k_fused<TY, S, true, A>,
-      WF_AX_CLASSES(X)
-#undef X
-  };
-  for (const void *f : fns) {
-    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
-}
-
-template <int TY, int S, bool FMA>
-cudaError_t launch_t(const FusedMaps &m, const FusedArgs &a, const int *items, int n_items,
-                     int ax, cudaStream_t s) {
-  using L = Layout<TY, S>;
-  if (n_items <= 0) return cudaSuccess;
-  switch (ax) {
-#define X(A)                                                                                 \
-  case A:                                                                                   \
-    k_fused<TY, S, FMA, A><<<n_items, L::THREADS, L::BYTES, s>>>(m.e, m.h, m.m, a, items); \
-    break;
-    WF_AX_CLASSES(X)
-#undef X
-    default:
-      return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
-}
-
-}  // namespace
-
-void fused_boxes(int ty, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]) {
-  e_box[0] = kTileX + 8; e_box[1] = ty + 2; e_box[2] = 1; e_box[3] = 3;
-  h_box[0] = kTileX + 4; h_box[1] = ty + 1; h_box[2] = 1; h_box[3] = 3;
+void fused_boxes(int ty, int prec, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]) {
+  const unsigned pad = prec == kPrecF32 ? 4u : 8u;  // 16 bytes of x
+  e_box[0] = kTileX + 2 * pad; e_box[1] = ty + 2; e_box[2] = 1; e_box[3] = 3;
+  h_box[0] = kTileX + pad; h_box[1] = ty + 1; h_box[2] = 1; h_box[3] = 3;
   m_box[0] = kTileX + 16; m_box[1] = ty + 1; m_box[2] = 1;
 }
 
@@ -648,25 +34,30 @@ int fused_item_class(const FusedArgs &a, int ty, int item) {
   return (mask == 0 || mask == 1 || mask == 2 || mask == 4) ? mask : 7;
 }
 
-// (tile rows, stages) combinations that are instantiated
-#define WF_FUSED_CONFIGS(X) X(4, 3) X(4, 4) X(8, 3) X(8, 4) X(16, 3)
-
-bool fused_supported(const FusedConfig &c) {
-#define X(T, S_) if (c.ty == T && c.stages == S_) return c.zchunk >= 1;
+bool fused_supported(const FusedConfig &c, int prec) {
+  if (c.zchunk < 1) return false;
+  if (prec != kPrecF32) return fused16_supported(c);
+#define X(T, S_) if (c.ty == T && c.stages == S_) return true;
   WF_FUSED_CONFIGS(X)
 #undef X
   return false;
 }
 
-int fused_smem_bytes(const FusedConfig &c) {
-#define X(T, S_) if (c.ty == T && c.stages == S_) return Layout<T, S_>::BYTES;
+int fused_smem_bytes(const FusedConfig &c, int prec) {
+  if (prec != kPrecF32) return fused16_smem_bytes(c, prec);
+#define X(T, S_) if (c.ty == T && c.stages == S_) return Layout<T, S_, float>::BYTES;
   WF_FUSED_CONFIGS(X)
 #undef X
   return -1;
 }
 
-cudaError_t fused_prepare(const FusedConfig &c) {
-#define X(T, S_) if (c.ty == T && c.stages == S_) return prepare_t<T, S_>();
+cudaError_t fused_prepare(const FusedConfig &c, int prec) {
+  if (prec != kPrecF32) return fused16_prepare(c, prec);
+#define X(T, S_)                                                    \
+  if (c.ty == T && c.stages == S_) {                                \
+    cudaError_t e = prepare_t<T, S_, false, float>();               \
+    return e != cudaSuccess ? e : prepare_t<T, S_, true, float>();  \
+  }
   WF_FUSED_CONFIGS(X)
 #undef X
   return cudaErrorInvalidValue;
@@ -674,10 +65,14 @@ cudaError_t fused_prepare(const FusedConfig &c) {
 
 cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                          const int *items, int n_items, int ax, bool fma, cudaStream_t s) {
-#define X(T, S_)                                                                        \
-  if (c.ty == T && c.stages == S_)                                                     \
-    return fma ? launch_t<T, S_, true>(m, a, items, n_items, ax, s)                    \
-               : launch_t<T, S_, false>(m, a, items, n_items, ax, s);
+  if (a.g.prec != kPrecF32) {
+    if (fma) return cudaErrorInvalidValue;  // 16-bit storage runs the exact arithmetic
+    return fused16_launch(c, m, a, items, n_items, ax, s);
+  }
+#define X(T, S_)                                                            \
+  if (c.ty == T && c.stages == S_)                                         \
+    return fma ? launch_t<T, S_, true, float>(m, a, items, n_items, ax, s) \
+               : launch_t<T, S_, false, float>(m, a, items, n_items, ax, s);
   WF_FUSED_CONFIGS(X)
 #undef X
   return cudaErrorInvalidValue;

@@ -53,17 +53,28 @@ struct ProbeDev {
   float *trace;
 };
 
+// Field storage of a handle (values match wf_precision of the C ABI).
+enum : int { kPrecF32 = 0, kPrecBF16 = 1, kPrecF16 = 2 };
+constexpr int kSlabPlanes = 8;  // z planes per storage-scale slab
+
 struct GridArgs {
   int nx, ny, nz;
   long long N;           // nx*ny*nz
   int periodic[3];
-  const float *cur;      // 6*N, component-major, x fastest
-  float *nxt;            // 6*N
+  const float *cur;      // 6*N, component-major, x fastest (16-bit elements
+  float *nxt;            // when prec != kPrecF32; the kernels cast)
   const uint8_t *mat;    // [nz][ny][mat_pitch]
   int mat_pitch;
   const float4 *coef;    // 256 x {ca, cb, da, db}
   PmlAxis pml[3];
   int *err;
+  // 16-bit storage only: per slab (z / kSlabPlanes) and kind (0 E, 1 H)
+  int prec;
+  const int *shift_rd;   // [nslab][2] shifts of the state read
+  const int *shift_wr;   // [nslab][2] shifts of the state written
+  unsigned *slab_max;    // [nslab][2] max |decoded value| bits of the state written
+  unsigned long long *ovf;  // binary16 saturations
+  int nslab;
 };
 
 __device__ __forceinline__ int slab_pos(int c, int n, int T, int W) {

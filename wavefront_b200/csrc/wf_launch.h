@@ -9,13 +9,23 @@
 namespace wf {
 
 struct TailArgs {
-  float *f;  // the new state (6*N)
+  float *f;  // the new state (6*N; 16-bit elements when prec != kPrecF32)
   int nx, ny, nz;
   const SrcDev *src;
   int nsrc;
   const ProbeDev *probe;
   int nprobe;
   long long *step;  // device step counter (read, then incremented)
+  // 16-bit storage: shifts of the new state (sources and probes decode and
+  // re-encode with them), its slab maxima, and the shifts the next step
+  // writes with (computed here, into the buffer the step just read)
+  int prec;
+  const int *shift_f;
+  unsigned *slab_max;
+  int *shift_next;
+  int nslab, periodic_z;
+  float kh, ke;  // 8 * max |Db|, 8 * max |Cb| over the material table
+  unsigned long long *ovf;
 };
 
 struct FusedArgs {
@@ -43,12 +53,12 @@ cudaError_t launch_soa_to_blocks(const float *soa, float *blk, int nx, int ny, i
 cudaError_t launch_blocks_to_soa(const float *blk, float *soa, int nx, int ny, int nz,
                                  cudaStream_t s);
 
-// TMA boxes the fused kernel needs for a tiling (encoded by the host).
-void fused_boxes(int ty, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]);
-bool fused_supported(const FusedConfig &c);
-int fused_smem_bytes(const FusedConfig &c);
+// TMA boxes the fused kernel needs for a tiling and storage (encoded by the host).
+void fused_boxes(int ty, int prec, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]);
+bool fused_supported(const FusedConfig &c, int prec);
+int fused_smem_bytes(const FusedConfig &c, int prec);
 // Sets the kernels' dynamic shared-memory limit (call outside graph capture).
-cudaError_t fused_prepare(const FusedConfig &c);
+cudaError_t fused_prepare(const FusedConfig &c, int prec);
 // Kernel class of work item `item` (tile x, tile y, z chunk): 0 interior,
 // 1 / 2 / 4 meets only the x / y / z CPML slab, 7 meets several.
 int fused_item_class(const FusedArgs &a, int ty, int item);
@@ -56,5 +66,27 @@ constexpr int kFusedClasses[5] = {0, 1, 2, 4, 7};
 // Launches the kernel of class `ax` over a device list of n_items items.
 cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                          const int *items, int n_items, int ax, bool fma, cudaStream_t s);
+// 16-bit storage (wf_fused16.cu)
+bool fused16_supported(const FusedConfig &c);
+int fused16_smem_bytes(const FusedConfig &c, int prec);
+cudaError_t fused16_prepare(const FusedConfig &c, int prec);
+cudaError_t fused16_launch(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
+                           const int *items, int n_items, int ax, cudaStream_t s);
+
+// 16-bit storage helpers (wf_split.cu).
+// Encodes FP32 values `in` (6*N) as the 16-bit state `out`: per slab and
+// kind the shift of the slab's own maximum (written to `shift`); leaves the
+// maxima of the encoded state in slab_max.
+cudaError_t launch_encode_state(const float *in, void *out, int prec, int nx, int ny, int nz,
+                                int *shift, unsigned *slab_max, unsigned long long *ovf,
+                                cudaStream_t s);
+cudaError_t launch_decode_state(const void *in, float *out, int prec, int nx, int ny, int nz,
+                                const int *shift, cudaStream_t s);
+// Slab maxima (bits of the largest decoded magnitude per slab and kind) of a
+// 16-bit state, into slab_max.
+cudaError_t launch_state_max(const void *in, int prec, int nx, int ny, int nz, const int *shift,
+                             unsigned *slab_max, cudaStream_t s);
+// Write shifts of the step with index `next` into t.shift_next (see k_tail).
+cudaError_t launch_next_shifts(const TailArgs &t, long long next, cudaStream_t s);
 
 }  // namespace wf

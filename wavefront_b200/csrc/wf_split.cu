@@ -8,6 +8,7 @@
 // the fused kernel, so either path can continue a run the other started.
 #include "wf_internal.cuh"
 #include "wf_launch.h"
+#include "wf_store.cuh"
 
 namespace wf {
 
@@ -149,36 +150,118 @@ __global__ void k_split_e(GridArgs g) {
   En[2 * N + i] = e_new<FMA>(cf.x, E[2 * N + i], cf.y, curl_ez);
 }
 
+// One stored value of a 16-bit state: decode / encode with a shift.
+__device__ __forceinline__ float dec16(const void *f, long long i, int prec, int shift) {
+  const unsigned short b = static_cast<const unsigned short *>(f)[i];
+  const float v = prec == kPrecF16 ? Store16<__half>::dec1(b) : Store16<__nv_bfloat16>::dec1(b);
+  return __fmul_rn(v, pow2f(shift));
+}
+// stores v; returns the decoded stored value
+__device__ __forceinline__ float enc16(void *f, long long i, int prec, int shift, float v,
+                                       unsigned long long *ovf) {
+  const float u = __fmul_rn(v, pow2f(-shift));
+  const unsigned short b =
+      prec == kPrecF16 ? Store16<__half>::enc1(u, ovf) : Store16<__nv_bfloat16>::enc1(u, ovf);
+  static_cast<unsigned short *>(f)[i] = b;
+  const float d = prec == kPrecF16 ? Store16<__half>::dec1(b) : Store16<__nv_bfloat16>::dec1(b);
+  return __fmul_rn(d, pow2f(shift));
+}
+
+// Write shifts of the step with index `next`, from the slab maxima of the
+// state it reads (then cleared): a slab's bound takes its neighbour slabs'
+// maxima (one step moves information one plane), the E/H cross-coupling
+// through the largest Cb/Db times 8 (four raw differences, each at most
+// doubled by the CPML correction), and the soft-source amplitudes that
+// step adds:  bh = 2*NH + kh*NE,  be = 2*NE + ke*bh + src  (f32, this
+// order); shift = store_shift_bits(bound).  Whole CTA; s_src >= nslab.
+__device__ void next_shifts(const TailArgs &t, long long next, float *s_src) {
+  for (int b = threadIdx.x; b < t.nslab; b += blockDim.x) s_src[b] = 0.0f;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < t.nsrc; ++i) {
+      const SrcDev q = t.src[i];
+      const float v = next < q.nvals ? fabsf(q.vals[next]) : 0.0f;
+      if (q.mode == 0) {
+        const int b = q.z / kSlabPlanes;
+        s_src[b] = __fadd_rn(s_src[b], v);
+      } else {
+        for (int b = 0; b < t.nslab; ++b) s_src[b] = __fadd_rn(s_src[b], v);
+      }
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < t.nslab; b += blockDim.x) {
+    unsigned me = t.slab_max[2 * b], mh = t.slab_max[2 * b + 1];
+    for (int d = -1; d <= 1; d += 2) {
+      int n = b + d;
+      if (n < 0 || n >= t.nslab) {
+        if (!t.periodic_z) continue;
+        n = (n + t.nslab) % t.nslab;
+      }
+      me = max(me, t.slab_max[2 * n]);
+      mh = max(mh, t.slab_max[2 * n + 1]);
+    }
+    const float ne = __uint_as_float(me), nh = __uint_as_float(mh);
+    const float bh = __fadd_rn(__fmul_rn(2.0f, nh), __fmul_rn(t.kh, ne));
+    const float be = __fadd_rn(__fadd_rn(__fmul_rn(2.0f, ne), __fmul_rn(t.ke, bh)), s_src[b]);
+    t.shift_next[2 * b] = store_shift_bits(__float_as_uint(be));
+    t.shift_next[2 * b + 1] = store_shift_bits(__float_as_uint(bh));
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < 2 * t.nslab; b += blockDim.x) t.slab_max[b] = 0u;
+}
+
+constexpr int kMaxSlabs = 1024;  // nz <= 8192 for 16-bit storage
+
 // Sources in list order (src/engine.rs:769-772, Source::inject
 // src/source.rs:79-95), then probes (src/probe.rs:126-138).  One CTA; the
 // step index lives in device memory so captured graphs stay replayable.
+// 16-bit storage: sources re-encode the cells they change (their magnitudes
+// join the slab maxima), probes decode, and the CTA then picks the shifts
+// the next step writes with.
 __global__ void k_tail(TailArgs t) {
   __shared__ long long s_step;
+  __shared__ float s_src[kMaxSlabs];
   if (threadIdx.x == 0) s_step = *t.step;
   __syncthreads();
   const long long st = s_step;
   const long long N = static_cast<long long>(t.nx) * t.ny * t.nz;
+  const bool f16 = t.prec != kPrecF32;
   for (int s = 0; s < t.nsrc; ++s) {
     const SrcDev q = t.src[s];
     const float v = st < q.nvals ? q.vals[st] : 0.0f;
-    float *F = t.f + q.comp * N;
     if (q.mode == 0) {
       if (threadIdx.x == 0) {
-        const long long i = (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x;
-        F[i] = __fadd_rn(F[i], v);
+        const long long i = q.comp * N + (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x;
+        if (f16) {
+          const int b = q.z / kSlabPlanes, sh = t.shift_f[2 * b];
+          const float d = enc16(t.f, i, t.prec, sh, __fadd_rn(dec16(t.f, i, t.prec, sh), v), t.ovf);
+          t.slab_max[2 * b] = max(t.slab_max[2 * b], __float_as_uint(fabsf(d)));
+        } else {
+          t.f[i] = __fadd_rn(t.f[i], v);
+        }
       }
     } else {
       const long long m = static_cast<long long>(t.ny) * t.nz;
       for (long long c = threadIdx.x; c < m; c += blockDim.x) {
         const long long yy = c % t.ny, zz = c / t.ny;
-        F[(zz * t.ny + yy) * t.nx + q.x] = v;
+        const long long i = q.comp * N + (zz * t.ny + yy) * t.nx + q.x;
+        if (f16) {
+          const int b = static_cast<int>(zz) / kSlabPlanes;
+          const float d = enc16(t.f, i, t.prec, t.shift_f[2 * b], v, t.ovf);
+          atomicMax(t.slab_max + 2 * b, __float_as_uint(fabsf(d)));
+        } else {
+          t.f[i] = v;
+        }
       }
     }
     __syncthreads();
   }
   for (int p = threadIdx.x; p < t.nprobe; p += blockDim.x) {
     const ProbeDev q = t.probe[p];
-    const float raw = t.f[q.comp * N + (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x];
+    const long long i = q.comp * N + (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x;
+    const float raw =
+        f16 ? dec16(t.f, i, t.prec, t.shift_f[2 * (q.z / kSlabPlanes) + (q.comp >= 3)]) : t.f[i];
     if (q.record && st < q.nsteps) q.trace[st] = raw;
     if (st >= q.first_step && st < q.nsteps) {
       const double v = static_cast<double>(raw);
@@ -190,7 +273,56 @@ __global__ void k_tail(TailArgs t) {
     }
   }
   __syncthreads();
+  if (f16) next_shifts(t, st + 1, s_src);
   if (threadIdx.x == 0) *t.step = st + 1;
+}
+
+__global__ void k_next_shifts(TailArgs t, long long next) {
+  __shared__ float s_src[kMaxSlabs];
+  next_shifts(t, next, s_src);
+}
+
+// 16-bit state from FP32 values, in three passes: slab maxima of the input,
+// the shifts they give, then the encoding (whose maxima remain).
+__global__ void k_slab_max_f32(const float *in, long long N, int nxy, unsigned *slab_max) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= 6 * N) return;
+  const int c = static_cast<int>(i / N);
+  const int b = static_cast<int>((i % N) / nxy) / kSlabPlanes;
+  const unsigned v = __float_as_uint(fabsf(in[i]));
+  if (v) atomicMax(slab_max + 2 * b + (c >= 3), v);
+}
+__global__ void k_shift_from_max(unsigned *slab_max, int *shift, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  shift[i] = store_shift_bits(slab_max[i]);
+  slab_max[i] = 0u;
+}
+__global__ void k_encode(const float *in, void *out, int prec, long long N, int nxy,
+                         const int *shift, unsigned *slab_max, unsigned long long *ovf) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= 6 * N) return;
+  const int c = static_cast<int>(i / N);
+  const int k = 2 * (static_cast<int>((i % N) / nxy) / kSlabPlanes) + (c >= 3);
+  const float d = enc16(out, i, prec, shift[k], in[i], ovf);
+  const unsigned v = __float_as_uint(fabsf(d));
+  if (v) atomicMax(slab_max + k, v);
+}
+__global__ void k_state_max(const void *in, int prec, long long N, int nxy, const int *shift,
+                            unsigned *slab_max) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= 6 * N) return;
+  const int c = static_cast<int>(i / N);
+  const int k = 2 * (static_cast<int>((i % N) / nxy) / kSlabPlanes) + (c >= 3);
+  const unsigned v = __float_as_uint(fabsf(dec16(in, i, prec, shift[k])));
+  if (v) atomicMax(slab_max + k, v);
+}
+__global__ void k_decode(const void *in, float *out, int prec, long long N, int nxy,
+                         const int *shift) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= 6 * N) return;
+  const int c = static_cast<int>(i / N);
+  out[i] = dec16(in, i, prec, shift[2 * (static_cast<int>((i % N) / nxy) / kSlabPlanes) + (c >= 3)]);
 }
 
 // SoA (x fastest) <-> FieldBlock order (src/layout.rs:697-755)
@@ -232,7 +364,46 @@ cudaError_t launch_split(const GridArgs &g, bool fma, cudaStream_t s) {
 }
 
 cudaError_t launch_tail(const TailArgs &t, cudaStream_t s) {
+  if (t.prec != kPrecF32 && t.nslab > kMaxSlabs) return cudaErrorInvalidValue;
   k_tail<<<1, 256, 0, s>>>(t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_next_shifts(const TailArgs &t, long long next, cudaStream_t s) {
+  if (t.nslab > kMaxSlabs) return cudaErrorInvalidValue;
+  k_next_shifts<<<1, 256, 0, s>>>(t, next);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_encode_state(const float *in, void *out, int prec, int nx, int ny, int nz,
+                                int *shift, unsigned *slab_max, unsigned long long *ovf,
+                                cudaStream_t s) {
+  const long long N = static_cast<long long>(nx) * ny * nz;
+  const unsigned blocks = static_cast<unsigned>((6 * N + 255) / 256);
+  const int nslab = nz / kSlabPlanes;
+  cudaError_t e = cudaMemsetAsync(slab_max, 0, sizeof(unsigned) * 2 * nslab, s);
+  if (e != cudaSuccess) return e;
+  k_slab_max_f32<<<blocks, 256, 0, s>>>(in, N, nx * ny, slab_max);
+  k_shift_from_max<<<(2 * nslab + 255) / 256, 256, 0, s>>>(slab_max, shift, 2 * nslab);
+  k_encode<<<blocks, 256, 0, s>>>(in, out, prec, N, nx * ny, shift, slab_max, ovf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_state_max(const void *in, int prec, int nx, int ny, int nz, const int *shift,
+                             unsigned *slab_max, cudaStream_t s) {
+  const long long N = static_cast<long long>(nx) * ny * nz;
+  cudaError_t e = cudaMemsetAsync(slab_max, 0, sizeof(unsigned) * 2 * (nz / kSlabPlanes), s);
+  if (e != cudaSuccess) return e;
+  k_state_max<<<static_cast<unsigned>((6 * N + 255) / 256), 256, 0, s>>>(in, prec, N, nx * ny,
+                                                                         shift, slab_max);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_decode_state(const void *in, float *out, int prec, int nx, int ny, int nz,
+                                const int *shift, cudaStream_t s) {
+  const long long N = static_cast<long long>(nx) * ny * nz;
+  k_decode<<<static_cast<unsigned>((6 * N + 255) / 256), 256, 0, s>>>(in, out, prec, N, nx * ny,
+                                                                       shift);
   return cudaGetLastError();
 }
 

@@ -22,6 +22,9 @@ from .layout import GridDims, MaterialGrid, MaterialTable, PmlContext
 _BOUNDARY = {"zero": 0, "periodic": 1}
 _ARITH = {"exact": 0, "fma": 1}
 _KERNEL = {"auto": 0, "fused": 1, "split": 2}
+# field storage: FP32 (reference parity) or 16-bit with per-slab power-of-two
+# scales (wf_precision)
+_PRECISION = {"f32": 0, "bf16": 1, "f16": 2}
 
 # PmlAux array order of src/layout.rs:545-558
 PSI_NAMES = ["psi_ez_dx", "psi_ey_dx", "psi_ez_dy", "psi_ex_dy", "psi_ey_dz", "psi_ex_dz",
@@ -30,15 +33,17 @@ PSI_NAMES = ["psi_ez_dx", "psi_ey_dx", "psi_ez_dy", "psi_ex_dy", "psi_ey_dz", "p
 
 class DeviceFieldGrid:
     def __init__(self, dims: GridDims, boundary=("zero", "zero", "zero"), arith: str = "exact",
-                 kernel: str = "auto", device: int = 0, stream: Optional[int] = None):
+                 kernel: str = "auto", device: int = 0, stream: Optional[int] = None,
+                 precision: str = "f32"):
         self.dims = dims
+        self.precision = precision
         d = _L.GridDesc()
         d.nx, d.ny, d.nz = dims.nx, dims.ny, dims.nz
         for i, b in enumerate(boundary):
             d.boundary[i] = _BOUNDARY[b]
         d.arith = _ARITH[arith]
         d.kernel = _KERNEL[kernel]
-        d.precision = 0
+        d.precision = _PRECISION[precision]
         d.device = device
         d.stream = stream
         h = C.c_void_p()
@@ -117,6 +122,16 @@ class DeviceFieldGrid:
     @property
     def steps_done(self) -> int:
         return int(_L.lib().wf_steps_done(self._h))
+
+    def storage_info(self):
+        """16-bit storage: (E shifts, H shifts) the next step stores with, per
+        8-plane z slab, and the number of binary16 saturations so far."""
+        nslab = self.dims.nz // 8
+        e = (C.c_int * nslab)()
+        h = (C.c_int * nslab)()
+        ov = C.c_uint64()
+        self._chk(_L.lib().wf_storage_info(self._h, e, h, C.byref(ov)))
+        return np.array(e[:], np.int32), np.array(h[:], np.int32), int(ov.value)
 
     @property
     def kernel_launches(self) -> int:
