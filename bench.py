@@ -140,17 +140,20 @@ def cpu_baseline(sc, seconds=15.0):
             "kind": "port", "sample": f"{n} full {GRID}^3 steps after 1 warm-up step, {el:.1f} s"}
 
 
-def scenario(args, steps):
+def scenario(args, steps, device_voxelize=None):
+    """The workload; random spheres above 256^3 are voxelized on the device
+    (the host voxelizer's 32 full-grid passes take minutes at 1024^3)."""
     from wavefront_b200 import configs
     if args.workload == "random_spheres":
-        return configs.random_spheres(n=GRID, steps=steps)
+        dv = GRID > 256 if device_voxelize is None else device_voxelize
+        return configs.random_spheres(n=GRID, steps=steps, device_voxelize=dv)
     return configs.two_spheres(n=GRID, steps=steps)
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    sc = scenario(args, args.warmup + args.steps)
+    sc = scenario(args, args.warmup + args.steps, device_voxelize=False)
     from oracle import oracle as O
     nt = os.cpu_count() or 1
     sim = O.sim_from_scenario(sc, steps=args.warmup + args.steps)
@@ -248,30 +251,39 @@ def run_ours(args, rank, world, local_rank):
             traffic = json.load(f).get("fused_two_spheres_512_bytes_per_launch")
 
     # ---- end to end through the C ABI from host buffers -----------------
-    pin_ids = torch.from_numpy(sc.grid.ids).pin_memory()
-    snap = torch.empty(N_CELLS * 6, dtype=torch.float32).pin_memory()
-    sc.grid.ids = pin_ids.numpy()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    g = build()
-    g.step(args.steps)
-    g.sync()
-    sums = [g.probe_sums(i, 1) for i in range(len(sc.probes))]
-    import ctypes as C
-    from wavefront_b200 import _lib as L
-    L.check(L.lib().wf_download_blocks(g._h, C.c_void_p(snap.data_ptr())), g._h)
-    e2e_s = time.perf_counter() - t0
-    g.close()
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-        dist.barrier()
-    e2e = world * N_CELLS * args.steps / e2e_s / 1e6
-    h2d = N_CELLS + 256 * 16 + total * (4 + 8 * 16)
-    d2h = len(sums) * (8 * 2 + 8) + N_CELLS * 24
+    e2e_line = {"value": None, "unit": METRIC, "skipped": "--no-e2e"}
+    if not args.no_e2e:
+        if sc.grid is not None:  # host ids travel pinned; a device scene sends only its text
+            pin_ids = torch.from_numpy(sc.grid.ids).pin_memory()
+        snap = torch.empty(N_CELLS * 6, dtype=torch.float32).pin_memory()
+        if sc.grid is not None:
+            sc.grid.ids = pin_ids.numpy()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = build()
+        g.step(args.steps)
+        g.sync()
+        sums = [g.probe_sums(i, 1) for i in range(len(sc.probes))]
+        import ctypes as C
+        from wavefront_b200 import _lib as L
+        L.check(L.lib().wf_download_blocks(g._h, C.c_void_p(snap.data_ptr())), g._h)
+        e2e_s = time.perf_counter() - t0
+        g.close()
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+            dist.barrier()
+        e2e = world * N_CELLS * args.steps / e2e_s / 1e6
+        h2d = (N_CELLS if sc.grid is not None else len(sc.scene_text)) + 256 * 16 + total * (4 + 8 * 16)
+        d2h = len(sums) * (8 * 2 + 8) + N_CELLS * 24
+        e2e_line = {"value": round(e2e, 1), "unit": METRIC,
+                    "h2d_bytes_per_step": int(h2d / args.steps),
+                    "d2h_bytes_per_step": int(d2h / args.steps),
+                    "includes": "handle creation, scene + table upload, K steps, probe sums, "
+                                "one FieldBlock snapshot download (pinned host buffers)"}
 
     if rank == 0:
         line = {
@@ -287,11 +299,7 @@ def run_ours(args, rank, world, local_rank):
                        "l2": f"inputs larger than L2 ({N_CELLS * 6 * ELEM[PRECISION] / 1e9:.1f} GB "
                              "of fields per state buffer)",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
-            "e2e": {"value": round(e2e, 1), "unit": METRIC,
-                    "h2d_bytes_per_step": int(h2d / args.steps),
-                    "d2h_bytes_per_step": int(d2h / args.steps),
-                    "includes": "handle creation, scene + table upload, K steps, probe sums, "
-                                "one FieldBlock snapshot download (pinned host buffers)"},
+            "e2e": e2e_line,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
@@ -299,7 +307,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": int(gpu_launches),
             "clocks": clocks,
         }
-        if world == 1 and not args.no_cpu:
+        if world == 1 and not args.no_cpu and sc.grid is not None:
             line["cpu_baseline"] = cpu_baseline(sc)
         print(json.dumps(line), flush=True)
     if dist:
@@ -314,6 +322,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tiling", default="", help="tile_rows,z_chunk,stages")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end leg (its snapshot needs 24 B/cell of pinned host RAM)")
     ap.add_argument("--grid", type=int, default=0,
                     help="cube edge (default 512 for two_spheres, 1024 for random_spheres)")
     ap.add_argument("--workload", default="two_spheres", choices=["two_spheres", "random_spheres"])

@@ -119,6 +119,19 @@ const char *wf_status_string(wf_status s);
 wf_status wf_set_materials(wf_handle *h, const uint8_t *ids,
                            const int32_t (*table_q16)[4]);
 
+/* Scene::parse + Scene::voxelize (src/scene.rs:81-230) with the ids
+ * rasterized on the device: every cell starts as material 0 (vacuum), then
+ * each primitive in file order overwrites the cells it covers (sphere:
+ * cell-centre test in f32, box: floor/ceil clamped ranges), the ids equal
+ * wf_scene_voxelize's.  table is in/out as for wf_scene_voxelize (entry 0 is
+ * the caller's vacuum; registered materials are written) and is uploaded as
+ * the coefficient table.  Parse errors return WF_ERR_ARG with the
+ * reference's message. */
+wf_status wf_set_scene(wf_handle *h, const char *text, float dt, float dx,
+                       int32_t (*table_q16)[4], int *n_materials);
+/* The material ids on the device, nz*ny*nx bytes (MaterialGrid order). */
+wf_status wf_get_materials(wf_handle *h, uint8_t *ids);
+
 /* CPML on one axis (0=x, 1=y, 2=z): the graded profile of that axis (n
  * entries each of b, a, 1/kappa: PmlProfile1D::build, src/layout.rs:471-513)
  * and the graded thickness T in voxels.  psi memory is kept for the cells
@@ -176,8 +189,9 @@ wf_status wf_get_psi(wf_handle *h, int which, float *out);
 /* Device pointers of the current six field arrays (FP32 precision only). */
 wf_status wf_device_fields(wf_handle *h, float **out6);
 /* 16-bit storage: the shifts the next step stores E and H with, per z slab
- * (nz/8 entries each; either may be NULL), and the count of binary16 values
- * saturated at +-65504 so far.  FP32 storage reports 0 overflows. */
+ * (nz/8 entries each; either may be NULL), and a saturation count: one per
+ * step, slab and kind whose largest stored binary16 magnitude was 65504 (where
+ * larger values saturate).  FP32 and bfloat16 storage report 0. */
 wf_status wf_storage_info(wf_handle *h, int *shift_e, int *shift_h, uint64_t *overflows);
 
 /* The handle's CUDA stream (cudaStream_t) for event timing and interop. */

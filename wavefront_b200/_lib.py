@@ -18,7 +18,7 @@ WF_OK, WF_ERR_ARG, WF_ERR_CUDA, WF_ERR_OOM, WF_ERR_TIMEOUT, WF_ERR_DEVICE_FLAG, 
 EXPORTS = [
     "wf_create", "wf_destroy", "wf_last_error", "wf_status_string", "wf_set_materials",
     "wf_set_pml", "wf_add_source", "wf_add_probe", "wf_step", "wf_sync", "wf_steps_done",
-    "wf_kernel_launches", "wf_storage_info",
+    "wf_kernel_launches", "wf_storage_info", "wf_set_scene", "wf_get_materials",
     "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
     "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
     "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
@@ -92,6 +92,10 @@ def lib() -> C.CDLL:
         L.wf_storage_info.argtypes = [_h, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_uint64)]
         L.wf_storage_info.restype = S
+        L.wf_set_scene.argtypes = [_h, C.c_char_p, C.c_float, C.c_float, _i32p, C.POINTER(C.c_int)]
+        L.wf_set_scene.restype = S
+        L.wf_get_materials.argtypes = [_h, _u8p]
+        L.wf_get_materials.restype = S
         L.wf_probe_sums.argtypes = [_h, C.c_int, _f64p, _f64p, C.POINTER(C.c_uint64)]
         L.wf_probe_sums.restype = S
         L.wf_probe_trace.argtypes = [_h, C.c_int, _f32p, C.c_int]

@@ -47,6 +47,8 @@ class Scenario:
     probes: List[Probe]
     steps: int
     meta: dict = field(default_factory=dict)
+    # set when the ids are to be rasterized on the device (grid is then None)
+    scene_text: Optional[str] = None
 
 
 def plain_cube_64(steps: int = 500, pml_cells: int = 10, exact_pml: bool = False,
@@ -105,25 +107,30 @@ def random_spheres_text(n: int, count: int = 32, seed: int = 1234) -> str:
 
 
 def random_spheres(n: int = 1024, steps: int = 2000, pml_cells: int = 16,
-                   seed: int = 1234) -> Scenario:
+                   seed: int = 1234, device_voxelize: bool = False) -> Scenario:
     """Mixed-precision workload: 32 seeded random dielectric spheres, 16-cell
     CPML, sinusoid Ez at the centre with 15 cells per wavelength, 8 Ez probes
     on a line at z = 7n/8 (x = n/16 + k*n/8, y = n/2), 2000 steps.  The same
-    scene at n = 128 is small enough for the FP64 oracle."""
+    scene at n = 128 is small enough for the FP64 oracle.  device_voxelize
+    leaves the ids to the device voxelizer (device_grid), which at 1024^3
+    takes milliseconds instead of the host's minutes."""
     dims = GridDims(n, n, n)
     dx = 1.0e-3
     dt = courant_dt(dx)
     f = float(np.float32(C0 / (15.0 * dx)))
-    grid = MaterialGrid(dims)
     table = MaterialTable.vacuum_filled(dt, dx)
-    Scene.parse(random_spheres_text(n, seed=seed)).voxelize(grid, table, dt, dx)
+    text = random_spheres_text(n, seed=seed)
+    grid = None
+    if not device_voxelize:
+        grid = MaterialGrid(dims)
+        Scene.parse(text).voxelize(grid, table, dt, dx)
     pml = PmlContext.build(dims, PmlConfig(thickness=pml_cells), dt, dx) if pml_cells else None
     c = n // 2
     src = Source(c, c, c, FieldComponent.Ez, 1.0, default_waveform("sinusoid", f))
     zp = (7 * n) // 8
     probes = [Probe(n // 16 + (n // 8) * k, c, zp, PC.Ez, [f], 0.0) for k in range(8)]
     return Scenario(f"random_spheres_{n}", dims, dx, dt, grid, table, pml, [src], probes, steps,
-                    {"f": f, "seed": seed})
+                    {"f": f, "seed": seed}, scene_text=text if device_voxelize else None)
 
 
 def demo_sphere_cube(n: int = 256, steps: int = 150, pml_cells: int = 8) -> Scenario:
@@ -143,7 +150,10 @@ def device_grid(sc: Scenario, **kw):
     """A DeviceFieldGrid loaded with the scenario's materials and CPML."""
     from .engine import DeviceFieldGrid
     g = DeviceFieldGrid(sc.dims, **kw)
-    g.set_materials(sc.grid, sc.table)
+    if sc.grid is None:
+        g.set_scene(sc.scene_text, sc.table, sc.dt, sc.dx)
+    else:
+        g.set_materials(sc.grid, sc.table)
     if sc.pml is not None:
         g.set_pml(sc.pml)
     return g

@@ -15,6 +15,7 @@
 
 #include "../../include/wavefront_gpu.h"
 #include "wf_launch.h"
+#include "wf_scene.h"
 
 using wf::FusedArgs;
 using wf::FusedConfig;
@@ -583,9 +584,10 @@ wf_status wf_destroy(wf_handle *h) {
   return WF_OK;
 }
 
-wf_status wf_set_materials(wf_handle *h, const uint8_t *ids, const int32_t (*table)[4]) {
-  if (!h || !ids || !table) return fail(h, WF_ERR_ARG, "null argument");
-  DeviceGuard guard(h->dev);
+namespace {
+
+// The coefficient table as the kernels read it (stream-ordered upload).
+wf_status upload_coef(wf_handle *h, const int32_t (*table)[4]) {
   // FixedQ16_16::to_f32 (src/layout.rs:123-125): q as f32 * (1/65536)
   float4 coef[256];
   float cbmax = 0.0f, dbmax = 0.0f;
@@ -599,8 +601,44 @@ wf_status wf_set_materials(wf_handle *h, const uint8_t *ids, const int32_t (*tab
   h->ke = 8.0f * cbmax;
   h->shifts_dirty = true;
   WF_CUDA(h, cudaMemcpyAsync(h->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, h->stream));
+  return WF_OK;
+}
+
+}  // namespace
+
+wf_status wf_set_materials(wf_handle *h, const uint8_t *ids, const int32_t (*table)[4]) {
+  if (!h || !ids || !table) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  wf_status st = upload_coef(h, table);
+  if (st != WF_OK) return st;
   WF_CUDA(h, cudaMemcpy2DAsync(h->mat, h->mat_pitch, ids, h->nx, h->nx,
                                static_cast<size_t>(h->ny) * h->nz, cudaMemcpyHostToDevice,
+                               h->stream));
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WF_OK;
+}
+
+wf_status wf_set_scene(wf_handle *h, const char *text, float dt, float dx,
+                       int32_t (*table)[4], int *n_materials) {
+  if (!h || !text || !table) return fail(h, WF_ERR_ARG, "null argument");
+  std::vector<wf::RasterOp> ops;
+  std::string msg;
+  if (!wf::scene_parse(text, h->nx, h->ny, h->nz, dt, dx, &ops, table, n_materials, &msg))
+    return fail(h, WF_ERR_ARG, msg);
+  DeviceGuard guard(h->dev);
+  wf_status st = upload_coef(h, table);
+  if (st != WF_OK) return st;
+  WF_CUDA(h, static_cast<cudaError_t>(
+                 wf::launch_voxelize(ops, h->mat, h->nx, h->ny, h->nz, h->mat_pitch, 0, h->stream)));
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return WF_OK;
+}
+
+wf_status wf_get_materials(wf_handle *h, uint8_t *ids) {
+  if (!h || !ids) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaMemcpy2DAsync(ids, h->nx, h->mat, h->mat_pitch, h->nx,
+                               static_cast<size_t>(h->ny) * h->nz, cudaMemcpyDeviceToHost,
                                h->stream));
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   return WF_OK;

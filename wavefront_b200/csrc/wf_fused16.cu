@@ -7,7 +7,7 @@
 namespace wf {
 
 // (tile rows, stages) combinations instantiated for 16-bit storage
-#define WF_FUSED16_CONFIGS(X) X(4, 3) X(4, 4) X(8, 3) X(8, 4)
+#define WF_FUSED16_CONFIGS(X) X(4, 3) X(4, 4) X(4, 5) X(4, 6) X(8, 3) X(8, 4)
 
 bool fused16_supported(const FusedConfig &c) {
 #define X(T, S_) if (c.ty == T && c.stages == S_) return true;

@@ -281,14 +281,24 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   const int cE = PAD + 4 * lane;
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;  // H(p-1), own cells
   ST *const nxt = reinterpret_cast<ST *>(g.nxt);
-  // 16-bit storage: this thread's largest stored |E|, |H| (bits) in slab `mslab`
+  // 16-bit storage: this thread's largest stored E, H magnitudes in slab
+  // `mslab` (two 16-bit lanes each, compared as integers: one shift per slab
+  // and kind) and that slab's decode scales
   unsigned mxE = 0, mxH = 0;
+  float wsE = 1.0f, wsH = 1.0f;
   int mslab = kfirst / kSlabPlanes;
+  // storage scales, reloaded when plane p or p+1 enters another slab:
+  // decode of planes p (E, H) and p+1 (E), encode and decode of the writes
+  float sEc = 1.0f, sEn = 1.0f, sHc = 1.0f, sEw = 1.0f, iEw = 1.0f, sHw = 1.0f, iHw = 1.0f;
+  int sl_c = -1, sl_n = -1;
   auto flush_max = [&]() {
     if constexpr (SD::k16) {
-      const unsigned e = __reduce_max_sync(0xffffffffu, mxE), h = __reduce_max_sync(0xffffffffu, mxH);
-      if (lane == 0 && e) atomicMax(g.slab_max + 2 * mslab, e);
-      if (lane == 0 && h) atomicMax(g.slab_max + 2 * mslab + 1, h);
+      const unsigned e = __reduce_max_sync(0xffffffffu, max(mxE & 0xffffu, mxE >> 16));
+      const unsigned h = __reduce_max_sync(0xffffffffu, max(mxH & 0xffffu, mxH >> 16));
+      if (lane == 0 && e)
+        atomicMax(g.slab_max + 2 * mslab, __float_as_uint(__fmul_rn(SD::dec_lo(e), wsE)));
+      if (lane == 0 && h)
+        atomicMax(g.slab_max + 2 * mslab + 1, __float_as_uint(__fmul_rn(SD::dec_lo(h), wsH)));
       mxE = mxH = 0;
     }
   };
@@ -350,22 +360,28 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     Psi2 qx = qx_n, qy = qy_n, qz = qz_n;
     HaloPsi hh = hh_n;  // (pml_corr updates its psi argument in place)
 
-    // storage scales: decode of planes p (E, H) and p+1 (E), encode of plane p
-    float sEc = 1.0f, sEn = 1.0f, sHc = 1.0f, sEw = 1.0f, iEw = 1.0f, sHw = 1.0f, iHw = 1.0f;
     if constexpr (SD::k16) {
       const int sl = p / kSlabPlanes, sln = min((p + 1) / kSlabPlanes, g.nslab - 1);
       if (sl != mslab) {
         flush_max();
         mslab = sl;
       }
-      sEc = pow2f(__ldg(g.shift_rd + 2 * sl));
-      sHc = pow2f(__ldg(g.shift_rd + 2 * sl + 1));
-      sEn = pow2f(__ldg(g.shift_rd + 2 * sln));
-      const int we = __ldg(g.shift_wr + 2 * sl), wh = __ldg(g.shift_wr + 2 * sl + 1);
-      sEw = pow2f(we);
-      iEw = pow2f(-we);
-      sHw = pow2f(wh);
-      iHw = pow2f(-wh);
+      if (sl != sl_c) {
+        sl_c = sl;
+        sEc = SD::dscale(__ldg(g.shift_rd + 2 * sl));
+        sHc = SD::dscale(__ldg(g.shift_rd + 2 * sl + 1));
+        const int we = __ldg(g.shift_wr + 2 * sl), wh = __ldg(g.shift_wr + 2 * sl + 1);
+        sEw = SD::dscale(we);
+        iEw = pow2f(-we);
+        sHw = SD::dscale(wh);
+        iHw = pow2f(-wh);
+        wsE = sEw;
+        wsH = sHw;
+      }
+      if (sln != sl_n) {
+        sl_n = sln;
+        sEn = SD::dscale(__ldg(g.shift_rd + 2 * sln));
+      }
     }
 
     const bool arrived = mbar_wait(smem_u32(&s_bar[(j + 1) % S]), ((j + 1) / S) & 1);
@@ -465,10 +481,18 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       }
       // every H value is used as stored (16-bit: rounded here, in place)
       const bool hstore = !warm && tile_warp && cell_ok;
-      unsigned long long *ovf = hstore ? g.ovf : nullptr;
-      const typename SD::Word wa = SD::enc4(ha, iHw, sHw, ovf);
-      const typename SD::Word wb = SD::enc4(hb, iHw, sHw, ovf);
-      const typename SD::Word wc = SD::enc4(hc, iHw, sHw, ovf);
+      const typename SD::Word wa = SD::enc4(ha, iHw);
+      const typename SD::Word wb = SD::enc4(hb, iHw);
+      const typename SD::Word wc = SD::enc4(hc, iHw);
+      if constexpr (SD::k16) {
+        const float4 da = SD::dec4(wa, sHw), db = SD::dec4(wb, sHw), dc = SD::dec4(wc, sHw);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          ha[q] = comp(da, q);
+          hb[q] = comp(db, q);
+          hc[q] = comp(dc, q);
+        }
+      }
       if (!warm) {
         stg4(pl_hz + r * kTileX + 4 * lane, make_float4(hc[0], hc[1], hc[2], hc[3]));
         stg4(pl_hx + r * kTileX + 4 * lane, make_float4(ha[0], ha[1], ha[2], ha[3]));
@@ -478,10 +502,9 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
           SD::st4(Hn + N, wb);
           SD::st4(Hn + 2 * N, wc);
           if constexpr (SD::k16) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              mxH = max(mxH, max(__float_as_uint(fabsf(ha[q])),
-                                 max(__float_as_uint(fabsf(hb[q])), __float_as_uint(fabsf(hc[q])))));
+            mxH = __vmaxu2(mxH, __vmaxu2(__vmaxu2(SD::mag(wa.x), SD::mag(wa.y)),
+                                         __vmaxu2(__vmaxu2(SD::mag(wb.x), SD::mag(wb.y)),
+                                                  __vmaxu2(SD::mag(wc.x), SD::mag(wc.y)))));
           }
         }
       }
@@ -519,8 +542,8 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
                            sub(d_ex_dz1, d_ez_dx1));
           hzv = h_new<FMA>(cf.z, SD::ld1(Hc + (2 * L::HH + rh) * L::HW + PAD - 1, sHc), cf.w,
                            sub(d_ey_dx1, d_ex_dy1));
-          hyv = SD::rt(hyv, iHw, sHw, nullptr);
-          hzv = SD::rt(hzv, iHw, sHw, nullptr);
+          hyv = SD::rt(hyv, iHw, sHw);
+          hzv = SD::rt(hzv, iHw, sHw);
         }
         pl_hzh[rh] = hzv;
         pl_hyh[rh] = hyv;
@@ -593,14 +616,15 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
             eo[2][q] = e_new<FMA>(cf.x, comp(ez4, q), cf.y, sub(d_hy_dx[q], d_hx_dy[q]));
           }
           ST *Ep = nxt + (static_cast<long long>(p) * ny + y) * nx + xg;
-          SD::st4(Ep, SD::enc4(eo[0], iEw, sEw, g.ovf));
-          SD::st4(Ep + N, SD::enc4(eo[1], iEw, sEw, g.ovf));
-          SD::st4(Ep + 2 * N, SD::enc4(eo[2], iEw, sEw, g.ovf));
+          const typename SD::Word w0 = SD::enc4(eo[0], iEw), w1 = SD::enc4(eo[1], iEw),
+                                   w2 = SD::enc4(eo[2], iEw);
+          SD::st4(Ep, w0);
+          SD::st4(Ep + N, w1);
+          SD::st4(Ep + 2 * N, w2);
           if constexpr (SD::k16) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              mxE = max(mxE, max(__float_as_uint(fabsf(eo[0][q])),
-                                 max(__float_as_uint(fabsf(eo[1][q])), __float_as_uint(fabsf(eo[2][q])))));
+            mxE = __vmaxu2(mxE, __vmaxu2(__vmaxu2(SD::mag(w0.x), SD::mag(w0.y)),
+                                         __vmaxu2(__vmaxu2(SD::mag(w1.x), SD::mag(w1.y)),
+                                                  __vmaxu2(SD::mag(w2.x), SD::mag(w2.y)))));
           }
         }
       }

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/wavefront_gpu.h"
+#include "wf_scene.h"
 
 namespace {
 
@@ -193,11 +194,71 @@ void wf_spectrum(const double *sum_cos, const double *sum_sin, uint64_t n,
 wf_status wf_scene_voxelize(const char *text, int nx, int ny, int nz, float dt,
                             float dx, uint8_t *grid, int32_t (*table)[4],
                             int *n_materials, char *err, int errlen) {
-  auto fail = [&](const std::string &msg) {
-    if (err && errlen > 0) std::snprintf(err, errlen, "%s", msg.c_str());
+  std::vector<wf::RasterOp> ops;
+  std::string msg;
+  if (!grid || !wf::scene_parse(text, nx, ny, nz, dt, dx, &ops, table, n_materials, &msg)) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", grid ? msg.c_str() : "null argument");
     return WF_ERR_ARG;
+  }
+  for (const wf::RasterOp &op : ops) {
+    if (op.sphere) {
+      for (long long z = op.z0; z < op.z1; ++z)
+        for (long long y = op.y0; y < op.y1; ++y)
+          for (long long x = op.x0; x < op.x1; ++x) {
+            // cell-centre test x + 0.5 - cx, src/scene.rs:198-204
+            const float ddx = static_cast<float>(x) + 0.5f - op.cx;
+            const float ddy = static_cast<float>(y) + 0.5f - op.cy;
+            const float ddz = static_cast<float>(z) + 0.5f - op.cz;
+            if (ddx * ddx + ddy * ddy + ddz * ddz <= op.r2)
+              grid[(static_cast<size_t>(z) * ny + y) * nx + x] = op.id;
+          }
+    } else {
+      for (long long z = op.z0; z < op.z1; ++z)
+        for (long long y = op.y0; y < op.y1; ++y)
+          for (long long x = op.x0; x < op.x1; ++x)
+            grid[(static_cast<size_t>(z) * ny + y) * nx + x] = op.id;
+    }
+  }
+  return WF_OK;
+}
+
+void wf_demo_sphere(int nx, int ny, int nz, uint8_t *grid) {
+  const float r = static_cast<float>(std::min(nx, std::min(ny, nz))) / 4.0f;
+  sphere_fill(grid, nx, ny, nz, static_cast<float>(nx) / 2.0f, static_cast<float>(ny) / 2.0f,
+              static_cast<float>(nz) / 2.0f, r, 1);
+}
+
+}  // extern "C"
+
+namespace wf {
+
+namespace {
+
+// Integer cell range [lo, hi) that contains every cell centre within r of c
+// on one axis (a margin of 2 cells covers the f32 rounding of the test);
+// the whole axis when c or r is not finite.
+void sphere_range(float c, float r, int n, long long *lo, long long *hi) {
+  if (!std::isfinite(c) || !std::isfinite(r)) {
+    *lo = 0;
+    *hi = n;
+    return;
+  }
+  const double a = std::floor(static_cast<double>(c) - std::fabs(static_cast<double>(r))) - 2.0;
+  const double b = std::ceil(static_cast<double>(c) + std::fabs(static_cast<double>(r))) + 2.0;
+  *lo = static_cast<long long>(std::max(0.0, std::min(a, static_cast<double>(n))));
+  *hi = static_cast<long long>(std::max(0.0, std::min(b, static_cast<double>(n))));
+}
+
+}  // namespace
+
+bool scene_parse(const char *text, int nx, int ny, int nz, float dt, float dx,
+                 std::vector<RasterOp> *ops, int32_t (*table)[4], int *n_materials,
+                 std::string *err) {
+  auto fail = [&](const std::string &msg) {
+    *err = msg;
+    return false;
   };
-  if (!text || !grid || !table) return fail("null argument");
+  if (!text || !table) return fail("null argument");
   // Scene::parse, src/scene.rs:81-143: every line first, then voxelize.
   std::vector<Primitive> prims;
   const std::string all(text);
@@ -215,10 +276,10 @@ wf_status wf_scene_voxelize(const char *text, int nx, int ny, int nz, float dt,
         std::vector<std::string> toks;
         size_t p = 0;
         while (p < line.size()) {
-          const size_t s = line.find_first_not_of(ws, p);
-          if (s == std::string::npos) break;
-          const size_t e = line.find_first_of(ws, s);
-          toks.push_back(line.substr(s, e == std::string::npos ? std::string::npos : e - s));
+          const size_t s0 = line.find_first_not_of(ws, p);
+          if (s0 == std::string::npos) break;
+          const size_t e = line.find_first_of(ws, s0);
+          toks.push_back(line.substr(s0, e == std::string::npos ? std::string::npos : e - s0));
           p = e == std::string::npos ? line.size() : e;
         }
         const bool sphere = toks[0] == "sphere", box = toks[0] == "box";
@@ -250,6 +311,7 @@ wf_status wf_scene_voxelize(const char *text, int nx, int ny, int nz, float dt,
   }
   // Scene::voxelize, src/scene.rs:149-188: ids de-duplicated by bit pattern.
   std::vector<std::array<uint32_t, 3>> keys;
+  ops->clear();
   for (const Primitive &pr : prims) {
     std::array<uint32_t, 3> key;
     std::memcpy(key.data(), pr.v, 12);
@@ -262,30 +324,35 @@ wf_status wf_scene_voxelize(const char *text, int nx, int ny, int nz, float dt,
       id = static_cast<int>(keys.size());
       wf_material_coeffs(pr.v[0], pr.v[1], pr.v[2], dt, dx, table[id]);
     }
+    RasterOp op{};
+    op.id = static_cast<uint8_t>(id);
     if (pr.sphere) {
-      sphere_fill(grid, nx, ny, nz, pr.v[3], pr.v[4], pr.v[5], pr.v[6], static_cast<uint8_t>(id));
+      op.sphere = 1;
+      op.cx = pr.v[3];
+      op.cy = pr.v[4];
+      op.cz = pr.v[5];
+      op.r2 = pr.v[6] * pr.v[6];
+      sphere_range(op.cx, pr.v[6], nx, &op.x0, &op.x1);
+      sphere_range(op.cy, pr.v[6], ny, &op.y0, &op.y1);
+      sphere_range(op.cz, pr.v[6], nz, &op.z0, &op.z1);
     } else {
       // src/scene.rs:212-226: floor/ceil clamps
       auto lo = [](float v) { return sat_usize(std::floor(std::fmax(v, 0.0f))); };
       auto hi = [](float v, int n) {
         return std::min(sat_usize(std::fmax(std::ceil(v), 0.0f)), static_cast<size_t>(n));
       };
-      const size_t x0 = lo(std::fmin(pr.v[3], pr.v[6])), x1 = hi(std::fmax(pr.v[3], pr.v[6]), nx);
-      const size_t y0 = lo(std::fmin(pr.v[4], pr.v[7])), y1 = hi(std::fmax(pr.v[4], pr.v[7]), ny);
-      const size_t z0 = lo(std::fmin(pr.v[5], pr.v[8])), z1 = hi(std::fmax(pr.v[5], pr.v[8]), nz);
-      for (size_t z = z0; z < z1; ++z)
-        for (size_t y = y0; y < y1; ++y)
-          for (size_t x = x0; x < x1; ++x) grid[(z * ny + y) * nx + x] = static_cast<uint8_t>(id);
+      auto clamp = [](size_t v, int n) { return static_cast<long long>(std::min(v, static_cast<size_t>(n))); };
+      op.x0 = clamp(lo(std::fmin(pr.v[3], pr.v[6])), nx);
+      op.x1 = static_cast<long long>(hi(std::fmax(pr.v[3], pr.v[6]), nx));
+      op.y0 = clamp(lo(std::fmin(pr.v[4], pr.v[7])), ny);
+      op.y1 = static_cast<long long>(hi(std::fmax(pr.v[4], pr.v[7]), ny));
+      op.z0 = clamp(lo(std::fmin(pr.v[5], pr.v[8])), nz);
+      op.z1 = static_cast<long long>(hi(std::fmax(pr.v[5], pr.v[8]), nz));
     }
+    ops->push_back(op);
   }
   if (n_materials) *n_materials = static_cast<int>(keys.size());
-  return WF_OK;
+  return true;
 }
 
-void wf_demo_sphere(int nx, int ny, int nz, uint8_t *grid) {
-  const float r = static_cast<float>(std::min(nx, std::min(ny, nz))) / 4.0f;
-  sphere_fill(grid, nx, ny, nz, static_cast<float>(nx) / 2.0f, static_cast<float>(ny) / 2.0f,
-              static_cast<float>(nz) / 2.0f, r, 1);
-}
-
-}  // extern "C"
+}  // namespace wf

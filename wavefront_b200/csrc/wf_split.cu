@@ -152,19 +152,17 @@ __global__ void k_split_e(GridArgs g) {
 
 // One stored value of a 16-bit state: decode / encode with a shift.
 __device__ __forceinline__ float dec16(const void *f, long long i, int prec, int shift) {
-  const unsigned short b = static_cast<const unsigned short *>(f)[i];
-  const float v = prec == kPrecF16 ? Store16<__half>::dec1(b) : Store16<__nv_bfloat16>::dec1(b);
-  return __fmul_rn(v, pow2f(shift));
+  const unsigned b = static_cast<const unsigned short *>(f)[i];
+  return prec == kPrecF16 ? __fmul_rn(Store<__half>::dec_lo(b), Store<__half>::dscale(shift))
+                          : __fmul_rn(Store<__nv_bfloat16>::dec_lo(b),
+                                      Store<__nv_bfloat16>::dscale(shift));
 }
 // stores v; returns the decoded stored value
-__device__ __forceinline__ float enc16(void *f, long long i, int prec, int shift, float v,
-                                       unsigned long long *ovf) {
+__device__ __forceinline__ float enc16(void *f, long long i, int prec, int shift, float v) {
   const float u = __fmul_rn(v, pow2f(-shift));
-  const unsigned short b =
-      prec == kPrecF16 ? Store16<__half>::enc1(u, ovf) : Store16<__nv_bfloat16>::enc1(u, ovf);
-  static_cast<unsigned short *>(f)[i] = b;
-  const float d = prec == kPrecF16 ? Store16<__half>::dec1(b) : Store16<__nv_bfloat16>::dec1(b);
-  return __fmul_rn(d, pow2f(shift));
+  const unsigned w = prec == kPrecF16 ? Store16<__half>::enc2(u, u) : Store16<__nv_bfloat16>::enc2(u, u);
+  static_cast<unsigned short *>(f)[i] = static_cast<unsigned short>(w & 0xffffu);
+  return dec16(f, i, prec, shift);
 }
 
 // Write shifts of the step with index `next`, from the slab maxima of the
@@ -174,7 +172,15 @@ __device__ __forceinline__ float enc16(void *f, long long i, int prec, int shift
 // doubled by the CPML correction), and the soft-source amplitudes that
 // step adds:  bh = 2*NH + kh*NE,  be = 2*NE + ke*bh + src  (f32, this
 // order); shift = store_shift_bits(bound).  Whole CTA; s_src >= nslab.
-__device__ void next_shifts(const TailArgs &t, long long next, float *s_src) {
+// count_sat (after a step, binary16): every slab and kind whose maximum is
+// binary16's largest finite magnitude (where .satfinite puts overflowing
+// values) adds one to *ovf.
+__device__ void next_shifts(const TailArgs &t, long long next, float *s_src, bool count_sat) {
+  if (count_sat && t.prec == kPrecF16) {
+    for (int k = threadIdx.x; k < 2 * t.nslab; k += blockDim.x)
+      if (t.slab_max[k] == __float_as_uint(__fmul_rn(65504.0f, pow2f(t.shift_f[k]))))
+        atomicAdd(t.ovf, 1ull);
+  }
   for (int b = threadIdx.x; b < t.nslab; b += blockDim.x) s_src[b] = 0.0f;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -235,7 +241,7 @@ __global__ void k_tail(TailArgs t) {
         const long long i = q.comp * N + (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x;
         if (f16) {
           const int b = q.z / kSlabPlanes, sh = t.shift_f[2 * b];
-          const float d = enc16(t.f, i, t.prec, sh, __fadd_rn(dec16(t.f, i, t.prec, sh), v), t.ovf);
+          const float d = enc16(t.f, i, t.prec, sh, __fadd_rn(dec16(t.f, i, t.prec, sh), v));
           t.slab_max[2 * b] = max(t.slab_max[2 * b], __float_as_uint(fabsf(d)));
         } else {
           t.f[i] = __fadd_rn(t.f[i], v);
@@ -248,7 +254,7 @@ __global__ void k_tail(TailArgs t) {
         const long long i = q.comp * N + (zz * t.ny + yy) * t.nx + q.x;
         if (f16) {
           const int b = static_cast<int>(zz) / kSlabPlanes;
-          const float d = enc16(t.f, i, t.prec, t.shift_f[2 * b], v, t.ovf);
+          const float d = enc16(t.f, i, t.prec, t.shift_f[2 * b], v);
           atomicMax(t.slab_max + 2 * b, __float_as_uint(fabsf(d)));
         } else {
           t.f[i] = v;
@@ -273,13 +279,13 @@ __global__ void k_tail(TailArgs t) {
     }
   }
   __syncthreads();
-  if (f16) next_shifts(t, st + 1, s_src);
+  if (f16) next_shifts(t, st + 1, s_src, true);
   if (threadIdx.x == 0) *t.step = st + 1;
 }
 
 __global__ void k_next_shifts(TailArgs t, long long next) {
   __shared__ float s_src[kMaxSlabs];
-  next_shifts(t, next, s_src);
+  next_shifts(t, next, s_src, false);
 }
 
 // 16-bit state from FP32 values, in three passes: slab maxima of the input,
@@ -299,12 +305,12 @@ __global__ void k_shift_from_max(unsigned *slab_max, int *shift, int n) {
   slab_max[i] = 0u;
 }
 __global__ void k_encode(const float *in, void *out, int prec, long long N, int nxy,
-                         const int *shift, unsigned *slab_max, unsigned long long *ovf) {
+                         const int *shift, unsigned *slab_max) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= 6 * N) return;
   const int c = static_cast<int>(i / N);
   const int k = 2 * (static_cast<int>((i % N) / nxy) / kSlabPlanes) + (c >= 3);
-  const float d = enc16(out, i, prec, shift[k], in[i], ovf);
+  const float d = enc16(out, i, prec, shift[k], in[i]);
   const unsigned v = __float_as_uint(fabsf(d));
   if (v) atomicMax(slab_max + k, v);
 }
@@ -385,7 +391,8 @@ cudaError_t launch_encode_state(const float *in, void *out, int prec, int nx, in
   if (e != cudaSuccess) return e;
   k_slab_max_f32<<<blocks, 256, 0, s>>>(in, N, nx * ny, slab_max);
   k_shift_from_max<<<(2 * nslab + 255) / 256, 256, 0, s>>>(slab_max, shift, 2 * nslab);
-  k_encode<<<blocks, 256, 0, s>>>(in, out, prec, N, nx * ny, shift, slab_max, ovf);
+  (void)ovf;  // encoding a given state saturates nothing it has to report
+  k_encode<<<blocks, 256, 0, s>>>(in, out, prec, N, nx * ny, shift, slab_max);
   return cudaGetLastError();
 }
 

@@ -4,11 +4,11 @@
 // field value as a 16-bit number (IEEE binary16 or bfloat16) of v * 2^-shift,
 // where the power-of-two shift belongs to the value's z slab (8 planes) and
 // kind (E or H); all arithmetic stays FP32.  Encoding is round to nearest
-// even (binary16 saturates finite values at +-65504 and counts them);
-// decoding multiplies by 2^shift, which is exact, so a kernel that rounds a
-// value it has just computed ("round trip") sees exactly the value any later
-// reader decodes.  The per-slab shifts are chosen between steps from the
-// slab maxima (see k_tail in wf_split.cu).
+// even (binary16 saturates finite values at +-65504); decoding moves the 16
+// bits into an FP32 value and multiplies by a power of two, both
+// exact, so a kernel that rounds a value it has just computed ("round trip")
+// sees exactly the value any later reader decodes.  The per-slab shifts are
+// chosen between steps from the slab maxima (see k_tail in wf_split.cu).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -30,80 +30,111 @@ struct Store<float> {
   using Word = float4;
   __device__ static float4 ld4(const float *p, float) { return *reinterpret_cast<const float4 *>(p); }
   __device__ static float ld1(const float *p, float) { return *p; }
-  __device__ static float rt(float v, float, float, unsigned long long *) { return v; }
-  __device__ static Word enc4(float v[4], float, float, unsigned long long *) {
-    return make_float4(v[0], v[1], v[2], v[3]);
-  }
+  __device__ static float rt(float v, float, float) { return v; }
+  __device__ static Word enc4(const float v[4], float) { return make_float4(v[0], v[1], v[2], v[3]); }
   __device__ static void st4(float *p, const Word &w) { *reinterpret_cast<float4 *>(p) = w; }
 };
 
+// Two values per conversion: cvt packs its first operand into the upper
+// half of the word.  binary16 saturates finite values at +-65504
+// (.satfinite); bfloat16 has FP32's range.
+//
+// Decoding: bfloat16 is the upper half of an FP32 pattern (a bit move);
+// binary16 converts exactly in hardware; dscale(shift) = 2^(shift + bias)
+// then restores the stored scale.
 template <typename H>
 struct Store16 {
   static constexpr bool k16 = true;
   static constexpr int PAD = 8;
-  using Word = uint2;
-  __device__ static unsigned short enc1(float u, unsigned long long *ovf);
-  __device__ static float dec1(unsigned short b);
+  using Word = uint2;  // 4 values, x ascending from the low half of .x
+  // encode (lo, hi) -> one word (lo in bits 0-15)
+  __device__ static unsigned enc2(float lo, float hi);
+  // bit-moved (not yet scaled) low / high value of a word
+  __device__ static float dec_lo(unsigned w);
+  __device__ static float dec_hi(unsigned w);
+  __device__ static float4 dec4(const Word &w, float s) {
+    return make_float4(__fmul_rn(dec_lo(w.x), s), __fmul_rn(dec_hi(w.x), s),
+                       __fmul_rn(dec_lo(w.y), s), __fmul_rn(dec_hi(w.y), s));
+  }
   // decoded values of 4 stored halves at p (8-byte aligned), times scale s
   __device__ static float4 ld4(const H *p, float s) {
-    const uint2 w = *reinterpret_cast<const uint2 *>(p);
-    return make_float4(__fmul_rn(dec1(w.x & 0xffffu), s), __fmul_rn(dec1(w.x >> 16), s),
-                       __fmul_rn(dec1(w.y & 0xffffu), s), __fmul_rn(dec1(w.y >> 16), s));
+    return dec4(*reinterpret_cast<const uint2 *>(p), s);
   }
   __device__ static float ld1(const H *p, float s) {
-    return __fmul_rn(dec1(*reinterpret_cast<const unsigned short *>(p)), s);
+    return __fmul_rn(dec_lo(*reinterpret_cast<const unsigned short *>(p)), s);
   }
-  // the value a reader decodes after v is stored (inv = 2^-shift, s = 2^shift)
-  __device__ static float rt(float v, float inv, float s, unsigned long long *ovf) {
-    return __fmul_rn(dec1(enc1(__fmul_rn(v, inv), ovf)), s);
+  // the value a reader decodes after v is stored (inv = 2^-shift, s = dscale)
+  __device__ static float rt(float v, float inv, float s) {
+    const float u = __fmul_rn(v, inv);
+    return __fmul_rn(dec_lo(enc2(u, u)), s);
   }
-  // encodes 4 values, replacing each by its decoded value; returns the word
-  __device__ static Word enc4(float v[4], float inv, float s, unsigned long long *ovf) {
-    unsigned short b[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      b[i] = enc1(__fmul_rn(v[i], inv), ovf);
-      v[i] = __fmul_rn(dec1(b[i]), s);
-    }
-    return make_uint2(b[0] | (static_cast<unsigned>(b[1]) << 16),
-                      b[2] | (static_cast<unsigned>(b[3]) << 16));
+  // the stored word of 4 values v * inv
+  __device__ static Word enc4(const float v[4], float inv) {
+    return make_uint2(enc2(__fmul_rn(v[0], inv), __fmul_rn(v[1], inv)),
+                      enc2(__fmul_rn(v[2], inv), __fmul_rn(v[3], inv)));
   }
   __device__ static void st4(H *p, const Word &w) { *reinterpret_cast<uint2 *>(p) = w; }
+  // per-half magnitudes (sign bits cleared): non-negative 16-bit floats of
+  // one shift order like these integers
+  __device__ static unsigned mag(unsigned w) { return w & 0x7fff7fffu; }
 };
 
-// ovf may be null (values that are recomputed, not stored, are not counted)
+template <typename H>
+struct DecBias;
 template <>
-__device__ __forceinline__ unsigned short Store16<__half>::enc1(float u, unsigned long long *ovf) {
-  if (u > 65504.0f || u < -65504.0f) {
-    if (ovf) atomicAdd(ovf, 1ull);
-    u = u > 0.0f ? 65504.0f : -65504.0f;
-  }
-  return __half_as_ushort(__float2half_rn(u));
+struct DecBias<__half> {
+  static constexpr int v = 0;  // hardware conversion (a bit move measured slower)
+};
+template <>
+struct DecBias<__nv_bfloat16> {
+  static constexpr int v = 0;
+};
+
+template <>
+__device__ __forceinline__ unsigned Store16<__half>::enc2(float lo, float hi) {
+  unsigned r;
+  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
 }
 template <>
-__device__ __forceinline__ float Store16<__half>::dec1(unsigned short b) {
-  return __half2float(__ushort_as_half(b));
+__device__ __forceinline__ float Store16<__half>::dec_lo(unsigned w) {
+  return __half2float(__ushort_as_half(static_cast<unsigned short>(w & 0xffffu)));
 }
 template <>
-__device__ __forceinline__ unsigned short Store16<__nv_bfloat16>::enc1(float u, unsigned long long *) {
-  return __bfloat16_as_ushort(__float2bfloat16_rn(u));
+__device__ __forceinline__ float Store16<__half>::dec_hi(unsigned w) {
+  return __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16)));
 }
 template <>
-__device__ __forceinline__ float Store16<__nv_bfloat16>::dec1(unsigned short b) {
-  return __bfloat162float(__ushort_as_bfloat16(b));
+__device__ __forceinline__ unsigned Store16<__nv_bfloat16>::enc2(float lo, float hi) {
+  unsigned r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+template <>
+__device__ __forceinline__ float Store16<__nv_bfloat16>::dec_lo(unsigned w) {
+  return __uint_as_float(w << 16);
+}
+template <>
+__device__ __forceinline__ float Store16<__nv_bfloat16>::dec_hi(unsigned w) {
+  return __uint_as_float(w & 0xffff0000u);
 }
 
 template <>
-struct Store<__half> : Store16<__half> {};
+struct Store<__half> : Store16<__half> {
+  __device__ static float dscale(int shift) { return pow2f(shift + DecBias<__half>::v); }
+};
 template <>
-struct Store<__nv_bfloat16> : Store16<__nv_bfloat16> {};
+struct Store<__nv_bfloat16> : Store16<__nv_bfloat16> {
+  __device__ static float dscale(int shift) { return pow2f(shift); }
+};
 
 // Shift mapping a bound into [2^13, 2^14): biased exponent of the bound minus
-// 140, clamped to [-60, 60] (zero or subnormal bounds take -60).
+// 140, clamped to [-60, 15] (zero or subnormal bounds take -60; the upper
+// clamp keeps 2^(shift + 112) an FP32 normal for the binary16 decode).
 __host__ __device__ __forceinline__ int store_shift_bits(unsigned bits) {
   const int e8 = static_cast<int>((bits >> 23) & 0xffu);
   const int sh = e8 == 0 ? -60 : e8 - 127 - 13;
-  return sh < -60 ? -60 : (sh > 60 ? 60 : sh);
+  return sh < -60 ? -60 : (sh > 15 ? 15 : sh);
 }
 
 }  // namespace wf

@@ -79,6 +79,23 @@ class DeviceFieldGrid:
         q = np.ascontiguousarray(table.q16, np.int32)
         self._chk(_L.lib().wf_set_materials(self._h, _L.ptr(ids, _L.u8p), _L.ptr(q, _L.i32p)))
 
+    def set_scene(self, text: str, table: MaterialTable, dt: float, dx: float) -> int:
+        """Scene text voxelized on the device (ids start as vacuum 0); the
+        registered materials are written into `table`, which becomes the
+        coefficient table.  Returns the number of registered materials."""
+        q = np.ascontiguousarray(table.q16, np.int32)
+        n = C.c_int()
+        self._chk(_L.lib().wf_set_scene(self._h, text.encode(), dt, dx, _L.ptr(q, _L.i32p),
+                                        C.byref(n)))
+        table.q16[:] = q
+        return n.value
+
+    def materials(self) -> np.ndarray:
+        """The device material ids, nz*ny*nx bytes."""
+        out = np.empty(self.dims.voxel_count(), np.uint8)
+        self._chk(_L.lib().wf_get_materials(self._h, _L.ptr(out, _L.u8p)))
+        return out
+
     def set_pml(self, ctx: PmlContext):
         for axis in range(3):
             p = ctx.profiles[axis]
@@ -125,7 +142,8 @@ class DeviceFieldGrid:
 
     def storage_info(self):
         """16-bit storage: (E shifts, H shifts) the next step stores with, per
-        8-plane z slab, and the number of binary16 saturations so far."""
+        8-plane z slab, and the saturation count: one per step, slab and kind
+        whose largest stored binary16 magnitude was 65504."""
         nslab = self.dims.nz // 8
         e = (C.c_int * nslab)()
         h = (C.c_int * nslab)()
