@@ -220,6 +220,36 @@ wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t);
 /* Times each candidate tiling for `steps` steps and keeps the fastest. */
 wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms);
 
+/* ---- batched stepping (no reference counterpart) ------------------------ */
+
+/* Many independent grids of uneven size stepped together: each step is one
+ * persistent kernel launch over the work items (tile x z chunk) of every
+ * grid, then one tail launch for every grid's sources and probes; runs of
+ * 32 steps replay a captured CUDA graph.  The grids are ordinary handles,
+ * created on the batch's stream: set them up and read them back with the
+ * per-grid calls through wf_batch_handle (wf_step on one of them is allowed
+ * but breaks the lockstep that wf_batch_step requires).  Every grid needs
+ * FP32 storage, the exact arithmetic, zero-field boundaries and CPML slabs
+ * of at most 64 cells; results equal wf_step's bit for bit. */
+typedef struct wf_batch wf_batch;
+wf_status wf_batch_create(int n, const wf_grid_desc *descs, wf_batch **out);
+wf_status wf_batch_destroy(wf_batch *b);
+int wf_batch_size(const wf_batch *b);
+wf_handle *wf_batch_handle(wf_batch *b, int i);
+/* Steps every grid nsteps times (all must have taken the same steps). */
+wf_status wf_batch_step(wf_batch *b, int nsteps);
+/* Waits for the batch's stream; reports any grid's latched device error. */
+wf_status wf_batch_sync(wf_batch *b);
+wf_status wf_batch_get_stream(wf_batch *b, void **out_stream);
+/* Kernel launches issued for batched steps so far (graph replays included). */
+int64_t wf_batch_kernel_launches(const wf_batch *b);
+wf_status wf_batch_get_tiling(const wf_batch *b, wf_tiling *out);
+wf_status wf_batch_set_tiling(wf_batch *b, const wf_tiling *t);
+/* Times the batched step kernel for `steps` steps under each instantiated
+ * tiling and z chunk, keeps the fastest, and restores every grid's fields
+ * and psi (sources and probes do not run during the trials). */
+wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best_ms);
+
 /* ---- allocation-free stepping of caller-owned fields --------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

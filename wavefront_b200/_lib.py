@@ -19,6 +19,9 @@ EXPORTS = [
     "wf_create", "wf_destroy", "wf_last_error", "wf_status_string", "wf_set_materials",
     "wf_set_pml", "wf_add_source", "wf_add_probe", "wf_step", "wf_sync", "wf_steps_done",
     "wf_kernel_launches", "wf_storage_info", "wf_set_scene", "wf_get_materials",
+    "wf_batch_create", "wf_batch_destroy", "wf_batch_size", "wf_batch_handle", "wf_batch_step",
+    "wf_batch_sync", "wf_batch_get_stream", "wf_batch_kernel_launches", "wf_batch_get_tiling",
+    "wf_batch_set_tiling", "wf_batch_autotune",
     "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
     "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
     "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
@@ -96,6 +99,28 @@ def lib() -> C.CDLL:
         L.wf_set_scene.restype = S
         L.wf_get_materials.argtypes = [_h, _u8p]
         L.wf_get_materials.restype = S
+        L.wf_batch_create.argtypes = [C.c_int, C.POINTER(GridDesc), C.POINTER(_h)]
+        L.wf_batch_create.restype = S
+        L.wf_batch_destroy.argtypes = [_h]
+        L.wf_batch_destroy.restype = S
+        L.wf_batch_size.argtypes = [_h]
+        L.wf_batch_size.restype = C.c_int
+        L.wf_batch_handle.argtypes = [_h, C.c_int]
+        L.wf_batch_handle.restype = _h
+        L.wf_batch_step.argtypes = [_h, C.c_int]
+        L.wf_batch_step.restype = S
+        L.wf_batch_sync.argtypes = [_h]
+        L.wf_batch_sync.restype = S
+        L.wf_batch_get_stream.argtypes = [_h, C.POINTER(C.c_void_p)]
+        L.wf_batch_get_stream.restype = S
+        L.wf_batch_kernel_launches.argtypes = [_h]
+        L.wf_batch_kernel_launches.restype = C.c_int64
+        L.wf_batch_get_tiling.argtypes = [_h, C.POINTER(Tiling)]
+        L.wf_batch_get_tiling.restype = S
+        L.wf_batch_set_tiling.argtypes = [_h, C.POINTER(Tiling)]
+        L.wf_batch_set_tiling.restype = S
+        L.wf_batch_autotune.argtypes = [_h, C.c_int, C.POINTER(Tiling), _f32p]
+        L.wf_batch_autotune.restype = S
         L.wf_probe_sums.argtypes = [_h, C.c_int, _f64p, _f64p, C.POINTER(C.c_uint64)]
         L.wf_probe_sums.restype = S
         L.wf_probe_trace.argtypes = [_h, C.c_int, _f32p, C.c_int]

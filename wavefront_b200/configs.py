@@ -133,6 +133,70 @@ def random_spheres(n: int = 1024, steps: int = 2000, pml_cells: int = 16,
                     {"f": f, "seed": seed}, scene_text=text if device_voxelize else None)
 
 
+def batched_sweep(n_scenes: int = 256, steps: int = 800, seed: int = 4321,
+                  sizes=(32, 48, 64, 96, 128), pml_cells: int = 10) -> List[Scenario]:
+    """Batched workload: `n_scenes` independent cubes drawn from numpy's PCG64
+    stream `seed`: edge uniform over `sizes`; 1-4 primitives (sphere: centre
+    U[0,n), radius U[n/16, n/4]; box: corner U[0,n), extents U[n/8, n/2]),
+    eps_r U[1,8], mu_r 1, sigma 0; a 10-cell CPML graded per cell (the
+    exact mode: the reference's block rounding would make a 32^3 cube all
+    CPML); a Ricker Ez source at a random interior point with 15-30 cells
+    per wavelength; one Ez probe at another interior point at the source
+    frequency; `steps` steps each."""
+    rng = np.random.default_rng(seed)
+    dx = 1.0e-3
+    dt = courant_dt(dx)
+    out = []
+    for k in range(n_scenes):
+        n = int(rng.choice(sizes))
+        lines = []
+        for _ in range(int(rng.integers(1, 5))):
+            eps = rng.uniform(1.0, 8.0)
+            if rng.random() < 0.5:
+                c = rng.uniform(0.0, n, 3)
+                r = rng.uniform(n / 16.0, n / 4.0)
+                lines.append(f"sphere {eps:.6f} 1.0 0.0 {c[0]:.4f} {c[1]:.4f} {c[2]:.4f} {r:.4f}")
+            else:
+                c = rng.uniform(0.0, n, 3)
+                e = rng.uniform(n / 8.0, n / 2.0, 3)
+                lines.append(f"box {eps:.6f} 1.0 0.0 {c[0]:.4f} {c[1]:.4f} {c[2]:.4f} "
+                             f"{c[0] + e[0]:.4f} {c[1] + e[1]:.4f} {c[2] + e[2]:.4f}")
+        text = "\n".join(lines) + "\n"
+        lo, hi = pml_cells + 2, n - pml_cells - 2
+        sx, sy, sz = (int(v) for v in rng.integers(lo, hi, 3))
+        px, py, pz = (int(v) for v in rng.integers(lo, hi, 3))
+        ppw = rng.uniform(15.0, 30.0)
+        f = float(np.float32(C0 / (ppw * dx)))
+        dims = GridDims(n, n, n)
+        grid = MaterialGrid(dims)
+        table = MaterialTable.vacuum_filled(dt, dx)
+        Scene.parse(text).voxelize(grid, table, dt, dx)
+        pml = PmlContext.build_exact(dims, PmlConfig(thickness=pml_cells), dt, dx)
+        src = Source(sx, sy, sz, FieldComponent.Ez, 1.0, default_waveform("ricker", f))
+        prb = Probe(px, py, pz, PC.Ez, [f], 0.0)
+        out.append(Scenario(f"batch_{k}_{n}", dims, dx, dt, grid, table, pml, [src], [prb], steps,
+                            {"f": f, "scene": text}))
+    return out
+
+
+def device_batch(scenes: List[Scenario], steps: Optional[int] = None, device: int = 0):
+    """A DeviceBatch with every scenario's materials, CPML, source values and
+    probe tables loaded (tables for `steps` steps, default each scenario's)."""
+    from .engine import DeviceBatch
+    b = DeviceBatch([sc.dims for sc in scenes], device=device)
+    for g, sc in zip(b.grids, scenes):
+        n = sc.steps if steps is None else steps
+        g.set_materials(sc.grid, sc.table)
+        if sc.pml is not None:
+            g.set_pml(sc.pml)
+        for s_ in sc.sources:
+            g.add_source_values(s_.x, s_.y, s_.z, s_.component, s_.values(sc.dt, n), s_.mode)
+        for p_ in sc.probes:
+            c, si = p_.tables(sc.dt, n)
+            g.add_probe_tables(p_.x, p_.y, p_.z, p_.component, c, si, p_.first_step(sc.dt))
+    return b
+
+
 def demo_sphere_cube(n: int = 256, steps: int = 150, pml_cells: int = 8) -> Scenario:
     dims = GridDims(n, n, n)
     dx, dt = 1.0e-3, 1.5e-12

@@ -81,6 +81,7 @@ struct wf_handle {
   long long *d_step = nullptr;
   int *d_err = nullptr;
   long long steps_done = 0;
+  long long version = 0;               // bumped when device tables are reallocated
   long long kernel_launches = 0;       // step + tail kernels issued so far
   long long graph_kernels[2] = {0, 0};  // kernels in one replay of graph[parity]
   FusedConfig cfg{4, 12, 3};
@@ -376,6 +377,7 @@ wf_status refresh_shifts(wf_handle *h) {
 
 wf_status upload_src_probe_tables(wf_handle *h) {
   drop_graphs(h);
+  ++h->version;
   h->shifts_dirty = true;  // source amplitudes enter the 16-bit shifts
   if (h->d_src) cudaFree(h->d_src);
   if (h->d_probe) cudaFree(h->d_probe);
@@ -418,6 +420,122 @@ wf_status check_device_error(wf_handle *h) {
   if (flag & wf::kErrTimeout)
     return fail(h, WF_ERR_TIMEOUT, "a device-side bounded wait timed out (TMA stage never arrived)");
   if (flag) return fail(h, WF_ERR_DEVICE_FLAG, "device error flag set: " + std::to_string(flag));
+  return WF_OK;
+}
+
+}  // namespace
+
+// A batch of independent grids stepped by one persistent kernel per step
+// (config: many small scenes of uneven size).  Each grid is an ordinary
+// handle on the batch's stream; the batch keeps device tables describing
+// all of them for the batched step kernel and the batched tail.
+struct wf_batch {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<wf_handle *> h;
+  FusedConfig cfg{4, 16, 3};
+  wf::BatchScene *d_scenes = nullptr;
+  int2 *d_items = nullptr;
+  int n_items = 0;
+  int *d_counter = nullptr;
+  TailArgs *d_tails[2] = {nullptr, nullptr};  // per parity of the state read
+  bool have_tail = false;
+  std::vector<long long> versions;  // handle versions the tables were built from
+  bool built = false;
+  int ctas = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long launches = 0;
+};
+
+namespace {
+
+void batch_drop(wf_batch *b) {
+  for (auto &g : b->graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  cudaFree(b->d_scenes);
+  cudaFree(b->d_items);
+  cudaFree(b->d_tails[0]);
+  cudaFree(b->d_tails[1]);
+  b->d_scenes = nullptr;
+  b->d_items = nullptr;
+  b->d_tails[0] = b->d_tails[1] = nullptr;
+  b->built = false;
+}
+
+// (Re)builds the batch's device tables when any grid's tables changed.
+wf_status batch_build(wf_batch *b) {
+  bool fresh = b->built && b->versions.size() == b->h.size();
+  for (size_t i = 0; fresh && i < b->h.size(); ++i) fresh = b->versions[i] == b->h[i]->version;
+  if (fresh) return WF_OK;
+  batch_drop(b);
+  const size_t n = b->h.size();
+  std::vector<wf::BatchScene> scenes(n);
+  std::vector<int2> items;
+  std::vector<TailArgs> tails[2];
+  b->have_tail = false;
+  for (size_t i = 0; i < n; ++i) {
+    wf_handle *h = b->h[i];
+    for (const AxisState &A : h->ax)
+      if (A.T > 0 && A.W > 64)
+        return fail(nullptr, WF_ERR_UNSUPPORTED, "batched grids need CPML slabs of at most 64 cells");
+    h->cfg = b->cfg;
+    h->cfg_user_set = true;
+    wf_status st = build_maps(h);
+    if (st != WF_OK) return st;
+    const int cur = h->cur;
+    for (int p = 0; p < 2; ++p) {
+      h->cur = p;
+      scenes[i].args[p] = fused_args(h);
+      scenes[i].maps[p][0] = h->maps[p].e;
+      scenes[i].maps[p][1] = h->maps[p].h;
+      scenes[i].maps[p][2] = h->maps[p].m;
+      tails[p].push_back(tail_args(h));
+    }
+    h->cur = cur;
+    if (!h->srcs.empty() || !h->probes.empty()) b->have_tail = true;
+    const FusedArgs &a = scenes[i].args[0];
+    const int nit = a.tiles_x * a.tiles_y * ((h->nz + a.zchunk - 1) / a.zchunk);
+    for (int k = 0; k < nit; ++k) items.push_back(make_int2(static_cast<int>(i), k));
+  }
+  WF_CUDA(nullptr, cudaMalloc(&b->d_scenes, sizeof(wf::BatchScene) * n));
+  WF_CUDA(nullptr, cudaMemcpy(b->d_scenes, scenes.data(), sizeof(wf::BatchScene) * n,
+                              cudaMemcpyHostToDevice));
+  WF_CUDA(nullptr, cudaMalloc(&b->d_items, sizeof(int2) * std::max<size_t>(items.size(), 1)));
+  WF_CUDA(nullptr, cudaMemcpy(b->d_items, items.data(), sizeof(int2) * items.size(),
+                              cudaMemcpyHostToDevice));
+  for (int p = 0; p < 2; ++p) {
+    WF_CUDA(nullptr, cudaMalloc(&b->d_tails[p], sizeof(TailArgs) * n));
+    WF_CUDA(nullptr, cudaMemcpy(b->d_tails[p], tails[p].data(), sizeof(TailArgs) * n,
+                                cudaMemcpyHostToDevice));
+  }
+  b->n_items = static_cast<int>(items.size());
+  WF_CUDA(nullptr, wf::fused_batch_prepare(b->cfg));
+  int sms = 0;
+  WF_CUDA(nullptr, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev));
+  const int per_sm = std::max(1, wf::fused_batch_ctas_per_sm(b->cfg));
+  b->ctas = std::max(1, std::min(sms * per_sm, b->n_items));
+  b->versions.clear();
+  for (wf_handle *h : b->h) b->versions.push_back(h->version);
+  b->built = true;
+  return WF_OK;
+}
+
+// The batched step kernel alone (reads parity `cur`).
+wf_status batch_kernel(wf_batch *b, int cur) {
+  WF_CUDA(nullptr, cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
+  WF_CUDA(nullptr, wf::launch_fused_batch(b->cfg, b->d_scenes, b->d_items, b->n_items,
+                                          b->d_counter, cur, b->ctas, b->stream));
+  return WF_OK;
+}
+
+// One batched step: the step kernel, then the tail of every grid.
+wf_status batch_enqueue(wf_batch *b, int cur) {
+  wf_status st = batch_kernel(b, cur);
+  if (st != WF_OK) return st;
+  if (b->have_tail)
+    WF_CUDA(nullptr, wf::launch_tail_batch(b->d_tails[cur], static_cast<int>(b->h.size()), b->stream));
   return WF_OK;
 }
 
@@ -650,6 +768,7 @@ wf_status wf_set_pml(wf_handle *h, int axis, int T, const float *b, const float 
   const int n = axis == 0 ? h->nx : (axis == 1 ? h->ny : h->nz);
   if (T < 0 || T > n) return fail(h, WF_ERR_ARG, "CPML thickness out of range");
   if (T > 0 && (!b || !a || !ik)) return fail(h, WF_ERR_ARG, "null profile");
+  ++h->version;  // psi and profile arrays are reallocated
   DeviceGuard guard(h->dev);
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   drop_graphs(h);
@@ -1063,6 +1182,7 @@ wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t) {
   drop_graphs(h);
   h->cfg = c;
   h->cfg_user_set = true;
+  ++h->version;
   h->maps_ok = false;
   return WF_OK;
 }
@@ -1136,6 +1256,241 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) 
     WF_CUDA(h, cudaMemset(h->d_step, 0, sizeof(long long)));
     WF_CUDA(h, cudaMemset(h->d_ovf, 0, sizeof(unsigned long long)));
   }
+  if (best) {
+    best->tile_rows = bc.ty;
+    best->z_chunk = bc.zchunk;
+    best->stages = bc.stages;
+  }
+  if (best_ms) *best_ms = bms;
+  return WF_OK;
+}
+
+
+/* ---- batched stepping -------------------------------------------------- */
+
+wf_status wf_batch_create(int n, const wf_grid_desc *descs, wf_batch **out) {
+  if (!out || !descs || n <= 0) return fail(nullptr, WF_ERR_ARG, "bad batch arguments");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    const wf_grid_desc &d = descs[i];
+    if (d.precision != WF_PREC_F32 || d.arith != WF_ARITH_EXACT || d.kernel == WF_KERNEL_SPLIT ||
+        d.boundary[0] || d.boundary[1] || d.boundary[2])
+      return fail(nullptr, WF_ERR_UNSUPPORTED,
+                  "batched grids use FP32 storage, the exact arithmetic and zero-field boundaries");
+    if (d.device != descs[0].device) return fail(nullptr, WF_ERR_ARG, "batched grids share one device");
+  }
+  DeviceGuard guard(descs[0].device);
+  wf_batch *b = new wf_batch();
+  b->dev = descs[0].device;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete b;
+    return cuda_fail(nullptr, e, "cudaStreamCreate");
+  }
+  if ((e = cudaMalloc(&b->d_counter, sizeof(int))) != cudaSuccess) {
+    wf_batch_destroy(b);
+    return cuda_fail(nullptr, e, "cudaMalloc(counter)");
+  }
+  for (int i = 0; i < n; ++i) {
+    wf_grid_desc d = descs[i];
+    d.stream = b->stream;  // one stream orders every grid's calls and the batch steps
+    wf_handle *h = nullptr;
+    wf_status st = wf_create(&d, &h);
+    if (st != WF_OK) {
+      wf_batch_destroy(b);
+      return st;
+    }
+    b->h.push_back(h);
+  }
+  *out = b;
+  return WF_OK;
+}
+
+wf_status wf_batch_destroy(wf_batch *b) {
+  if (!b) return WF_OK;
+  DeviceGuard guard(b->dev);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop(b);
+  for (wf_handle *h : b->h) wf_destroy(h);
+  cudaFree(b->d_counter);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return WF_OK;
+}
+
+int wf_batch_size(const wf_batch *b) { return b ? static_cast<int>(b->h.size()) : 0; }
+
+wf_handle *wf_batch_handle(wf_batch *b, int i) {
+  if (!b || i < 0 || i >= static_cast<int>(b->h.size())) return nullptr;
+  return b->h[i];
+}
+
+wf_status wf_batch_set_tiling(wf_batch *b, const wf_tiling *t) {
+  if (!b || !t) return fail(nullptr, WF_ERR_ARG, "null argument");
+  FusedConfig c{t->tile_rows, t->z_chunk, t->stages};
+  if (!wf::fused_supported(c, wf::kPrecF32)) return fail(nullptr, WF_ERR_ARG, "tiling not instantiated");
+  DeviceGuard guard(b->dev);
+  WF_CUDA(nullptr, cudaStreamSynchronize(b->stream));
+  batch_drop(b);
+  b->cfg = c;
+  return WF_OK;
+}
+
+wf_status wf_batch_get_tiling(const wf_batch *b, wf_tiling *out) {
+  if (!b || !out) return fail(nullptr, WF_ERR_ARG, "null argument");
+  out->tile_rows = b->cfg.ty;
+  out->z_chunk = b->cfg.zchunk;
+  out->stages = b->cfg.stages;
+  return WF_OK;
+}
+
+wf_status wf_batch_step(wf_batch *b, int nsteps) {
+  if (!b) return fail(nullptr, WF_ERR_ARG, "null batch");
+  if (nsteps < 0) return fail(nullptr, WF_ERR_ARG, "negative step count");
+  if (nsteps == 0) return WF_OK;
+  const wf_handle *h0 = b->h[0];
+  std::string why;
+  for (wf_handle *h : b->h) {
+    if (h->steps_done != h0->steps_done || h->cur != h0->cur)
+      return fail(nullptr, WF_ERR_STATE, "batched grids must have taken the same steps");
+    if (!tables_cover(h, h->steps_done + nsteps, &why)) return fail(nullptr, WF_ERR_ARG, why);
+  }
+  DeviceGuard guard(b->dev);
+  wf_status st = batch_build(b);
+  if (st != WF_OK) return st;
+  const int G = 32;  // even: the state buffers return to the same parity
+  int left = nsteps;
+  int cur = h0->cur;
+  while (left >= G) {
+    cudaGraphExec_t &ge = b->graph[cur];
+    if (!ge) {
+      cudaGraph_t graph;
+      WF_CUDA(nullptr, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      wf_status s2 = WF_OK;
+      for (int i = 0; i < G && s2 == WF_OK; ++i) s2 = batch_enqueue(b, (cur + i) & 1);
+      cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+      if (s2 != WF_OK) return s2;
+      if (ec != cudaSuccess) return cuda_fail(nullptr, ec, "cudaStreamEndCapture");
+      ec = cudaGraphInstantiate(&ge, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ec != cudaSuccess) return cuda_fail(nullptr, ec, "cudaGraphInstantiate");
+    }
+    WF_CUDA(nullptr, cudaGraphLaunch(ge, b->stream));
+    b->launches += static_cast<long long>(G) * (b->have_tail ? 2 : 1);
+    left -= G;
+  }
+  for (int i = 0; i < left; ++i) {
+    st = batch_enqueue(b, cur);
+    if (st != WF_OK) return st;
+    b->launches += b->have_tail ? 2 : 1;
+    cur ^= 1;
+  }
+  for (wf_handle *h : b->h) {
+    h->cur = cur;
+    h->steps_done += nsteps;
+  }
+  return WF_OK;
+}
+
+wf_status wf_batch_sync(wf_batch *b) {
+  if (!b) return fail(nullptr, WF_ERR_ARG, "null batch");
+  DeviceGuard guard(b->dev);
+  WF_CUDA(nullptr, cudaStreamSynchronize(b->stream));
+  for (wf_handle *h : b->h) {
+    wf_status st = check_device_error(h);
+    if (st != WF_OK) return st;
+  }
+  return WF_OK;
+}
+
+int64_t wf_batch_kernel_launches(const wf_batch *b) { return b ? b->launches : -1; }
+
+wf_status wf_batch_get_stream(wf_batch *b, void **out) {
+  if (!b || !out) return fail(nullptr, WF_ERR_ARG, "null argument");
+  *out = b->stream;
+  return WF_OK;
+}
+
+wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best_ms) {
+  if (!b || steps <= 0) return fail(nullptr, WF_ERR_ARG, "bad autotune arguments");
+  DeviceGuard guard(b->dev);
+  WF_CUDA(nullptr, cudaStreamSynchronize(b->stream));
+  // Trials advance fields and psi: keep device copies of both and put them back.
+  std::vector<void *> saved;
+  auto free_saved = [&]() {
+    for (void *p : saved) cudaFree(p);
+  };
+  for (wf_handle *h : b->h) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(float) * 6 * h->N) != cudaSuccess) {
+      free_saved();
+      return fail(nullptr, WF_ERR_OOM, "autotune: no room to save the state");
+    }
+    saved.push_back(p);
+    cudaMemcpyAsync(p, h->fld[h->cur], sizeof(float) * 6 * h->N, cudaMemcpyDeviceToDevice, b->stream);
+    for (auto &A : h->ax) {
+      void *q = nullptr;
+      if (A.T > 0) {
+        if (cudaMalloc(&q, sizeof(float) * 4 * A.cells) != cudaSuccess) {
+          free_saved();
+          return fail(nullptr, WF_ERR_OOM, "autotune: no room to save the state");
+        }
+        cudaMemcpyAsync(q, A.psi[h->cur], sizeof(float) * 4 * A.cells, cudaMemcpyDeviceToDevice,
+                        b->stream);
+      }
+      saved.push_back(q);
+    }
+  }
+  const FusedConfig orig = b->cfg;
+  const int cur0 = b->h[0]->cur;
+  float bms = 1e30f;
+  FusedConfig bc = orig;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int tys[] = {4, 8, 16}, stg[] = {3, 4}, zcs[] = {8, 16, 32, 64, 128};
+  for (int ty : tys)
+    for (int sg : stg)
+      for (int zc : zcs) {
+        FusedConfig c{ty, zc, sg};
+        if (!wf::fused_supported(c, wf::kPrecF32)) continue;
+        batch_drop(b);
+        b->cfg = c;
+        if (batch_build(b) != WF_OK) continue;
+        int parity = cur0;
+        bool okc = batch_kernel(b, parity) == WF_OK;  // warm-up
+        parity ^= 1;
+        cudaEventRecord(e0, b->stream);
+        for (int i = 0; i < steps && okc; ++i, parity ^= 1) okc = batch_kernel(b, parity) == WF_OK;
+        cudaEventRecord(e1, b->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess || !okc) continue;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= steps;
+        if (ms < bms) {
+          bms = ms;
+          bc = c;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  batch_drop(b);
+  b->cfg = bc;
+  size_t k = 0;
+  for (wf_handle *h : b->h) {
+    cudaMemcpyAsync(h->fld[h->cur], saved[k++], sizeof(float) * 6 * h->N, cudaMemcpyDeviceToDevice,
+                    b->stream);
+    for (auto &A : h->ax) {
+      void *q = saved[k++];
+      if (q)
+        cudaMemcpyAsync(A.psi[h->cur], q, sizeof(float) * 4 * A.cells, cudaMemcpyDeviceToDevice,
+                        b->stream);
+    }
+    cudaMemsetAsync(h->d_err, 0, sizeof(int), b->stream);
+  }
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  free_saved();
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "autotune restore");
   if (best) {
     best->tile_rows = bc.ty;
     best->z_chunk = bc.zchunk;

@@ -63,6 +63,30 @@ cudaError_t fused_prepare(const FusedConfig &c, int prec) {
   return cudaErrorInvalidValue;
 }
 
+cudaError_t fused_batch_prepare(const FusedConfig &c) {
+#define X(T, S_) if (c.ty == T && c.stages == S_) return batch_prepare_t<T, S_>();
+  WF_FUSED_CONFIGS(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fused_batch(const FusedConfig &c, const BatchScene *scenes, const int2 *items,
+                               int n_items, int *counter, int parity, int ctas, cudaStream_t s) {
+#define X(T, S_)                                                                         \
+  if (c.ty == T && c.stages == S_)                                                      \
+    return batch_launch_t<T, S_>(scenes, items, n_items, counter, parity, ctas, s);
+  WF_FUSED_CONFIGS(X)
+#undef X
+  return cudaErrorInvalidValue;
+}
+
+int fused_batch_ctas_per_sm(const FusedConfig &c) {
+#define X(T, S_) if (c.ty == T && c.stages == S_) return batch_ctas_per_sm_t<T, S_>();
+  WF_FUSED_CONFIGS(X)
+#undef X
+  return 0;
+}
+
 cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                          const int *items, int n_items, int ax, bool fma, cudaStream_t s) {
   if (a.g.prec != kPrecF32) {

@@ -687,6 +687,93 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 3 : 1)
   fused_body<TY, S, FMA, AX, ST>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
 }
 
+// Batched step: a persistent CTA takes (grid, item) pairs from a counter and
+// runs the all-axes CPML body (AX = 7) for each, with that grid's arguments
+// copied to shared memory and its TMA maps read from global memory.  The
+// mbarrier ring is re-initialised per item (every copy of the previous item
+// has completed: the body consumes or drains all it issued).
+template <int TY, int S>
+__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 3 : 1)
+    k_fused_batch(const BatchScene *scenes, const int2 *items, int n_items, int *counter,
+                  int parity) {
+  using L = Layout<TY, S, float>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *smem = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
+  __shared__ int s_item;
+  __shared__ FusedArgs s_args;
+  uint64_t *s_bar = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+  bool first = true;
+  for (;;) {
+    __syncthreads();  // the previous item is done with shared memory
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const int2 si = items[it];
+    const BatchScene *sc = scenes + si.x;
+    {
+      const int *src = reinterpret_cast<const int *>(&sc->args[parity]);
+      int *dst = reinterpret_cast<int *>(&s_args);
+      for (int i = threadIdx.x; i < static_cast<int>(sizeof(FusedArgs) / 4); i += blockDim.x)
+        dst[i] = src[i];
+    }
+    __syncthreads();
+    const FusedArgs &a = s_args;
+    int item = si.y;
+    const int txi = item % a.tiles_x;
+    item /= a.tiles_x;
+    const int tyi = item % a.tiles_y;
+    const int zc = item / a.tiles_y;
+    const int x0 = txi * kTileX, y0 = tyi * TY;
+    const int k0 = zc * a.zchunk;
+    const int k1 = min(k0 + a.zchunk, a.g.nz);
+    float4 *s_coef = reinterpret_cast<float4 *>(smem);
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) s_coef[i] = a.g.coef[i];
+    float *s_prof = reinterpret_cast<float *>(smem + L::PROF_OFF);
+    for (int i = threadIdx.x; i < kProfSmem; i += blockDim.x) {
+      const int cap = kProfSmem / 9;
+      const int ax = i / (3 * cap), k = (i / cap) % 3, s = i % cap;
+      const PmlAxis &P = a.g.pml[ax];
+      s_prof[i] = (P.T > 0 && s < P.W) ? P.prof[k * P.W + s] : 0.0f;
+    }
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < S; ++s) {
+        if (!first) mbar_inval(smem_u32(&s_bar[s]));
+        mbar_init(smem_u32(&s_bar[s]), 1);
+      }
+      mbar_fence_init();
+    }
+    first = false;
+    __syncthreads();
+    fused_body<TY, S, false, 7, float>(&sc->maps[parity][0], &sc->maps[parity][1],
+                                       &sc->maps[parity][2], a, smem, x0, y0, k0, k1);
+  }
+}
+
+template <int TY, int S>
+cudaError_t batch_prepare_t() {
+  return cudaFuncSetAttribute((const void *)k_fused_batch<TY, S>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, Layout<TY, S, float>::BYTES);
+}
+
+template <int TY, int S>
+cudaError_t batch_launch_t(const BatchScene *scenes, const int2 *items, int n_items, int *counter,
+                           int parity, int ctas, cudaStream_t s) {
+  using L = Layout<TY, S, float>;
+  k_fused_batch<TY, S><<<ctas, L::THREADS, L::BYTES, s>>>(scenes, items, n_items, counter, parity);
+  return cudaGetLastError();
+}
+
+template <int TY, int S>
+int batch_ctas_per_sm_t() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_batch<TY, S>, Layout<TY, S, float>::THREADS,
+                                                    Layout<TY, S, float>::BYTES) != cudaSuccess)
+    return 0;
+  return n;
+}
+
 #define WF_AX_CLASSES(X) X(0) X(1) X(2) X(4) X(7)
 
 template <int TY, int S, bool FMA, typename ST>

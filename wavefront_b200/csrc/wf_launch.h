@@ -46,6 +46,14 @@ struct FusedMaps {
   CUtensorMap e, h, m;
 };
 
+// One grid of a batched step, in device memory (64-byte aligned for the
+// tensor maps): per parity of the state read, its TMA maps (E, H, ids) and
+// fused-kernel arguments.
+struct BatchScene {
+  CUtensorMap maps[2][3];
+  FusedArgs args[2];
+};
+
 cudaError_t launch_split(const GridArgs &g, bool fma, cudaStream_t s);
 cudaError_t launch_tail(const TailArgs &t, cudaStream_t s);
 cudaError_t launch_soa_to_blocks(const float *soa, float *blk, int nx, int ny, int nz,
@@ -66,6 +74,17 @@ constexpr int kFusedClasses[5] = {0, 1, 2, 4, 7};
 // Launches the kernel of class `ax` over a device list of n_items items.
 cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                          const int *items, int n_items, int ax, bool fma, cudaStream_t s);
+// Batched step (FP32 storage, exact arithmetic): one persistent launch of
+// `ctas` CTAs that take (grid, item) pairs from *counter (zeroed by the
+// caller before each launch) until n_items are done.
+cudaError_t fused_batch_prepare(const FusedConfig &c);
+cudaError_t launch_fused_batch(const FusedConfig &c, const BatchScene *scenes, const int2 *items,
+                               int n_items, int *counter, int parity, int ctas, cudaStream_t s);
+// CTAs per SM the batched kernel of a tiling fits (for sizing `ctas`).
+int fused_batch_ctas_per_sm(const FusedConfig &c);
+// The step tail of n grids at once: one CTA per grid, t[i] as for launch_tail.
+cudaError_t launch_tail_batch(const TailArgs *t, int n, cudaStream_t s);
+
 // 16-bit storage (wf_fused16.cu)
 bool fused16_supported(const FusedConfig &c);
 int fused16_smem_bytes(const FusedConfig &c, int prec);

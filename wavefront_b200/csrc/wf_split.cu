@@ -225,9 +225,21 @@ constexpr int kMaxSlabs = 1024;  // nz <= 8192 for 16-bit storage
 // 16-bit storage: sources re-encode the cells they change (their magnitudes
 // join the slab maxima), probes decode, and the CTA then picks the shifts
 // the next step writes with.
+__device__ void tail_body(const TailArgs &t, float *s_src);
+
 __global__ void k_tail(TailArgs t) {
-  __shared__ long long s_step;
   __shared__ float s_src[kMaxSlabs];
+  tail_body(t, s_src);
+}
+
+// one CTA per grid of a batch (FP32 storage: no slab scales)
+__global__ void k_tail_batch(const TailArgs *ts) {
+  const TailArgs t = ts[blockIdx.x];
+  tail_body(t, nullptr);
+}
+
+__device__ void tail_body(const TailArgs &t, float *s_src) {
+  __shared__ long long s_step;
   if (threadIdx.x == 0) s_step = *t.step;
   __syncthreads();
   const long long st = s_step;
@@ -372,6 +384,12 @@ cudaError_t launch_split(const GridArgs &g, bool fma, cudaStream_t s) {
 cudaError_t launch_tail(const TailArgs &t, cudaStream_t s) {
   if (t.prec != kPrecF32 && t.nslab > kMaxSlabs) return cudaErrorInvalidValue;
   k_tail<<<1, 256, 0, s>>>(t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tail_batch(const TailArgs *t, int n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_tail_batch<<<n, 256, 0, s>>>(t);
   return cudaGetLastError();
 }
 

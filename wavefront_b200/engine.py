@@ -49,13 +49,27 @@ class DeviceFieldGrid:
         h = C.c_void_p()
         _L.check(_L.lib().wf_create(C.byref(d), C.byref(h)))
         self._h = h
+        self._owned = True
         self.n_sources = 0
         self.n_probes = 0
+
+    @classmethod
+    def _member(cls, handle, dims: GridDims) -> "DeviceFieldGrid":
+        """A view of a grid owned by a DeviceBatch (closing it frees nothing)."""
+        g = cls.__new__(cls)
+        g.dims = dims
+        g.precision = "f32"
+        g._h = C.c_void_p(handle)
+        g._owned = False
+        g.n_sources = 0
+        g.n_probes = 0
+        return g
 
     # -- lifetime ----------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None):
-            _L.lib().wf_destroy(self._h)
+            if getattr(self, "_owned", True):
+                _L.lib().wf_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -282,3 +296,77 @@ def run(grid: DeviceFieldGrid, sources: Sequence, probes: Sequence, config: Engi
         print(f"wavefront_b200: {n} steps in {wall:.3f}s ({n / max(wall, 1e-9):.1f} steps/s, "
               f"{d.voxel_count() * n / max(wall, 1e-9) / 1e6:.1f} Mcell/s)")
     return wall
+
+
+class DeviceBatch:
+    """Many independent grids stepped together by one persistent kernel per
+    step (wf_batch_*).  grid(i) gives the per-grid handle for setup (scene,
+    CPML, sources, probes) and read-back; step() advances every grid."""
+
+    def __init__(self, dims_list: Sequence[GridDims], device: int = 0):
+        n = len(dims_list)
+        descs = (_L.GridDesc * n)()
+        for d, dims in zip(descs, dims_list):
+            d.nx, d.ny, d.nz = dims.nx, dims.ny, dims.nz
+            d.kernel = _KERNEL["fused"]
+            d.device = device
+        b = C.c_void_p()
+        _L.check(_L.lib().wf_batch_create(n, descs, C.byref(b)))
+        self._b = b
+        self.grids = [DeviceFieldGrid._member(_L.lib().wf_batch_handle(b, i), dims)
+                      for i, dims in enumerate(dims_list)]
+
+    def grid(self, i: int) -> DeviceFieldGrid:
+        return self.grids[i]
+
+    def __len__(self):
+        return len(self.grids)
+
+    def close(self):
+        if getattr(self, "_b", None):
+            for g in self.grids:
+                g._h = None
+            _L.lib().wf_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step(self, n: int = 1):
+        _L.check(_L.lib().wf_batch_step(self._b, n))
+
+    def sync(self):
+        _L.check(_L.lib().wf_batch_sync(self._b))
+
+    def stream(self) -> int:
+        v = C.c_void_p()
+        _L.check(_L.lib().wf_batch_get_stream(self._b, C.byref(v)))
+        return int(v.value or 0)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(_L.lib().wf_batch_kernel_launches(self._b))
+
+    def tiling(self):
+        t = _L.Tiling()
+        _L.check(_L.lib().wf_batch_get_tiling(self._b, C.byref(t)))
+        return t.tile_rows, t.z_chunk, t.stages
+
+    def set_tiling(self, tile_rows, z_chunk, stages):
+        t = _L.Tiling(tile_rows, z_chunk, stages)
+        _L.check(_L.lib().wf_batch_set_tiling(self._b, C.byref(t)))
+
+    def autotune(self, steps: int = 3):
+        t = _L.Tiling()
+        ms = C.c_float()
+        _L.check(_L.lib().wf_batch_autotune(self._b, steps, C.byref(t), C.byref(ms)))
+        return (t.tile_rows, t.z_chunk, t.stages), ms.value
