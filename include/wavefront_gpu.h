@@ -220,6 +220,53 @@ wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t);
 /* Times each candidate tiling for `steps` steps and keeps the fastest. */
 wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms);
 
+/* ---- learned boundary closure (no reference counterpart) ---------------- */
+
+/* A per-face 3-layer 3D conv network (3x3x3 kernels, channels 10 -> 16 -> 16
+ * -> 6, GELU after the first two layers, no bias, bfloat16 weights, FP32
+ * accumulation) that corrects the fields in the 8-cell band next to each
+ * face of a grid with a thin CPML.  Its input is the band's six fields and
+ * the four psi terms of the face's normal axis, E-side values times gain_e
+ * and H-side values times gain_h; its output, divided by the same gains, is
+ * added to the band's fields after every step kernel (before sources and
+ * probes).  Band tensors are [6 faces][channels][8][n][n] (cubic grids:
+ * face f has normal axis f/2, at the low side for even f; distance 0 is the
+ * outermost cell; the two tangential axes follow in increasing order).
+ * Weights are device or host arrays of bfloat16 [6][cout][cin][27]. */
+wf_status wf_set_closure(wf_handle *h, const void *w1_bf16, const void *w2_bf16,
+                         const void *w3_bf16, float gain_e, float gain_h);  /* w1 NULL: off */
+/* The current state's bands into device X[6][10][8][n][n] (scaled as above). */
+wf_status wf_band_gather(wf_handle *h, float *X, float gain_e, float gain_h);
+/* fields += Y[6][6][8][n][n] / gain over the current state's bands. */
+wf_status wf_band_scatter_add(wf_handle *h, const float *Y, float gain_e, float gain_h);
+/* Student state = teacher state restricted to the student's extent at
+ * `offset` cells on every axis: fields, and the student's psi from the
+ * teacher's psi at the same cells (zero where the teacher keeps none). */
+wf_status wf_restrict_state(wf_handle *teacher, wf_handle *student, int offset);
+
+/* The closure network's training kernels on device arrays (stream: a
+ * cudaStream_t or NULL).  Tensors are [n][c][d][h][w]; sample i uses the
+ * weights of face[i] (face NULL: all use face 0); weights bfloat16
+ * [faces][cout][cin][27]; accumulation FP32.  forward: pre (may be NULL) =
+ * conv(in), out = GELU(pre) if gelu else pre.  backward_data: din =
+ * conv^T(dpre).  backward_weight: dw[face] += sum over the face's samples.
+ * mse: loss += mean((y-t)^2), dy = 2(y-t)/m.  adam: one Adam step on FP32
+ * master weights w (t counts from 1), refreshing the bfloat16 copy. */
+wf_status wf_nn_conv3d_forward(const float *in, const void *w_bf16, const int32_t *face,
+                               float *pre, float *out, int n, int cin, int cout, int d, int h,
+                               int w, int gelu, void *stream);
+wf_status wf_nn_conv3d_backward_data(const float *dpre, const void *w_bf16, const int32_t *face,
+                                     float *din, int n, int cin, int cout, int d, int h, int w,
+                                     void *stream);
+wf_status wf_nn_conv3d_backward_weight(const float *in, const float *dpre, const int32_t *face,
+                                       float *dw, int n, int cin, int cout, int d, int h, int w,
+                                       int nface, void *stream);
+wf_status wf_nn_gelu_backward(const float *dout, const float *pre, float *dpre, int64_t m,
+                              void *stream);
+wf_status wf_nn_mse(const float *y, const float *t, float *dy, float *loss, int64_t m, void *stream);
+wf_status wf_nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, int64_t n,
+                     float lr, float b1, float b2, float eps, int t, void *stream);
+
 /* ---- batched stepping (no reference counterpart) ------------------------ */
 
 /* Many independent grids of uneven size stepped together: each step is one

@@ -22,6 +22,9 @@ EXPORTS = [
     "wf_batch_create", "wf_batch_destroy", "wf_batch_size", "wf_batch_handle", "wf_batch_step",
     "wf_batch_sync", "wf_batch_get_stream", "wf_batch_kernel_launches", "wf_batch_get_tiling",
     "wf_batch_set_tiling", "wf_batch_autotune",
+    "wf_set_closure", "wf_band_gather", "wf_band_scatter_add", "wf_restrict_state",
+    "wf_nn_conv3d_forward", "wf_nn_conv3d_backward_data", "wf_nn_conv3d_backward_weight",
+    "wf_nn_gelu_backward", "wf_nn_mse", "wf_nn_adam",
     "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
     "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
     "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
@@ -121,6 +124,23 @@ def lib() -> C.CDLL:
         L.wf_batch_set_tiling.restype = S
         L.wf_batch_autotune.argtypes = [_h, C.c_int, C.POINTER(Tiling), _f32p]
         L.wf_batch_autotune.restype = S
+        vp = C.c_void_p
+        L.wf_set_closure.argtypes = [_h, vp, vp, vp, C.c_float, C.c_float]
+        L.wf_band_gather.argtypes = [_h, vp, C.c_float, C.c_float]
+        L.wf_band_scatter_add.argtypes = [_h, vp, C.c_float, C.c_float]
+        L.wf_restrict_state.argtypes = [_h, _h, C.c_int]
+        L.wf_nn_conv3d_forward.argtypes = [vp, vp, vp, vp, vp] + [C.c_int] * 8 + [vp]
+        L.wf_nn_conv3d_backward_data.argtypes = [vp, vp, vp, vp] + [C.c_int] * 7 + [vp]
+        L.wf_nn_conv3d_backward_weight.argtypes = [vp, vp, vp, vp] + [C.c_int] * 8 + [vp]
+        L.wf_nn_gelu_backward.argtypes = [vp, vp, vp, C.c_int64, vp]
+        L.wf_nn_mse.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
+        L.wf_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float,
+                                 C.c_float, C.c_int, vp]
+        for name in ("wf_set_closure", "wf_band_gather", "wf_band_scatter_add", "wf_restrict_state",
+                     "wf_nn_conv3d_forward", "wf_nn_conv3d_backward_data",
+                     "wf_nn_conv3d_backward_weight", "wf_nn_gelu_backward", "wf_nn_mse",
+                     "wf_nn_adam"):
+            getattr(L, name).restype = S
         L.wf_probe_sums.argtypes = [_h, C.c_int, _f64p, _f64p, C.POINTER(C.c_uint64)]
         L.wf_probe_sums.restype = S
         L.wf_probe_trace.argtypes = [_h, C.c_int, _f32p, C.c_int]

@@ -1,0 +1,336 @@
+// wf_closure.cu -- the learned thin-CPML boundary closure (no reference
+// counterpart): a per-face 3-layer 3D convolutional network that corrects
+// the fields in the 8-cell band next to each face of a grid with a thin
+// (4-cell) CPML, so that it behaves like a thick one.
+//
+// Tensors are "band" tensors [N][C][D=8][H][W]: sample n (a face, or a crop
+// of one), channel c, distance d from the outer face (0 = outermost cell),
+// and the two tangential coordinates in increasing axis order.  Every conv
+// is 3x3x3, stride 1, zero padding, no bias; weights are bfloat16
+// [F][Co][Ci][27] (F = 6 faces; sample n uses face[n]) and every sum
+// accumulates in FP32.  GELU is the erf form 0.5 z (1 + erf(z / sqrt 2)).
+//
+// Training runs on these kernels too: forward (keeping pre-activations),
+// backward to the input and to the weights, GELU backward, the MSE loss and
+// its gradient, and Adam on FP32 master weights with a bfloat16 copy for
+// the forward pass.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "wf_closure.h"
+
+namespace wf {
+
+namespace {
+
+constexpr int kMaxC = 16;       // channels per layer at most
+constexpr int kTaps = 27;
+constexpr float kInvSqrt2 = 0.70710678118654752f;
+constexpr float kInvSqrt2Pi = 0.39894228040143268f;
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * kInvSqrt2)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.0f + erff(z * kInvSqrt2)) + z * kInvSqrt2Pi * expf(-0.5f * z * z);
+}
+
+// out[n][co][p] = sum_ci sum_tap w[face[n]][co][ci][tap] * in[n][ci][p + tap]
+// (one thread per output voxel, all output channels in registers; the
+// sample's weights staged in shared memory as FP32)
+__global__ void k_conv_fwd(const float *in, const __nv_bfloat16 *w, const int *face, float *z,
+                           float *a, int n, int ci, int co, int D, int H, int W, int act) {
+  extern __shared__ float s_w[];  // [co][ci][27] of the block's sample
+  const long long P = static_cast<long long>(D) * H * W;
+  const int s = blockIdx.y;       // sample
+  const int f = face ? face[s] : 0;
+  const int nw = co * ci * kTaps;
+  for (int i = threadIdx.x; i < nw; i += blockDim.x)
+    s_w[i] = __bfloat162float(w[static_cast<long long>(f) * nw + i]);
+  __syncthreads();
+  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= P || s >= n) return;
+  const int x = static_cast<int>(p % W), y = static_cast<int>((p / W) % H), d = static_cast<int>(p / (static_cast<long long>(W) * H));
+  float acc[kMaxC];
+#pragma unroll
+  for (int o = 0; o < kMaxC; ++o) acc[o] = 0.0f;
+  const float *src = in + static_cast<long long>(s) * ci * P;
+  for (int c = 0; c < ci; ++c) {
+    const float *sc = src + c * P;
+    for (int t = 0; t < kTaps; ++t) {
+      const int dd = d + t / 9 - 1, yy = y + (t / 3) % 3 - 1, xx = x + t % 3 - 1;
+      if (dd < 0 || dd >= D || yy < 0 || yy >= H || xx < 0 || xx >= W) continue;
+      const float v = sc[(static_cast<long long>(dd) * H + yy) * W + xx];
+#pragma unroll
+      for (int o = 0; o < kMaxC; ++o)
+        if (o < co) acc[o] = __fmaf_rn(s_w[(o * ci + c) * kTaps + t], v, acc[o]);
+    }
+  }
+  for (int o = 0; o < co; ++o) {
+    const long long k = (static_cast<long long>(s) * co + o) * P + p;
+    if (z) z[k] = acc[o];
+    a[k] = act ? gelu(acc[o]) : acc[o];
+  }
+}
+
+// din[n][ci][p] = sum_co sum_tap w[co][ci][tap] * dz[n][co][p - tap]
+__global__ void k_conv_bwd_data(const float *dz, const __nv_bfloat16 *w, const int *face, float *din,
+                                int n, int ci, int co, int D, int H, int W) {
+  extern __shared__ float s_w[];
+  const long long P = static_cast<long long>(D) * H * W;
+  const int s = blockIdx.y;
+  const int f = face ? face[s] : 0;
+  const int nw = co * ci * kTaps;
+  for (int i = threadIdx.x; i < nw; i += blockDim.x)
+    s_w[i] = __bfloat162float(w[static_cast<long long>(f) * nw + i]);
+  __syncthreads();
+  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= P || s >= n) return;
+  const int x = static_cast<int>(p % W), y = static_cast<int>((p / W) % H), d = static_cast<int>(p / (static_cast<long long>(W) * H));
+  float acc[kMaxC];
+#pragma unroll
+  for (int c = 0; c < kMaxC; ++c) acc[c] = 0.0f;
+  const float *src = dz + static_cast<long long>(s) * co * P;
+  for (int o = 0; o < co; ++o) {
+    const float *so = src + o * P;
+    for (int t = 0; t < kTaps; ++t) {
+      const int dd = d - (t / 9 - 1), yy = y - ((t / 3) % 3 - 1), xx = x - (t % 3 - 1);
+      if (dd < 0 || dd >= D || yy < 0 || yy >= H || xx < 0 || xx >= W) continue;
+      const float g = so[(static_cast<long long>(dd) * H + yy) * W + xx];
+#pragma unroll
+      for (int c = 0; c < kMaxC; ++c)
+        if (c < ci) acc[c] = __fmaf_rn(s_w[(o * ci + c) * kTaps + t], g, acc[c]);
+    }
+  }
+  for (int c = 0; c < ci; ++c) din[(static_cast<long long>(s) * ci + c) * P + p] = acc[c];
+}
+
+// dw[face][co][ci][tap] += sum over samples of that face and voxels p of
+// dz[n][co][p] * in[n][ci][p + tap]: one thread per weight entry, the
+// samples split over blockIdx.y (partial sums added atomically)
+__global__ void k_conv_bwd_weight(const float *in, const float *dz, const int *face, float *dw,
+                                  int n, int ci, int co, int D, int H, int W, int nface) {
+  const int nw = co * ci * kTaps;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nw) return;
+  const int o = e / (ci * kTaps), c = (e / kTaps) % ci, t = e % kTaps;
+  const int od = t / 9 - 1, oy = (t / 3) % 3 - 1, ox = t % 3 - 1;
+  const long long P = static_cast<long long>(D) * H * W;
+  float acc[8];
+  for (int f = 0; f < 8; ++f) acc[f] = 0.0f;
+  for (int s = blockIdx.y; s < n; s += gridDim.y) {
+    const int f = face ? face[s] : 0;
+    const float *g = dz + (static_cast<long long>(s) * co + o) * P;
+    const float *v = in + (static_cast<long long>(s) * ci + c) * P;
+    float sum = 0.0f;
+    for (int d = 0; d < D; ++d) {
+      const int dd = d + od;
+      if (dd < 0 || dd >= D) continue;
+      for (int y = 0; y < H; ++y) {
+        const int yy = y + oy;
+        if (yy < 0 || yy >= H) continue;
+        const float *gr = g + (static_cast<long long>(d) * H + y) * W;
+        const float *vr = v + (static_cast<long long>(dd) * H + yy) * W;
+        for (int x = 0; x < W; ++x) {
+          const int xx = x + ox;
+          if (xx < 0 || xx >= W) continue;
+          sum = __fmaf_rn(gr[x], vr[xx], sum);
+        }
+      }
+    }
+    if (f < 8) acc[f] += sum;
+  }
+  for (int f = 0; f < nface && f < 8; ++f)
+    if (acc[f] != 0.0f) atomicAdd(dw + static_cast<long long>(f) * nw + e, acc[f]);
+}
+
+__global__ void k_gelu_bwd(const float *da, const float *z, float *dz, long long m) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < m) dz[i] = da[i] * gelu_grad(z[i]);
+}
+
+// loss += sum (y - t)^2 / m;  dy = 2 (y - t) / m
+__global__ void k_mse(const float *y, const float *t, float *dy, float *loss, long long m) {
+  __shared__ float s_sum[256];
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  float d = 0.0f;
+  if (i < m) {
+    d = y[i] - t[i];
+    dy[i] = 2.0f * d / static_cast<float>(m);
+  }
+  s_sum[threadIdx.x] = d * d;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) s_sum[threadIdx.x] += s_sum[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(loss, s_sum[0] / static_cast<float>(m));
+}
+
+// Adam (Kingma & Ba) on FP32 master weights; the bfloat16 copy is what the
+// forward pass reads.
+__global__ void k_adam(float *w, __nv_bfloat16 *wb, const float *g, float *m1, float *m2, long long n,
+                       float lr, float b1, float b2, float eps, float c1, float c2) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float a = b1 * m1[i] + (1.0f - b1) * gi;
+  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  const float wi = w[i] - lr * (a / c1) / (sqrtf(b / c2) + eps);
+  w[i] = wi;
+  wb[i] = __float2bfloat16_rn(wi);
+}
+
+// ---- band gather / scatter on a grid's state --------------------------------
+
+// Cell (x, y, z) of band coordinates (d, u, v) of face f (axis f/2, side f%2).
+__device__ __forceinline__ void band_cell(const BandGrid &g, int f, int d, int u, int v, int &x,
+                                          int &y, int &z) {
+  const int ax = f >> 1;
+  const int n = ax == 0 ? g.nx : (ax == 1 ? g.ny : g.nz);
+  const int c = (f & 1) ? n - 1 - d : d;
+  if (ax == 0) { x = c; y = u; z = v; }
+  else if (ax == 1) { x = u; y = c; z = v; }
+  else { x = u; y = v; z = c; }
+}
+
+// The psi slot index of cell (x, y, z) on axis `ax`, or -1 outside its slab.
+__device__ __forceinline__ long long psi_index(const BandGrid &g, int ax, int x, int y, int z) {
+  const BandPsi &P = g.psi[ax];
+  if (P.T <= 0) return -1;
+  const int n = ax == 0 ? g.nx : (ax == 1 ? g.ny : g.nz);
+  const int c = ax == 0 ? x : (ax == 1 ? y : z);
+  int s = -1;
+  if (c < P.T) s = c;
+  else if (c >= n - P.T) s = c - (n - P.W);
+  if (s < 0) return -1;
+  if (ax == 0) return (static_cast<long long>(z) * g.ny + y) * P.pitch + s;
+  if (ax == 1) return (static_cast<long long>(z) * P.W + s) * g.nx + x;
+  return (static_cast<long long>(s) * g.ny + y) * g.nx + x;
+}
+
+// X[f][10][8][H][W]: 6 fields scaled by gain (E by ge, H by gh), then the 4
+// psi of the face's normal axis (terms of E differences by ge, of H by gh).
+__global__ void k_band_gather(BandGrid g, float *X, int H, int W, float ge, float gh) {
+  const int f = blockIdx.y;
+  const long long P = static_cast<long long>(kBandDepth) * H * W;
+  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int v = static_cast<int>(p % W), u = static_cast<int>((p / W) % H), d = static_cast<int>(p / (static_cast<long long>(W) * H));
+  int x, y, z;
+  band_cell(g, f, d, u, v, x, y, z);
+  float *out = X + static_cast<long long>(f) * kBandIn * P + p;
+  const long long cell = (static_cast<long long>(z) * g.ny + y) * g.nx + x;
+  for (int c = 0; c < 6; ++c) out[c * P] = g.fields[c * g.N + cell] * (c < 3 ? ge : gh);
+  const long long k = psi_index(g, f >> 1, x, y, z);
+  for (int c = 0; c < 4; ++c)
+    out[(6 + c) * P] = k >= 0 ? g.psi[f >> 1].p[c * g.psi[f >> 1].cells + k] * (c < 2 ? ge : gh) : 0.0f;
+}
+
+// fields += Y / gain over every face's band (faces in order; a cell in two
+// bands gets both corrections, edges first by the lower face index)
+__global__ void k_band_scatter_add(BandGrid g, const float *Y, int H, int W, float ge, float gh,
+                                   int f) {
+  const long long P = static_cast<long long>(kBandDepth) * H * W;
+  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int v = static_cast<int>(p % W), u = static_cast<int>((p / W) % H), d = static_cast<int>(p / (static_cast<long long>(W) * H));
+  int x, y, z;
+  band_cell(g, f, d, u, v, x, y, z);
+  const float *in = Y + static_cast<long long>(f) * 6 * P + p;
+  const long long cell = (static_cast<long long>(z) * g.ny + y) * g.nx + x;
+  for (int c = 0; c < 6; ++c) g.fields[c * g.N + cell] += in[c * P] / (c < 3 ? ge : gh);
+}
+
+// Student state (nx, ny, nz) = teacher state at offset `off` on every axis:
+// the six fields, and on each axis the student's psi slab from the teacher's
+// psi at the same physical cells.
+__global__ void k_restrict(BandGrid t, BandGrid s, int off) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= s.N) return;
+  const int x = static_cast<int>(i % s.nx), y = static_cast<int>((i / s.nx) % s.ny), z = static_cast<int>(i / (static_cast<long long>(s.nx) * s.ny));
+  const int X = x + off, Y = y + off, Z = z + off;
+  const long long ti = (static_cast<long long>(Z) * t.ny + Y) * t.nx + X;
+  for (int c = 0; c < 6; ++c) s.fields[c * s.N + i] = t.fields[c * t.N + ti];
+  for (int ax = 0; ax < 3; ++ax) {
+    const long long ks = psi_index(s, ax, x, y, z);
+    if (ks < 0) continue;
+    const long long kt = psi_index(t, ax, X, Y, Z);
+    for (int c = 0; c < 4; ++c)
+      s.psi[ax].p[c * s.psi[ax].cells + ks] = kt >= 0 ? t.psi[ax].p[c * t.psi[ax].cells + kt] : 0.0f;
+  }
+}
+
+inline unsigned blocks_for(long long n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
+
+}  // namespace
+
+int nn_conv_fwd(const float *in, const void *w_bf16, const int *face, float *z, float *a, int n,
+                int ci, int co, int D, int H, int W, int act, void *stream) {
+  if (ci > kMaxC || co > kMaxC || ci < 1 || co < 1 || n < 1) return cudaErrorInvalidValue;
+  const long long P = static_cast<long long>(D) * H * W;
+  dim3 grid(blocks_for(P, 128), n);
+  k_conv_fwd<<<grid, 128, sizeof(float) * co * ci * kTaps, static_cast<cudaStream_t>(stream)>>>(
+      in, static_cast<const __nv_bfloat16 *>(w_bf16), face, z, a, n, ci, co, D, H, W, act);
+  return cudaGetLastError();
+}
+
+int nn_conv_bwd_data(const float *dz, const void *w_bf16, const int *face, float *din, int n,
+                     int ci, int co, int D, int H, int W, void *stream) {
+  if (ci > kMaxC || co > kMaxC || ci < 1 || co < 1 || n < 1) return cudaErrorInvalidValue;
+  const long long P = static_cast<long long>(D) * H * W;
+  dim3 grid(blocks_for(P, 128), n);
+  k_conv_bwd_data<<<grid, 128, sizeof(float) * co * ci * kTaps, static_cast<cudaStream_t>(stream)>>>(
+      dz, static_cast<const __nv_bfloat16 *>(w_bf16), face, din, n, ci, co, D, H, W);
+  return cudaGetLastError();
+}
+
+int nn_conv_bwd_weight(const float *in, const float *dz, const int *face, float *dw, int n, int ci,
+                       int co, int D, int H, int W, int nface, void *stream) {
+  if (ci > kMaxC || co > kMaxC || nface > 8 || n < 1) return cudaErrorInvalidValue;
+  const int nw = co * ci * kTaps;
+  dim3 grid(blocks_for(nw, 128), n < 64 ? n : 64);
+  k_conv_bwd_weight<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(in, dz, face, dw, n, ci, co,
+                                                                         D, H, W, nface);
+  return cudaGetLastError();
+}
+
+int nn_gelu_bwd(const float *da, const float *z, float *dz, long long m, void *stream) {
+  k_gelu_bwd<<<blocks_for(m, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(da, z, dz, m);
+  return cudaGetLastError();
+}
+
+int nn_mse(const float *y, const float *t, float *dy, float *loss, long long m, void *stream) {
+  k_mse<<<blocks_for(m, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(y, t, dy, loss, m);
+  return cudaGetLastError();
+}
+
+int nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, long long n, float lr,
+            float b1, float b2, float eps, int t, void *stream) {
+  const float c1 = 1.0f - powf(b1, static_cast<float>(t)), c2 = 1.0f - powf(b2, static_cast<float>(t));
+  k_adam<<<blocks_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      w, static_cast<__nv_bfloat16 *>(w_bf16), g, m1, m2, n, lr, b1, b2, eps, c1, c2);
+  return cudaGetLastError();
+}
+
+int band_gather(const BandGrid &g, float *X, int H, int W, float ge, float gh, void *stream) {
+  const long long P = static_cast<long long>(kBandDepth) * H * W;
+  k_band_gather<<<dim3(blocks_for(P, 256), 6), 256, 0, static_cast<cudaStream_t>(stream)>>>(g, X, H, W, ge, gh);
+  return cudaGetLastError();
+}
+
+int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, float gh,
+                     void *stream) {
+  const long long P = static_cast<long long>(kBandDepth) * H * W;
+  for (int f = 0; f < 6; ++f)
+    k_band_scatter_add<<<blocks_for(P, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(g, Y, H, W, ge, gh, f);
+  return cudaGetLastError();
+}
+
+int band_restrict(const BandGrid &teacher, const BandGrid &student, int off, void *stream) {
+  k_restrict<<<blocks_for(student.N, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(teacher, student, off);
+  return cudaGetLastError();
+}
+
+}  // namespace wf

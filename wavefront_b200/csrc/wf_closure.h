@@ -1,0 +1,47 @@
+// wf_closure.h -- kernels of the learned thin-CPML boundary closure (see
+// wf_closure.cu): the small 3D conv network's training and inference
+// kernels, and the moves of a grid's boundary bands in and out of them.
+#pragma once
+
+#include <stdint.h>
+
+namespace wf {
+
+constexpr int kBandDepth = 8;  // cells from each face the closure sees and corrects
+constexpr int kBandIn = 10;    // 6 fields + the 4 psi terms of the face's normal axis
+
+struct BandPsi {
+  int T, W, pitch;   // graded thickness, slab width, row pitch (x axis)
+  float *p;          // [4][cells]
+  long long cells;
+};
+
+// Raw view of one state buffer of a grid (fields component-major, x fastest).
+struct BandGrid {
+  int nx, ny, nz;
+  long long N;
+  float *fields;     // 6*N
+  BandPsi psi[3];
+};
+
+// All return a cudaError_t value; every launch goes to `stream`.
+int nn_conv_fwd(const float *in, const void *w_bf16, const int *face, float *z, float *a, int n,
+                int ci, int co, int D, int H, int W, int act, void *stream);
+int nn_conv_bwd_data(const float *dz, const void *w_bf16, const int *face, float *din, int n,
+                     int ci, int co, int D, int H, int W, void *stream);
+int nn_conv_bwd_weight(const float *in, const float *dz, const int *face, float *dw, int n, int ci,
+                       int co, int D, int H, int W, int nface, void *stream);
+int nn_gelu_bwd(const float *da, const float *z, float *dz, long long m, void *stream);
+int nn_mse(const float *y, const float *t, float *dy, float *loss, long long m, void *stream);
+int nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, long long n, float lr,
+            float b1, float b2, float eps, int t, void *stream);
+// X[6][kBandIn][kBandDepth][H][W] from a cubic grid's bands (fields and psi
+// scaled by the E / H gains).
+int band_gather(const BandGrid &g, float *X, int H, int W, float ge, float gh, void *stream);
+// fields += Y[6][6][kBandDepth][H][W] / gain, face by face.
+int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, float gh,
+                     void *stream);
+// student = teacher restricted at offset `off` (fields and each axis's psi).
+int band_restrict(const BandGrid &teacher, const BandGrid &student, int off, void *stream);
+
+}  // namespace wf

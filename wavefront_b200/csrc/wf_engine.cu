@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/wavefront_gpu.h"
+#include "wf_closure.h"
 #include "wf_launch.h"
 #include "wf_scene.h"
 
@@ -81,6 +82,12 @@ struct wf_handle {
   long long *d_step = nullptr;
   int *d_err = nullptr;
   long long steps_done = 0;
+  // learned boundary closure (applied after every step kernel when on)
+  bool closure = false;
+  void *cl_w[3] = {nullptr, nullptr, nullptr};  // bf16 weights, 6 faces per layer
+  float *cl_buf = nullptr;                      // X, A1, A2, Y band tensors
+  float cl_ge = 1.0f, cl_gh = 1.0f;
+  int *cl_face = nullptr;                       // device {0, 1, ..., 5}
   long long version = 0;               // bumped when device tables are reallocated
   long long kernel_launches = 0;       // step + tail kernels issued so far
   long long graph_kernels[2] = {0, 0};  // kernels in one replay of graph[parity]
@@ -267,6 +274,40 @@ GridArgs grid_args(const wf_handle *h) {
   return g;
 }
 
+// Raw view of state buffer b for the closure kernels.
+wf::BandGrid band_grid(const wf_handle *h, int b) {
+  wf::BandGrid g{};
+  g.nx = h->nx;
+  g.ny = h->ny;
+  g.nz = h->nz;
+  g.N = h->N;
+  g.fields = h->fld[b];
+  for (int a = 0; a < 3; ++a) {
+    const AxisState &A = h->ax[a];
+    g.psi[a] = wf::BandPsi{A.T, A.W, A.pitch, A.psi[b], A.cells};
+  }
+  return g;
+}
+
+constexpr int kClHidden = 16;  // closure hidden channels
+
+// The closure on the state just written (buffer cur ^ 1): bands of the six
+// faces -> conv 10->16 GELU -> conv 16->16 GELU -> conv 16->6 -> fields +=.
+cudaError_t closure_enqueue(wf_handle *h) {
+  const int n = h->nx, D = wf::kBandDepth;
+  const long long P = static_cast<long long>(D) * n * n;
+  float *X = h->cl_buf, *A1 = X + 6 * wf::kBandIn * P, *A2 = A1 + 6 * kClHidden * P,
+        *Y = A2 + 6 * kClHidden * P;
+  const wf::BandGrid g = band_grid(h, h->cur ^ 1);
+  int e = wf::band_gather(g, X, n, n, h->cl_ge, h->cl_gh, h->stream);
+  // sample s of the band tensors is face s and uses face s's weights
+  if (!e) e = wf::nn_conv_fwd(X, h->cl_w[0], h->cl_face, nullptr, A1, 6, wf::kBandIn, kClHidden, D, n, n, 1, h->stream);
+  if (!e) e = wf::nn_conv_fwd(A1, h->cl_w[1], h->cl_face, nullptr, A2, 6, kClHidden, kClHidden, D, n, n, 1, h->stream);
+  if (!e) e = wf::nn_conv_fwd(A2, h->cl_w[2], h->cl_face, nullptr, Y, 6, kClHidden, 6, D, n, n, 0, h->stream);
+  if (!e) e = wf::band_scatter_add(g, Y, n, n, h->cl_ge, h->cl_gh, h->stream);
+  return static_cast<cudaError_t>(e);
+}
+
 // Tail arguments of a step that reads buffer h->cur (16-bit fields included).
 TailArgs tail_args(const wf_handle *h) {
   TailArgs t{};
@@ -348,6 +389,11 @@ wf_status enqueue_one(wf_handle *h) {
     if (e == cudaSuccess) h->kernel_launches += 2;  // H pass, E pass
   }
   if (e != cudaSuccess) return cuda_fail(h, e, "step kernel launch");
+  if (h->closure) {
+    e = closure_enqueue(h);
+    if (e != cudaSuccess) return cuda_fail(h, e, "closure launch");
+    h->kernel_launches += 10;  // gather, 3 convs, 6 face scatters
+  }
   if (h->timing) {
     cudaEvent_t ev = timing_event(h);
     if (!ev) return fail(h, WF_ERR_CUDA, "cudaEventCreate");
@@ -677,6 +723,9 @@ wf_status wf_destroy(wf_handle *h) {
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   for (auto &f : h->fld) cudaFree(f);
   for (auto &s : h->shift) cudaFree(s);
+  for (auto &w : h->cl_w) cudaFree(w);
+  cudaFree(h->cl_buf);
+  cudaFree(h->cl_face);
   cudaFree(h->slab_max);
   cudaFree(h->d_ovf);
   cudaFree(h->mat);
@@ -1265,6 +1314,117 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) 
   return WF_OK;
 }
 
+
+/* ---- learned boundary closure -------------------------------------------- */
+
+wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const void *w3,
+                         float gain_e, float gain_h) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  drop_graphs(h);
+  if (!w1) {
+    h->closure = false;
+    return WF_OK;
+  }
+  if (!w2 || !w3) return fail(h, WF_ERR_ARG, "closure needs three weight arrays");
+  if (store16(h)) return fail(h, WF_ERR_UNSUPPORTED, "the closure works on FP32 fields");
+  if (h->nx != h->ny || h->ny != h->nz || h->nx < wf::kBandDepth)
+    return fail(h, WF_ERR_UNSUPPORTED, "the closure needs a cubic grid");
+  const size_t nw[3] = {6u * kClHidden * wf::kBandIn * 27, 6u * kClHidden * kClHidden * 27,
+                        6u * 6 * kClHidden * 27};
+  const void *src[3] = {w1, w2, w3};
+  for (int l = 0; l < 3; ++l) {
+    if (!h->cl_w[l]) WF_CUDA(h, cudaMalloc(&h->cl_w[l], 2 * nw[l]));
+    WF_CUDA(h, cudaMemcpy(h->cl_w[l], src[l], 2 * nw[l], cudaMemcpyDefault));
+  }
+  if (!h->cl_buf) {
+    const long long P = static_cast<long long>(wf::kBandDepth) * h->nx * h->nx;
+    WF_CUDA(h, cudaMalloc(&h->cl_buf, sizeof(float) * 6 * P * (wf::kBandIn + 2 * kClHidden + 6)));
+    const int faces[6] = {0, 1, 2, 3, 4, 5};
+    WF_CUDA(h, cudaMalloc(&h->cl_face, sizeof(faces)));
+    WF_CUDA(h, cudaMemcpy(h->cl_face, faces, sizeof(faces), cudaMemcpyHostToDevice));
+  }
+  h->cl_ge = gain_e;
+  h->cl_gh = gain_h;
+  h->closure = true;
+  return WF_OK;
+}
+
+wf_status wf_band_gather(wf_handle *h, float *X, float gain_e, float gain_h) {
+  if (!h || !X) return fail(h, WF_ERR_ARG, "null argument");
+  if (store16(h) || h->nx != h->ny || h->ny != h->nz)
+    return fail(h, WF_ERR_UNSUPPORTED, "band moves need a cubic FP32 grid");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, static_cast<cudaError_t>(
+                 wf::band_gather(band_grid(h, h->cur), X, h->nx, h->nx, gain_e, gain_h, h->stream)));
+  return WF_OK;
+}
+
+wf_status wf_band_scatter_add(wf_handle *h, const float *Y, float gain_e, float gain_h) {
+  if (!h || !Y) return fail(h, WF_ERR_ARG, "null argument");
+  if (store16(h) || h->nx != h->ny || h->ny != h->nz)
+    return fail(h, WF_ERR_UNSUPPORTED, "band moves need a cubic FP32 grid");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, static_cast<cudaError_t>(wf::band_scatter_add(band_grid(h, h->cur), Y, h->nx, h->nx,
+                                                           gain_e, gain_h, h->stream)));
+  return WF_OK;
+}
+
+wf_status wf_restrict_state(wf_handle *teacher, wf_handle *student, int offset) {
+  if (!teacher || !student) return fail(student, WF_ERR_ARG, "null handle");
+  if (store16(teacher) || store16(student) || offset < 0 || student->nx + offset > teacher->nx ||
+      student->ny + offset > teacher->ny || student->nz + offset > teacher->nz)
+    return fail(student, WF_ERR_ARG, "the student must fit inside the teacher (FP32 grids)");
+  DeviceGuard guard(student->dev);
+  WF_CUDA(student, cudaStreamSynchronize(teacher->stream));
+  WF_CUDA(student, static_cast<cudaError_t>(wf::band_restrict(
+                       band_grid(teacher, teacher->cur), band_grid(student, student->cur), offset,
+                       student->stream)));
+  WF_CUDA(student, cudaStreamSynchronize(student->stream));
+  return WF_OK;
+}
+
+wf_status wf_nn_conv3d_forward(const float *in, const void *w_bf16, const int32_t *face,
+                               float *pre, float *out, int n, int cin, int cout, int d, int hh,
+                               int ww, int gelu, void *stream) {
+  WF_CUDA(nullptr, static_cast<cudaError_t>(
+                       wf::nn_conv_fwd(in, w_bf16, face, pre, out, n, cin, cout, d, hh, ww, gelu, stream)));
+  return WF_OK;
+}
+
+wf_status wf_nn_conv3d_backward_data(const float *dpre, const void *w_bf16, const int32_t *face,
+                                     float *din, int n, int cin, int cout, int d, int hh, int ww,
+                                     void *stream) {
+  WF_CUDA(nullptr, static_cast<cudaError_t>(
+                       wf::nn_conv_bwd_data(dpre, w_bf16, face, din, n, cin, cout, d, hh, ww, stream)));
+  return WF_OK;
+}
+
+wf_status wf_nn_conv3d_backward_weight(const float *in, const float *dpre, const int32_t *face,
+                                       float *dw, int n, int cin, int cout, int d, int hh, int ww,
+                                       int nface, void *stream) {
+  WF_CUDA(nullptr, static_cast<cudaError_t>(wf::nn_conv_bwd_weight(in, dpre, face, dw, n, cin, cout,
+                                                                   d, hh, ww, nface, stream)));
+  return WF_OK;
+}
+
+wf_status wf_nn_gelu_backward(const float *dout, const float *pre, float *dpre, int64_t m,
+                              void *stream) {
+  WF_CUDA(nullptr, static_cast<cudaError_t>(wf::nn_gelu_bwd(dout, pre, dpre, m, stream)));
+  return WF_OK;
+}
+
+wf_status wf_nn_mse(const float *y, const float *t, float *dy, float *loss, int64_t m, void *stream) {
+  WF_CUDA(nullptr, static_cast<cudaError_t>(wf::nn_mse(y, t, dy, loss, m, stream)));
+  return WF_OK;
+}
+
+wf_status wf_nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, int64_t n,
+                     float lr, float b1, float b2, float eps, int t, void *stream) {
+  WF_CUDA(nullptr, static_cast<cudaError_t>(wf::nn_adam(w, w_bf16, g, m1, m2, n, lr, b1, b2, eps, t, stream)));
+  return WF_OK;
+}
 
 /* ---- batched stepping -------------------------------------------------- */
 
