@@ -66,3 +66,28 @@ def test_null_handle_calls_fail_cleanly():
     assert lib.wf_sync(None) == L.WF_ERR_ARG
     assert lib.wf_destroy(None) == L.WF_OK
     assert lib.wf_status_string(L.WF_ERR_TIMEOUT) == b"device wait timed out"
+
+
+def _header_arity():
+    """Number of parameters of every function the header declares."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(wf_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every binding the Python layer declares has the header's arity (a
+    mismatch would pass garbage through the ABI)."""
+    lib = L.lib()
+    arity = _header_arity()
+    checked = 0
+    for name in L.EXPORTS:
+        fn = getattr(lib, name)
+        if fn.argtypes is None:
+            continue
+        assert len(fn.argtypes) == arity[name], (name, len(fn.argtypes), arity[name])
+        checked += 1
+    assert checked >= 40

@@ -129,9 +129,9 @@ def lib() -> C.CDLL:
         L.wf_band_gather.argtypes = [_h, vp, C.c_float, C.c_float]
         L.wf_band_scatter_add.argtypes = [_h, vp, C.c_float, C.c_float]
         L.wf_restrict_state.argtypes = [_h, _h, C.c_int]
-        L.wf_nn_conv3d_forward.argtypes = [vp, vp, vp, vp, vp] + [C.c_int] * 8 + [vp]
-        L.wf_nn_conv3d_backward_data.argtypes = [vp, vp, vp, vp] + [C.c_int] * 7 + [vp]
-        L.wf_nn_conv3d_backward_weight.argtypes = [vp, vp, vp, vp] + [C.c_int] * 8 + [vp]
+        L.wf_nn_conv3d_forward.argtypes = [vp, vp, vp, vp, vp] + [C.c_int] * 7 + [vp]
+        L.wf_nn_conv3d_backward_data.argtypes = [vp, vp, vp, vp] + [C.c_int] * 6 + [vp]
+        L.wf_nn_conv3d_backward_weight.argtypes = [vp, vp, vp, vp] + [C.c_int] * 7 + [vp]
         L.wf_nn_gelu_backward.argtypes = [vp, vp, vp, C.c_int64, vp]
         L.wf_nn_mse.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
         L.wf_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float,
