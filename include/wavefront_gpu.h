@@ -227,8 +227,9 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms);
  * accumulation) that corrects the fields in the 8-cell band next to each
  * face of a grid with a thin CPML.  Its input is the band's six fields and
  * the four psi terms of the face's normal axis, E-side values times gain_e
- * and H-side values times gain_h; its output, divided by the same gains, is
- * added to the band's fields after every step kernel (before sources and
+ * and H-side values times gain_h, each face's band then divided by the RMS
+ * of its E channels; its output, times that RMS and divided by the gains,
+ * is added to the band's fields after every step kernel (before sources and
  * probes).  Band tensors are [6 faces][channels][8][n][n] (cubic grids:
  * face f has normal axis f/2, at the low side for even f; distance 0 is the
  * outermost cell; the two tangential axes follow in increasing order).

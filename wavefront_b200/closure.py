@@ -141,9 +141,12 @@ class ClosureNet:
         self.adam_step(lr)
         return loss
 
-    def attach(self, grid: DeviceFieldGrid):
-        """The network as grid's closure (applied after every step kernel)."""
-        _chk(_L.lib().wf_set_closure(grid._h, _p(self.wb[0]), _p(self.wb[1]), _p(self.wb[2]),
+    def attach(self, grid: DeviceFieldGrid, alpha: float = 1.0):
+        """The network as grid's closure (applied after every step kernel),
+        its correction scaled by alpha (folded into the last layer)."""
+        torch = _torch()
+        w3 = self.wb[2] if alpha == 1.0 else (self.w[2] * alpha).to(torch.bfloat16)
+        _chk(_L.lib().wf_set_closure(grid._h, _p(self.wb[0]), _p(self.wb[1]), _p(w3),
                                      self.gain_e, self.gain_h))
 
     @staticmethod
@@ -177,9 +180,12 @@ class Run:
 def random_run(rng: np.random.Generator, dx: float) -> Run:
     """One teacher run: 1-3 dielectric inclusions (eps_r U[1,6]) and a Ricker
     or Gaussian source (15-30 cells per wavelength) inside the student's
-    interior."""
+    interior; the source stays out of the 8-cell bands (the student has no
+    source, so a source inside a band would put its injection into the
+    residual the network learns)."""
     lines = []
     lo, hi = OFFSET + THIN + 2, TEACHER_N - OFFSET - THIN - 2
+    slo, shi = OFFSET + BAND + 1, TEACHER_N - OFFSET - BAND - 1
     for _ in range(int(rng.integers(1, 4))):
         eps = rng.uniform(1.0, 6.0)
         c = rng.uniform(lo, hi, 3)
@@ -191,9 +197,32 @@ def random_run(rng: np.random.Generator, dx: float) -> Run:
             lines.append(f"box {eps:.5f} 1.0 0.0 {c[0]:.3f} {c[1]:.3f} {c[2]:.3f} "
                          f"{c[0] + e[0]:.3f} {c[1] + e[1]:.3f} {c[2] + e[2]:.3f}")
     f = float(np.float32(C0 / (rng.uniform(15.0, 30.0) * dx)))
-    src = tuple(int(v) for v in rng.integers(lo, hi, 3))
+    src = tuple(int(v) for v in rng.integers(slo, shi, 3))
     return Run("\n".join(lines) + "\n", int(rng.integers(0, 3)), str(rng.choice(["ricker", "gaussian"])),
                f, src)
+
+
+def truncated_profiles(n: int, dt: float, dx: float):
+    """The thin layer's CPML: on each axis of an n-cell grid, the THIN cells
+    next to each face carry the innermost THIN cells of the THICK-cell
+    grading of the grid (n + 2 (THICK - THIN)) that the thin grid is the
+    interior of; identity (b=1, a=0, 1/kappa=1) elsewhere.  The closure then
+    stands in for the missing outer THICK - THIN cells."""
+    cut = THICK - THIN
+    nt = n + 2 * cut
+    ctx = PmlContext.build_exact(GridDims(nt, nt, nt), PmlConfig(thickness=THICK), dt, dx)
+    out = []
+    for ax in range(3):
+        p = ctx.profiles[ax]
+        out.append(tuple(np.ascontiguousarray(v[cut:cut + n], np.float32)
+                         for v in (p.b, p.a, p.inv_kappa)))
+    return out
+
+
+def set_thin_cpml(grid: DeviceFieldGrid, dt: float, dx: float):
+    n = grid.dims.nx
+    for ax, (b, a, ik) in enumerate(truncated_profiles(n, dt, dx)):
+        grid.set_pml_axis(ax, THIN, b, a, ik)
 
 
 def _grids(run: Run, dx: float, dt: float, steps: int, device: int):
@@ -206,7 +235,7 @@ def _grids(run: Run, dx: float, dt: float, steps: int, device: int):
     sgrid = MaterialGrid(sdims, ids[sl, sl, sl].copy())
     teacher = DeviceFieldGrid(tdims, kernel="fused", device=device)
     teacher.set_materials(tgrid, table)
-    teacher.set_pml(PmlContext.build(tdims, PmlConfig(thickness=THICK), dt, dx))
+    teacher.set_pml(PmlContext.build_exact(tdims, PmlConfig(thickness=THICK), dt, dx))
     wf = default_waveform(run.kind, run.freq)
     from .source import Source
     s = Source(run.src[0], run.src[1], run.src[2], FieldComponent(run.comp), 1.0, wf)
@@ -215,17 +244,24 @@ def _grids(run: Run, dx: float, dt: float, steps: int, device: int):
     for _ in range(2):
         st = DeviceFieldGrid(sdims, kernel="fused", device=device)
         st.set_materials(sgrid, table)
-        st.set_pml(PmlContext.build_exact(sdims, PmlConfig(thickness=THIN), dt, dx))
+        set_thin_cpml(st, dt, dx)
         students.append(st)
     return teacher, students
 
 
 def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, crop: int = 16,
-             seed: int = 1, device: int = 0):
+             seed: int = 1, device: int = 0, net: Optional["ClosureNet"] = None, max_lead: int = 12):
     """Teacher-forced one-step samples: returns (X [M][10][8][c][c],
-    R [M][6][8][c][c], face [M] int32) on the device, with E-side values in
-    units of the first 8 runs' band RMS of E (H side times ETA0 as well),
-    and that RMS.  One random c x c crop per face and sampled step."""
+    R [M][6][8][c][c], face [M] int32, 1.0) on the device.  H-side values
+    are times ETA0, and every sample is divided by the RMS of the E channels
+    of its whole face band -- the normalization the closure applies at run
+    time.  One random c x c crop per face and sampled step.
+
+    With `net`, each sample is taken after the student has run a random
+    1..max_lead steps with `net` as its closure from the teacher's state
+    (the last of them without the closure, whose input is the sample): the
+    target is the teacher's state at the same time, so the network also
+    learns to pull a drifting student back (a DAgger-style round)."""
     torch = _torch()
     dev = torch.device("cuda", device)
     rng = np.random.default_rng(seed)
@@ -241,9 +277,18 @@ def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, cr
         try:
             done = 0
             for k in range(first, steps, every):
-                teacher.step(k - done)
-                done = k
+                lead = int(rng.integers(1, max_lead + 1)) if net is not None else 1
+                lead = min(lead, k - done + 1)  # the teacher cannot step back
+                teacher.step(k - lead + 1 - done)
+                done = k - lead + 1
                 _chk(_L.lib().wf_restrict_state(teacher._h, s1._h, OFFSET))
+                if lead > 1:
+                    net.attach(s1)
+                    for _ in range(lead - 1):
+                        s1.step(1)
+                        teacher.step(1)
+                        done += 1
+                    ClosureNet.detach(s1)
                 s1.step(1)
                 teacher.step(1)
                 done += 1
@@ -253,10 +298,11 @@ def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, cr
                 s1.sync()
                 s2.sync()
                 for f in range(6):
+                    sf = float(torch.sqrt(torch.mean(band[f, :3] ** 2)).item()) + 1e-30
                     u0, v0 = (int(v) for v in rng.integers(0, n - crop + 1, 2))
-                    xs.append(band[f, :, :, u0:u0 + crop, v0:v0 + crop].clone())
+                    xs.append(band[f, :, :, u0:u0 + crop, v0:v0 + crop] / sf)
                     rs.append((band2[f, :6, :, u0:u0 + crop, v0:v0 + crop]
-                               - band[f, :6, :, u0:u0 + crop, v0:v0 + crop]).clone())
+                               - band[f, :6, :, u0:u0 + crop, v0:v0 + crop]) / sf)
                     fs.append(f)
         finally:
             teacher.close()
@@ -265,22 +311,33 @@ def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, cr
     X = torch.stack(xs)
     R = torch.stack(rs)
     F = torch.tensor(fs, dtype=torch.int32, device=dev)
-    rms = float(torch.sqrt(torch.mean(X[:, :3] ** 2)).item()) or 1.0
-    return X / rms, R / rms, F, rms
+    return X, R, F, 1.0
 
 
-def train(X, R, F, rms: float, iters: int = 2000, batch: int = 64, lr: float = 1e-3, seed: int = 0,
-          device: int = 0, log_every: int = 0):
-    """Adam on the MSE of the predicted correction; returns (net, losses)."""
+def train(X, R, F, rms: float, iters: int = 3000, batch: int = 64, lr: float = 3e-4,
+          seed: int = 0, device: int = 0, log_every: int = 0, net: Optional[ClosureNet] = None):
+    """Adam on the MSE of the predicted correction, targets normalized to
+    unit RMS during training (the scale is folded into the last layer
+    afterwards), learning rate on a cosine from lr to lr/30; returns (net,
+    [(iteration, loss on normalized targets)])."""
     torch = _torch()
-    net = ClosureNet(device=device, seed=seed, gain_e=1.0 / rms, gain_h=ETA0 / rms)
+    r_scale = float(torch.sqrt(torch.mean(R * R)).item()) or 1.0
+    if net is None:
+        net = ClosureNet(device=device, seed=seed, gain_e=1.0 / rms, gain_h=ETA0 / rms)
+    else:  # continue: back to the normalized-target units of training
+        net.w[2].div_(r_scale)
+        net.wb[2].copy_(net.w[2].to(torch.bfloat16))
+    Rn = R / r_scale
     g = torch.Generator(device=X.device).manual_seed(seed)
     losses = []
     for it in range(iters):
+        lr_it = lr / 30.0 + 0.5 * (lr - lr / 30.0) * (1.0 + math.cos(math.pi * it / max(iters - 1, 1)))
         idx = torch.randint(0, X.shape[0], (batch,), generator=g, device=X.device)
-        loss = net.train_step(X[idx].contiguous(), R[idx].contiguous(), F[idx].contiguous(), lr)
+        loss = net.train_step(X[idx].contiguous(), Rn[idx].contiguous(), F[idx].contiguous(), lr_it)
         if log_every and (it % log_every == 0 or it == iters - 1):
             losses.append((it, float(loss.item())))
+    net.w[2].mul_(r_scale)
+    net.wb[2].copy_(net.w[2].to(torch.bfloat16))
     return net, losses
 
 
@@ -302,7 +359,8 @@ def residual_loss(net: Optional[ClosureNet], X, R, F, batch: int = 256) -> float
 
 
 def reflection_test(interior: int = 48, steps: int = 260, net: Optional[ClosureNet] = None,
-                    cpml: int = THIN, device: int = 0, seed: int = 3) -> dict:
+                    cpml: int = THIN, device: int = 0, seed: int = 3, alpha: float = 1.0,
+                    truncated: bool = False) -> dict:
     """Reflection of the boundary of an interior^3 region with a `cpml`-cell
     CPML (plus `net` as its closure), against a reference run in a domain
     large enough that nothing returns within `steps`: a Ricker Ez source
@@ -321,12 +379,14 @@ def reflection_test(interior: int = 48, steps: int = 260, net: Optional[ClosureN
     margin = int(math.ceil(steps * 0.58)) + 8
     from .source import Source
 
-    def run(n_total: int, off: int, pml: Optional[PmlContext], closure: bool):
+    def run(n_total: int, off: int, pml, closure: bool):
         dims = GridDims(n_total, n_total, n_total)
         g = DeviceFieldGrid(dims, kernel="fused", device=device)
         try:
             g.set_materials(MaterialGrid(dims), MaterialTable.vacuum_filled(dt, dx))
-            if pml is not None:
+            if pml == "truncated":
+                set_thin_cpml(g, dt, dx)
+            elif pml is not None:
                 g.set_pml(pml)
             s = Source(src_i[0] + off, src_i[1] + off, src_i[2] + off, FieldComponent.Ez, 1.0, wf)
             g.add_source_values(s.x, s.y, s.z, s.component, s.values(dt, steps))
@@ -334,7 +394,7 @@ def reflection_test(interior: int = 48, steps: int = 260, net: Optional[ClosureN
                 g.add_probe_tables(p[0] + off, p[1] + off, p[2] + off, PC.Ez,
                                    np.zeros((steps, 0)), np.zeros((steps, 0)), 0, record_trace=True)
             if closure:
-                net.attach(g)
+                net.attach(g, alpha)
             g.step(steps)
             g.sync()
             return np.stack([g.probe_trace(i, steps) for i in range(len(probes_i))]).astype(np.float64)
@@ -347,11 +407,12 @@ def reflection_test(interior: int = 48, steps: int = 260, net: Optional[ClosureN
     n_b = interior + 2 * cpml
     n_b += (-n_b) % 8
     dims_b = GridDims(n_b, n_b, n_b)
-    pml = PmlContext.build_exact(dims_b, PmlConfig(thickness=cpml), dt, dx)
+    pml = "truncated" if truncated else PmlContext.build_exact(dims_b, PmlConfig(thickness=cpml), dt, dx)
     got = run(n_b, cpml, pml, net is not None)
     peak = np.max(np.abs(ref), axis=1)
     err = np.max(np.abs(got - ref), axis=1) / peak
     l2 = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
     return {"max_rel_error": float(err.max()), "per_probe": err.tolist(),
             "trace_rel_l2": float(l2.max()), "cpml": cpml, "closure": net is not None,
+            "profile": "innermost cells of the 16-cell grading" if truncated else "graded over the layer",
             "interior": interior, "steps": steps}

@@ -262,6 +262,32 @@ __global__ void k_restrict(BandGrid t, BandGrid s, int off) {
   }
 }
 
+// s[f] = RMS of the E channels (0..2) of face f's band tensor (a tiny floor
+// keeps an all-zero band at zero after scaling).
+__global__ void k_face_rms(const float *X, int C, long long P, float *s) {
+  __shared__ float s_sum[256];
+  const int f = blockIdx.x;
+  const float *x = X + static_cast<long long>(f) * C * P;
+  float acc = 0.0f;
+  for (long long i = threadIdx.x; i < 3 * P; i += blockDim.x) acc += x[i] * x[i];
+  s_sum[threadIdx.x] = acc;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) s_sum[threadIdx.x] += s_sum[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) s[f] = sqrtf(s_sum[0] / static_cast<float>(3 * P)) + 1e-30f;
+}
+
+// X[f][c][p] *= s[f] (or / s[f])
+__global__ void k_face_scale(float *X, int C, long long P, const float *s, int divide) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (i >= C * P) return;
+  const float m = divide ? 1.0f / s[f] : s[f];
+  X[static_cast<long long>(f) * C * P + i] *= m;
+}
+
 inline unsigned blocks_for(long long n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
 
 }  // namespace
@@ -325,6 +351,16 @@ int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, 
   const long long P = static_cast<long long>(kBandDepth) * H * W;
   for (int f = 0; f < 6; ++f)
     k_band_scatter_add<<<blocks_for(P, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(g, Y, H, W, ge, gh, f);
+  return cudaGetLastError();
+}
+
+int face_rms(const float *X, int C, long long P, float *s, void *stream) {
+  k_face_rms<<<6, 256, 0, static_cast<cudaStream_t>(stream)>>>(X, C, P, s);
+  return cudaGetLastError();
+}
+
+int face_scale(float *X, int C, long long P, const float *s, int divide, void *stream) {
+  k_face_scale<<<dim3(blocks_for(C * P, 256), 6), 256, 0, static_cast<cudaStream_t>(stream)>>>(X, C, P, s, divide);
   return cudaGetLastError();
 }
 

@@ -41,6 +41,9 @@ int band_gather(const BandGrid &g, float *X, int H, int W, float ge, float gh, v
 // fields += Y[6][6][kBandDepth][H][W] / gain, face by face.
 int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, float gh,
                      void *stream);
+// s[f] = RMS of face f's E channels in X[6][C][P]; X[f] *= s[f] (or /=).
+int face_rms(const float *X, int C, long long P, float *s, void *stream);
+int face_scale(float *X, int C, long long P, const float *s, int divide, void *stream);
 // student = teacher restricted at offset `off` (fields and each axis's psi).
 int band_restrict(const BandGrid &teacher, const BandGrid &student, int off, void *stream);
 

@@ -292,18 +292,24 @@ wf::BandGrid band_grid(const wf_handle *h, int b) {
 constexpr int kClHidden = 16;  // closure hidden channels
 
 // The closure on the state just written (buffer cur ^ 1): bands of the six
-// faces -> conv 10->16 GELU -> conv 16->16 GELU -> conv 16->6 -> fields +=.
+// faces (times the gains), each face divided by its band's E RMS -> conv
+// 10->16 GELU -> conv 16->16 GELU -> conv 16->6 -> times that RMS -> fields
+// += (over the gains).
 cudaError_t closure_enqueue(wf_handle *h) {
   const int n = h->nx, D = wf::kBandDepth;
   const long long P = static_cast<long long>(D) * n * n;
   float *X = h->cl_buf, *A1 = X + 6 * wf::kBandIn * P, *A2 = A1 + 6 * kClHidden * P,
         *Y = A2 + 6 * kClHidden * P;
   const wf::BandGrid g = band_grid(h, h->cur ^ 1);
+  float *scale = Y + 6 * 6 * P;
   int e = wf::band_gather(g, X, n, n, h->cl_ge, h->cl_gh, h->stream);
+  if (!e) e = wf::face_rms(X, wf::kBandIn, P, scale, h->stream);
+  if (!e) e = wf::face_scale(X, wf::kBandIn, P, scale, 1, h->stream);
   // sample s of the band tensors is face s and uses face s's weights
   if (!e) e = wf::nn_conv_fwd(X, h->cl_w[0], h->cl_face, nullptr, A1, 6, wf::kBandIn, kClHidden, D, n, n, 1, h->stream);
   if (!e) e = wf::nn_conv_fwd(A1, h->cl_w[1], h->cl_face, nullptr, A2, 6, kClHidden, kClHidden, D, n, n, 1, h->stream);
   if (!e) e = wf::nn_conv_fwd(A2, h->cl_w[2], h->cl_face, nullptr, Y, 6, kClHidden, 6, D, n, n, 0, h->stream);
+  if (!e) e = wf::face_scale(Y, 6, P, scale, 0, h->stream);
   if (!e) e = wf::band_scatter_add(g, Y, n, n, h->cl_ge, h->cl_gh, h->stream);
   return static_cast<cudaError_t>(e);
 }
@@ -392,7 +398,7 @@ wf_status enqueue_one(wf_handle *h) {
   if (h->closure) {
     e = closure_enqueue(h);
     if (e != cudaSuccess) return cuda_fail(h, e, "closure launch");
-    h->kernel_launches += 10;  // gather, 3 convs, 6 face scatters
+    h->kernel_launches += 13;  // gather, RMS, 2 scales, 3 convs, 6 face scatters
   }
   if (h->timing) {
     cudaEvent_t ev = timing_event(h);
@@ -1340,7 +1346,7 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
   }
   if (!h->cl_buf) {
     const long long P = static_cast<long long>(wf::kBandDepth) * h->nx * h->nx;
-    WF_CUDA(h, cudaMalloc(&h->cl_buf, sizeof(float) * 6 * P * (wf::kBandIn + 2 * kClHidden + 6)));
+    WF_CUDA(h, cudaMalloc(&h->cl_buf, sizeof(float) * (6 * P * (wf::kBandIn + 2 * kClHidden + 6) + 8)));
     const int faces[6] = {0, 1, 2, 3, 4, 5};
     WF_CUDA(h, cudaMalloc(&h->cl_face, sizeof(faces)));
     WF_CUDA(h, cudaMemcpy(h->cl_face, faces, sizeof(faces), cudaMemcpyHostToDevice));
