@@ -313,6 +313,90 @@ def cpu_baseline_batched(scenes, seconds=15.0):
             "sample": f"first {k} scenes x 10 steps each, {el:.1f} s (scene setup included)"}
 
 
+def run_closure(args, rank, world, local_rank):
+    """Learned thin-CPML closure: wall time of the same 224^3 physical
+    interior with a 16-cell CPML (256^3 cells) and with the 4-cell thin layer
+    (232^3 cells) alone and with the closure network applied every step (a
+    Ricker Ez source at the centre, vacuum), plus the reflection test (48^3
+    interior, 260 steps, against a reference domain nothing returns from)
+    of a closure trained here on teacher-forced samples (96 runs of 64^3)."""
+    import torch
+    from wavefront_b200 import closure as CL
+    from wavefront_b200 import configs
+    from wavefront_b200.engine import DeviceFieldGrid
+    from wavefront_b200.layout import GridDims, MaterialGrid, MaterialTable, PmlConfig, PmlContext
+    from wavefront_b200.source import FieldComponent, Source, default_waveform
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return
+    interior = 224
+    dx = 1.0e-3
+    dt = configs.courant_dt(dx)
+    wf_ = default_waveform("ricker", float(np.float32(configs.C0 / (20.0 * dx))))
+    total = args.warmup + args.steps
+    X, R, F, _ = CL.generate(96, seed=1, device=local_rank)
+    net, _ = CL.train(X, R, F, 1.0, iters=4000, lr=3e-4, device=local_rank)
+    del X, R, F
+
+    def timed(n, pml, closure):
+        dims = GridDims(n, n, n)
+        g = DeviceFieldGrid(dims, kernel="fused", device=local_rank)
+        try:
+            g.set_materials(MaterialGrid(dims), MaterialTable.vacuum_filled(dt, dx))
+            if pml == "thin":
+                CL.set_thin_cpml(g, dt, dx)
+            else:
+                g.set_pml(pml)
+            c = n // 2
+            s = Source(c, c, c, FieldComponent.Ez, 1.0, wf_)
+            g.add_source_values(s.x, s.y, s.z, s.component, s.values(dt, total))
+            if closure:
+                net.attach(g, 0.5)
+            g.step(args.warmup)
+            g.sync()
+            st = torch.cuda.ExternalStream(g.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k0 = g.kernel_launches
+            e0.record(st)
+            g.step(args.steps)
+            e1.record(st)
+            g.sync()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / args.steps, g.kernel_launches - k0
+        finally:
+            g.close()
+
+    n16 = interior + 32
+    thick_ms, _ = timed(n16, PmlContext.build(GridDims(n16, n16, n16), PmlConfig(thickness=16), dt, dx),
+                        False)
+    with ClockSampler(local_rank) as clk:
+        closure_ms, launches = timed(interior + 8, "thin", True)
+    thin_ms, _ = timed(interior + 8, "thin", False)
+    refl = {k: CL.reflection_test(**kw)["max_rel_error"] for k, kw in (
+        ("thin_layer_alone", {"truncated": True}),
+        ("thin_layer_with_closure_gain_0.5", {"net": net, "alpha": 0.5, "truncated": True}),
+        ("plain_cpml_4", {"cpml": 4}), ("plain_cpml_16", {"cpml": 16}))}
+    value = interior ** 3 / (closure_ms / 1e3) / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(closure_ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "interior": [interior] * 3,
+                   "cells_counted": "physical interior (224^3) per step",
+                   "closure": "per-face 3x3x3 conv 10-16-16-6, GELU, bf16 weights, fp32 accumulation, "
+                              "8-cell band, correction gain 0.5",
+                   "parallelism": "1 GPU"},
+        "comparison_ms_per_step": {"cpml16_256^3": round(thick_ms, 4),
+                                   "thin4_232^3_with_closure": round(closure_ms, 4),
+                                   "thin4_232^3_alone": round(thin_ms, 4)},
+        "reflection_test_max_rel_error": {k: round(v, 5) for k, v in refl.items()},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from wavefront_b200 import configs
@@ -455,7 +539,7 @@ def main():
     ap.add_argument("--grid", type=int, default=0,
                     help="cube edge (default 512 for two_spheres, 1024 for random_spheres)")
     ap.add_argument("--workload", default="two_spheres",
-                    choices=["two_spheres", "random_spheres", "batched"])
+                    choices=["two_spheres", "random_spheres", "batched", "closure"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
                     help="field storage (16-bit: per-slab power-of-two scales, FP32 math)")
     args = ap.parse_args()
@@ -465,6 +549,8 @@ def main():
     PRECISION = args.precision
     if args.workload == "batched":
         WORKLOAD = "batched_sweep_256_scenes_32-128^3_fp32_cpml10_ricker"
+    elif args.workload == "closure":
+        WORKLOAD = "learned_closure_224^3_interior_thin4_vs_cpml16_ricker"
     elif args.workload == "random_spheres":
         WORKLOAD = f"random_spheres_{GRID}^3_{PRECISION}_storage_cpml16_sinusoid_8probes"
     elif PRECISION == "f32":
@@ -480,6 +566,8 @@ def main():
         run_reference(args, rank, world)
     elif args.workload == "batched":
         run_batched(args, rank, world, local_rank)
+    elif args.workload == "closure":
+        run_closure(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 
