@@ -80,9 +80,10 @@ def test_closure_in_step_equals_explicit_pipeline():
         L.check(L.lib().wf_band_scatter_add(g2._h, CL._p(Y), net.gain_e, net.gain_h))
         torch.cuda.synchronize()
         got, want = g1.fields(), g2.fields()
-        # the per-face RMS is reduced in a different order here: allow its
-        # rounding to move the corrections by a few ulps
-        assert np.allclose(got, want, rtol=1e-5, atol=1e-9 * np.abs(want).max())
+        # the per-face RMS is reduced in a different order here, so the
+        # corrections may differ in their last bits: bound the difference by
+        # 1e-6 of the largest field value
+        assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
         assert not np.array_equal(got, f0)
     finally:
         g1.close()
