@@ -327,23 +327,25 @@ static inline float or_round_bf16(float v) {
   return or_u2f(u & 0xffff0000u);
 }
 
-/* Stores v as a 16-bit value of v * 2^-shift and returns the decoded f32
- * value: kind 1 = IEEE binary16, round to nearest even, finite values
- * saturating at +-65504; kind 2 = bf16, round to nearest even.  Scaling by a
- * power of two is exact, so the decoded value is exactly what a device
- * kernel storing the same format reads back.  (overflow is unused: the
- * simulation counts slabs whose maximum reached +-65504, see next_shifts.) */
-float or_store16(float v, int kind, int shift, long long *overflow) {
-  (void)overflow;
-  float u = v * ldexpf(1.0f, -shift);
+/* Rounds u to the 16-bit format: kind 1 = IEEE binary16, round to nearest
+ * even, finite values saturating at +-65504; kind 2 = bf16, round to nearest
+ * even.  The result is exactly what a device kernel reads back after storing
+ * u in that format. */
+float or_round16(float u, int kind) {
   if (kind == 1) {
     if (u > 65504.0f) u = 65504.0f;
     if (u < -65504.0f) u = -65504.0f;
-    u = (float)(_Float16)u;
-  } else {
-    u = or_round_bf16(u);
+    return (float)(_Float16)u;
   }
-  return u * ldexpf(1.0f, shift);
+  return or_round_bf16(u);
+}
+
+/* Stores v as a 16-bit value of v * 2^-shift and returns the decoded f32
+ * value (scaling by a power of two is exact).  overflow is unused: the
+ * simulation counts slabs whose maximum reached +-65504, see next_shifts. */
+float or_store16(float v, int kind, int shift, long long *overflow) {
+  (void)overflow;
+  return or_round16(v * ldexpf(1.0f, -shift), kind) * ldexpf(1.0f, shift);
 }
 
 #define REAL float

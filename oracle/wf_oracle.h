@@ -63,8 +63,9 @@ void or_demo_sphere(int nx, int ny, int nz, uint8_t *grid);
 /* Shift mapping a bound into [2^13, 2^14) (biased exponent - 140, clamped
  * to [-60, 15]). */
 int   or_store_shift(float bound);
-/* Decoded value of v stored as kind (1 f16 saturating, 2 bf16; both round to
- * nearest even) of v * 2^-shift. */
+/* u rounded to kind (1 f16 saturating, 2 bf16; both round to nearest even). */
+float or_round16(float u, int kind);
+/* Decoded value of v stored as kind of v * 2^-shift. */
 float or_store16(float v, int kind, int shift, long long *overflow);
 
 /* ---- the timestep engine (src/engine.rs, src/fdtd.rs) ------------------ */

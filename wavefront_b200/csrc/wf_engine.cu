@@ -95,11 +95,11 @@ struct wf_handle {
   bool cfg_user_set = false;  // otherwise chosen from the grid at first use
   wf::FusedMaps maps[2];      // per state buffer (the one read by the step)
   int *d_items = nullptr;     // work items grouped by kernel class
-  int class_off[5] = {0, 0, 0, 0, 0}, class_n[5] = {0, 0, 0, 0, 0};
+  int class_off[wf::kFusedClassCount] = {}, class_n[wf::kFusedClassCount] = {};
   // the class launches of one step run concurrently: forked from the main
   // stream onto these streams and joined back before the step tail
-  cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};
-  cudaEvent_t fork_ev = nullptr, join_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t side[wf::kFusedClassCount - 1] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[wf::kFusedClassCount - 1] = {};
   bool maps_ok = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_steps = 0;
@@ -222,14 +222,10 @@ wf_status build_maps(wf_handle *h) {
   // kernel instantiation that carries only the CPML code it needs.
   const FusedArgs a = fused_args(h);
   const int n_items = a.tiles_x * a.tiles_y * ((h->nz + a.zchunk - 1) / a.zchunk);
-  std::vector<int> lists[5];
-  for (int i = 0; i < n_items; ++i) {
-    const int c = wf::fused_item_class(a, h->cfg.ty, i);
-    for (int k = 0; k < 5; ++k)
-      if (wf::kFusedClasses[k] == c) lists[k].push_back(i);
-  }
+  std::vector<int> lists[wf::kFusedClassCount];
+  for (int i = 0; i < n_items; ++i) lists[wf::fused_item_class(a, h->cfg.ty, i)].push_back(i);
   std::vector<int> all;
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < wf::kFusedClassCount; ++k) {
     h->class_off[k] = static_cast<int>(all.size());
     h->class_n[k] = static_cast<int>(lists[k].size());
     all.insert(all.end(), lists[k].begin(), lists[k].end());
@@ -378,12 +374,12 @@ wf_status enqueue_one(wf_handle *h) {
     // streams forked from it; they touch disjoint cells of the next state
     WF_CUDA(h, cudaEventRecord(h->fork_ev, h->stream));
     e = cudaSuccess;
-    for (int k = 0; k < 5 && e == cudaSuccess; ++k) {
+    for (int k = 0; k < wf::kFusedClassCount && e == cudaSuccess; ++k) {
       if (h->class_n[k] == 0) continue;
       cudaStream_t s = k == 0 ? h->stream : h->side[k - 1];
       if (k > 0) WF_CUDA(h, cudaStreamWaitEvent(s, h->fork_ev, 0));
       e = wf::launch_fused(h->cfg, h->maps[h->cur], a, h->d_items + h->class_off[k],
-                           h->class_n[k], wf::kFusedClasses[k], fma, s);
+                           h->class_n[k], k, fma, s);
       if (e == cudaSuccess) h->kernel_launches += 1;
       if (e == cudaSuccess && k > 0) {
         WF_CUDA(h, cudaEventRecord(h->join_ev[k - 1], s));
@@ -671,7 +667,7 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaStreamCreate"));
     h->own_stream = true;
   }
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < wf::kFusedClassCount - 1; ++k) {
     if ((e = cudaStreamCreateWithFlags(&h->side[k], cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&h->join_ev[k], cudaEventDisableTiming)) != cudaSuccess)
       return cleanup_fail(cuda_fail(nullptr, e, "side stream setup"));
@@ -719,7 +715,7 @@ wf_status wf_destroy(wf_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   for (auto ev : h->ev_pool) cudaEventDestroy(ev);
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < wf::kFusedClassCount - 1; ++k) {
     if (h->side[k]) {
       cudaStreamSynchronize(h->side[k]);
       cudaStreamDestroy(h->side[k]);

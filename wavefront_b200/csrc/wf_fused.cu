@@ -31,7 +31,7 @@ int fused_item_class(const FusedArgs &a, int ty, int item) {
   if (X.T > 0 && (x0 - 1 < X.T || xh >= a.g.nx - X.T)) mask |= 1;
   if (Y.T > 0 && (y0 - 1 < Y.T || yh >= a.g.ny - Y.T)) mask |= 2;
   if (Z.T > 0 && (k0 - 1 < Z.T || k1 - 1 >= a.g.nz - Z.T)) mask |= 4;
-  return (mask == 0 || mask == 1 || mask == 2 || mask == 4) ? mask : 7;
+  return mask;
 }
 
 bool fused_supported(const FusedConfig &c, int prec) {

@@ -32,15 +32,20 @@
 // All per-cell arithmetic goes through wf_internal.cuh, so results are
 // bit-identical to the split kernels and to the reference.
 //
-// 16-bit storage: staged planes are decoded with their slab's shift as they
-// are read; every H value computed (tile, halo row and column, warm-up
-// plane) is rounded through the storage format before any use, exactly as
-// if it had been stored and re-read, and E values are rounded as they are
-// stored.  Each warp keeps the largest stored magnitude per slab and kind
-// and folds it into the slab maxima (one atomic per warp and slab).
+// 16-bit storage: a plane computes in the units of its slab's write shift
+// w.  Staged values are decoded into those units (a power-of-two factor only
+// where the read shift differs: a slab whose shift changed, or plane p+1 in
+// the next slab), H(p-1) is rescaled once when p enters a new slab, and psi
+// stays in field units (raw differences enter the recursion times 2^w and
+// leave it times 2^-w).  Every H value computed (tile, halo row and column,
+// warm-up plane) is rounded through the storage format before any use,
+// exactly as if it had been stored and re-read, and E values are rounded as
+// they are stored.  Each warp keeps the largest stored magnitude per slab
+// and kind and folds it into the slab maxima (one atomic per warp and slab).
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "wf_internal.cuh"
 #include "wf_launch.h"
@@ -160,14 +165,27 @@ __device__ __forceinline__ Psi2 load_psi2(const PmlAxis &P, int comp0, long long
   return Psi2{ldg4(P.psi_cur + comp0 * P.cells + idx), ldg4(P.psi_cur + (comp0 + 1) * P.cells + idx)};
 }
 
+// Computing units <-> field units of psi: 16-bit storage (U) computes in
+// units of 2^w (su = 2^w, iu = 2^-w) and keeps psi in field units, so a raw
+// difference enters the recursion times su and its result leaves times iu
+// (both exact).
+struct Units {
+  float su, iu;
+};
+template <bool FMA, bool U>
+__device__ __forceinline__ float corr_u(float raw, float b, float a, float ik, float &psi, Units u) {
+  if (!U) return pml_corr<FMA>(raw, b, a, ik, psi);
+  return __fmul_rn(pml_corr<FMA>(__fmul_rn(raw, u.su), b, a, ik, psi), u.iu);
+}
+
 // psi recursion of one axis over 4 cells with one coefficient set (y, z).
-template <bool FMA>
+template <bool FMA, bool U>
 __device__ __forceinline__ void corr4_uniform(float d0[4], float d1[4], Psi2 &q, float b, float a,
-                                              float ik) {
+                                              float ik, Units u) {
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    d0[i] = pml_corr<FMA>(d0[i], b, a, ik, el(q.p0, i));
-    d1[i] = pml_corr<FMA>(d1[i], b, a, ik, el(q.p1, i));
+    d0[i] = corr_u<FMA, U>(d0[i], b, a, ik, el(q.p0, i), u);
+    d1[i] = corr_u<FMA, U>(d1[i], b, a, ik, el(q.p1, i), u);
   }
 }
 
@@ -183,47 +201,33 @@ struct Prof {
 };
 
 // x axis: per-cell coefficients at slab positions s0..s0+3.
-template <bool FMA>
-__device__ __forceinline__ void corr4_x(float d0[4], float d1[4], Psi2 &q, const Prof &pf, int s0) {
+template <bool FMA, bool U>
+__device__ __forceinline__ void corr4_x(float d0[4], float d1[4], Psi2 &q, const Prof &pf, int s0,
+                                        Units u) {
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const float b = pf.b(0, s0 + i), a = pf.a(0, s0 + i), ik = pf.ik(0, s0 + i);
-    d0[i] = pml_corr<FMA>(d0[i], b, a, ik, el(q.p0, i));
-    d1[i] = pml_corr<FMA>(d1[i], b, a, ik, el(q.p1, i));
+    d0[i] = corr_u<FMA, U>(d0[i], b, a, ik, el(q.p0, i), u);
+    d1[i] = corr_u<FMA, U>(d1[i], b, a, ik, el(q.p1, i), u);
   }
 }
 
-// x axis, one cell at a time (lanes straddling a slab edge, the x-halo cell).
-template <bool FMA>
+// x axis, one cell at a time (lanes straddling a slab edge).
+template <bool FMA, bool U>
 __device__ __forceinline__ void corr_x_cell(const GridArgs &g, const Prof &pf, int comp0, int x,
-                                            int y, int p, float &d0, float &d1, bool store) {
+                                            int y, int p, float &d0, float &d1, bool store, Units u) {
   const PmlAxis &P = g.pml[0];
   const int s = slab_pos(x, g.nx, P.T, P.W);
   if (s < 0) return;
   const long long idx = (static_cast<long long>(p) * g.ny + y) * P.pitch + s;
   float p0 = __ldg(P.psi_cur + comp0 * P.cells + idx), p1 = __ldg(P.psi_cur + (comp0 + 1) * P.cells + idx);
   const float b = pf.b(0, s), a = pf.a(0, s), ik = pf.ik(0, s);
-  d0 = pml_corr<FMA>(d0, b, a, ik, p0);
-  d1 = pml_corr<FMA>(d1, b, a, ik, p1);
+  d0 = corr_u<FMA, U>(d0, b, a, ik, p0, u);
+  d1 = corr_u<FMA, U>(d1, b, a, ik, p1, u);
   if (store) {
     P.psi_nxt[comp0 * P.cells + idx] = p0;
     P.psi_nxt[(comp0 + 1) * P.cells + idx] = p1;
   }
-}
-
-// y or z axis, one cell (the x-halo cell).
-template <bool FMA>
-__device__ __forceinline__ void corr_yz_cell(const GridArgs &g, const Prof &pf, int axis, int x,
-                                             int y, int p, float &d0, float &d1) {
-  const PmlAxis &P = g.pml[axis];
-  const int s = axis == 1 ? slab_pos(y, g.ny, P.T, P.W) : slab_pos(p, g.nz, P.T, P.W);
-  if (s < 0) return;
-  const long long idx = axis == 1 ? (static_cast<long long>(p) * P.W + s) * g.nx + x
-                                  : (static_cast<long long>(s) * g.ny + y) * g.nx + x;
-  float p0 = __ldg(P.psi_cur + idx), p1 = __ldg(P.psi_cur + P.cells + idx);
-  const float b = pf.b(axis, s), a = pf.a(axis, s), ik = pf.ik(axis, s);
-  d0 = pml_corr<FMA>(d0, b, a, ik, p0);
-  d1 = pml_corr<FMA>(d1, b, a, ik, p1);
 }
 
 // AX: the CPML axes this body handles (bit 1 x, 2 y, 4 z; 0 = interior).
@@ -280,25 +284,28 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   const bool cell_ok = row_in && x_in;
   const int cE = PAD + 4 * lane;
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;  // H(p-1), own cells
+  // E(p+1) of the own row as decoded for plane p's z differences: plane p+1's
+  // own ex, ey when the warp worked on plane p and p+1 is in the same slab
+  float4 ex_nx = hxp, ey_nx = hxp;
+  bool have_nx = false;
   ST *const nxt = reinterpret_cast<ST *>(g.nxt);
   // 16-bit storage: this thread's largest stored E, H magnitudes in slab
-  // `mslab` (two 16-bit lanes each, compared as integers: one shift per slab
-  // and kind) and that slab's decode scales
+  // sl_c (two 16-bit lanes each, compared as integers: one shift per slab),
+  // that slab's write shift w_c, and the unit factors of the plane: fC
+  // (plane p's stored values into units of 2^w_c), fN (plane p+1's) and su,
+  // iu (field units <-> computing units)
   unsigned mxE = 0, mxH = 0;
-  float wsE = 1.0f, wsH = 1.0f;
-  int mslab = kfirst / kSlabPlanes;
-  // storage scales, reloaded when plane p or p+1 enters another slab:
-  // decode of planes p (E, H) and p+1 (E), encode and decode of the writes
-  float sEc = 1.0f, sEn = 1.0f, sHc = 1.0f, sEw = 1.0f, iEw = 1.0f, sHw = 1.0f, iHw = 1.0f;
-  int sl_c = -1, sl_n = -1;
+  int sl_c = -1, w_c = 0;
+  float fC = 1.0f, fN = 1.0f;
+  Units un{1.0f, 1.0f};
   auto flush_max = [&]() {
     if constexpr (SD::k16) {
       const unsigned e = __reduce_max_sync(0xffffffffu, max(mxE & 0xffffu, mxE >> 16));
       const unsigned h = __reduce_max_sync(0xffffffffu, max(mxH & 0xffffu, mxH >> 16));
       if (lane == 0 && e)
-        atomicMax(g.slab_max + 2 * mslab, __float_as_uint(__fmul_rn(SD::dec_lo(e), wsE)));
+        atomicMax(g.slab_max + 2 * sl_c, __float_as_uint(__fmul_rn(SD::dec_lo(e), un.su)));
       if (lane == 0 && h)
-        atomicMax(g.slab_max + 2 * mslab + 1, __float_as_uint(__fmul_rn(SD::dec_lo(h), wsH)));
+        atomicMax(g.slab_max + 2 * sl_c + 1, __float_as_uint(__fmul_rn(SD::dec_lo(h), un.su)));
       mxE = mxH = 0;
     }
   };
@@ -361,27 +368,26 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     HaloPsi hh = hh_n;  // (pml_corr updates its psi argument in place)
 
     if constexpr (SD::k16) {
-      const int sl = p / kSlabPlanes, sln = min((p + 1) / kSlabPlanes, g.nslab - 1);
-      if (sl != mslab) {
-        flush_max();
-        mslab = sl;
-      }
+      const int sl = p / kSlabPlanes;
       if (sl != sl_c) {
+        const int w = __ldg(g.shift_wr + 2 * sl);
+        if (sl_c >= 0) {
+          flush_max();
+          if (w != w_c) {  // H(p-1), computed in the previous slab's units
+            const float f = pow2f(w_c - w);
+            hxp = make_float4(__fmul_rn(hxp.x, f), __fmul_rn(hxp.y, f), __fmul_rn(hxp.z, f),
+                              __fmul_rn(hxp.w, f));
+            hyp = make_float4(__fmul_rn(hyp.x, f), __fmul_rn(hyp.y, f), __fmul_rn(hyp.z, f),
+                              __fmul_rn(hyp.w, f));
+          }
+        }
         sl_c = sl;
-        sEc = SD::dscale(__ldg(g.shift_rd + 2 * sl));
-        sHc = SD::dscale(__ldg(g.shift_rd + 2 * sl + 1));
-        const int we = __ldg(g.shift_wr + 2 * sl), wh = __ldg(g.shift_wr + 2 * sl + 1);
-        sEw = SD::dscale(we);
-        iEw = pow2f(-we);
-        sHw = SD::dscale(wh);
-        iHw = pow2f(-wh);
-        wsE = sEw;
-        wsH = sHw;
+        w_c = w;
+        un = Units{pow2f(w), pow2f(-w)};
+        fC = pow2f(__ldg(g.shift_rd + 2 * sl) - w);
       }
-      if (sln != sl_n) {
-        sl_n = sln;
-        sEn = SD::dscale(__ldg(g.shift_rd + 2 * sln));
-      }
+      const int sln = min((p + 1) / kSlabPlanes, g.nslab - 1);
+      fN = sln == sl ? fC : pow2f(__ldg(g.shift_rd + 2 * sln) - w_c);
     }
 
     const bool arrived = mbar_wait(smem_u32(&s_bar[(j + 1) % S]), ((j + 1) / S) & 1);
@@ -402,23 +408,45 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     uchar4 m4;
     Psi2 ex_{}, ey_{}, ez_{};  // E-term psi (x, y, z axes), loaded before the barrier
     if (active) {
-      auto E4 = [&](const ST *B, int c, int row, float s) {
-        return SD::ld4(B + (c * L::EH + row) * L::EW + cE, s);
+      // the staged values in computing units (SC: times fC / fN)
+      float4 ex_py, ez_py, ex_pz, ey_pz, hx4, hy4, hz4;
+      auto load = [&](auto sc) {
+        constexpr bool SC = decltype(sc)::value;
+        auto E4 = [&](const ST *B, int c, int row, float f) {
+          return SD::template ld4<SC>(B + (c * L::EH + row) * L::EW + cE, f);
+        };
+        if (have_nx && (!SD::k16 || p % kSlabPlanes != 0)) {
+          ex4 = ex_nx;
+          ey4 = ey_nx;
+        } else {
+          ex4 = E4(Ec, 0, r, fC);
+          ey4 = E4(Ec, 1, r, fC);
+        }
+        ez4 = E4(Ec, 2, r, fC);
+        ex_py = E4(Ec, 0, r + 1, fC);
+        ez_py = E4(Ec, 2, r + 1, fC);
+        ex_pz = E4(En, 0, r, fN);
+        ey_pz = E4(En, 1, r, fN);
+        hx4 = SD::template ld4<SC>(Hc + (0 * L::HH + r) * L::HW + cE, fC);
+        hy4 = SD::template ld4<SC>(Hc + (1 * L::HH + r) * L::HW + cE, fC);
+        hz4 = SD::template ld4<SC>(Hc + (2 * L::HH + r) * L::HW + cE, fC);
       };
-      ex4 = E4(Ec, 0, r, sEc);
-      ey4 = E4(Ec, 1, r, sEc);
-      ez4 = E4(Ec, 2, r, sEc);
-      const float4 ex_py = E4(Ec, 0, r + 1, sEc), ez_py = E4(Ec, 2, r + 1, sEc);
-      const float4 ex_pz = E4(En, 0, r, sEn), ey_pz = E4(En, 1, r, sEn);
+      if constexpr (SD::k16) {
+        if (fC != 1.0f || fN != 1.0f)
+          load(std::true_type{});
+        else
+          load(std::false_type{});
+      } else {
+        load(std::false_type{});
+      }
+      ex_nx = ex_pz;
+      ey_nx = ey_pz;
       float ez_n = __shfl_down_sync(0xffffffffu, ez4.x, 1);
       float ey_n = __shfl_down_sync(0xffffffffu, ey4.x, 1);
       if (lane == 31) {
-        ez_n = SD::ld1(Ec + (2 * L::EH + r) * L::EW + PAD + kTileX, sEc);
-        ey_n = SD::ld1(Ec + (1 * L::EH + r) * L::EW + PAD + kTileX, sEc);
+        ez_n = SD::template ld1<SD::k16>(Ec + (2 * L::EH + r) * L::EW + PAD + kTileX, fC);
+        ey_n = SD::template ld1<SD::k16>(Ec + (1 * L::EH + r) * L::EW + PAD + kTileX, fC);
       }
-      const float4 hx4 = SD::ld4(Hc + (0 * L::HH + r) * L::HW + cE, sHc);
-      const float4 hy4 = SD::ld4(Hc + (1 * L::HH + r) * L::HW + cE, sHc);
-      const float4 hz4 = SD::ld4(Hc + (2 * L::HH + r) * L::HW + cE, sHc);
       m4 = *reinterpret_cast<const uchar4 *>(Mc + r * L::MW + 16 + 4 * lane);
 
       float d_ez_dy[4], d_ex_dy[4], d_ey_dz[4], d_ex_dz[4], d_ez_dx[4], d_ey_dx[4];
@@ -434,7 +462,7 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       if (PML && cell_ok) {  // CPML on the H terms (pml_correct_*, src/fdtd.rs:136-163)
         const bool wpsi = tile_warp && !warm;
         if (AXX && lp.xmode == 1) {
-          corr4_x<FMA>(d_ez_dx, d_ey_dx, qx, pf, lp.sx);
+          corr4_x<FMA, SD::k16>(d_ez_dx, d_ey_dx, qx, pf, lp.sx, un);
           if (wpsi) {
             const PmlAxis &P = g.pml[0];
             stg4(P.psi_nxt + lp.ix, qx.p0);
@@ -443,10 +471,11 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         } else if (AXX && lp.xmode == 2) {
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            corr_x_cell<FMA>(g, pf, 0, xg + q, y, p, d_ez_dx[q], d_ey_dx[q], wpsi);
+            corr_x_cell<FMA, SD::k16>(g, pf, 0, xg + q, y, p, d_ez_dx[q], d_ey_dx[q], wpsi, un);
         }
         if (AXY && lp.y) {
-          corr4_uniform<FMA>(d_ez_dy, d_ex_dy, qy, pf.b(1, lp.sy), pf.a(1, lp.sy), pf.ik(1, lp.sy));
+          corr4_uniform<FMA, SD::k16>(d_ez_dy, d_ex_dy, qy, pf.b(1, lp.sy), pf.a(1, lp.sy),
+                                      pf.ik(1, lp.sy), un);
           if (wpsi) {
             const PmlAxis &P = g.pml[1];
             stg4(P.psi_nxt + lp.iy, qy.p0);
@@ -454,7 +483,8 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
           }
         }
         if (AXZ && lp.z) {
-          corr4_uniform<FMA>(d_ey_dz, d_ex_dz, qz, pf.b(2, lp.sz), pf.a(2, lp.sz), pf.ik(2, lp.sz));
+          corr4_uniform<FMA, SD::k16>(d_ey_dz, d_ex_dz, qz, pf.b(2, lp.sz), pf.a(2, lp.sz),
+                                      pf.ik(2, lp.sz), un);
           if (wpsi) {
             const PmlAxis &P = g.pml[2];
             stg4(P.psi_nxt + lp.iz, qz.p0);
@@ -481,11 +511,11 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       }
       // every H value is used as stored (16-bit: rounded here, in place)
       const bool hstore = !warm && tile_warp && cell_ok;
-      const typename SD::Word wa = SD::enc4(ha, iHw);
-      const typename SD::Word wb = SD::enc4(hb, iHw);
-      const typename SD::Word wc = SD::enc4(hc, iHw);
+      const typename SD::Word wa = SD::enc4(ha);
+      const typename SD::Word wb = SD::enc4(hb);
+      const typename SD::Word wc = SD::enc4(hc);
       if constexpr (SD::k16) {
-        const float4 da = SD::dec4(wa, sHw), db = SD::dec4(wb, sHw), dc = SD::dec4(wc, sHw);
+        const float4 da = SD::dec4(wa), db = SD::dec4(wb), dc = SD::dec4(wc);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           ha[q] = comp(da, q);
@@ -513,42 +543,46 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         const int rh = lane + 1, yh = y0 + lane;
         float hzv = 0.0f, hyv = 0.0f;
         if (x0 > 0 && yh < ny) {
-          auto Ev = [&](const ST *B, int c, int row, int col, float s) {
-            return SD::ld1(B + (c * L::EH + row) * L::EW + col, s);
+          auto Ev = [&](const ST *B, int c, int row, int col, float f) {
+            return SD::template ld1<SD::k16>(B + (c * L::EH + row) * L::EW + col, f);
           };
-          const float ex = Ev(Ec, 0, rh, PAD - 1, sEc);
-          const float ey = Ev(Ec, 1, rh, PAD - 1, sEc);
-          const float ez = Ev(Ec, 2, rh, PAD - 1, sEc);
-          float d_ez_dx1 = sub(Ev(Ec, 2, rh, PAD, sEc), ez);
-          float d_ey_dx1 = sub(Ev(Ec, 1, rh, PAD, sEc), ey);
-          float d_ex_dz1 = sub(Ev(En, 0, rh, PAD - 1, sEn), ex);
-          float d_ey_dz1 = sub(Ev(En, 1, rh, PAD - 1, sEn), ey);
-          float d_ex_dy1 = sub(Ev(Ec, 0, rh + 1, PAD - 1, sEc), ex);
-          float d_ez_dy1 = sub(Ev(Ec, 2, rh + 1, PAD - 1, sEc), ez);
+          const float ex = Ev(Ec, 0, rh, PAD - 1, fC);
+          const float ey = Ev(Ec, 1, rh, PAD - 1, fC);
+          const float ez = Ev(Ec, 2, rh, PAD - 1, fC);
+          float d_ez_dx1 = sub(Ev(Ec, 2, rh, PAD, fC), ez);
+          float d_ey_dx1 = sub(Ev(Ec, 1, rh, PAD, fC), ey);
+          float d_ex_dz1 = sub(Ev(En, 0, rh, PAD - 1, fN), ex);
+          float d_ey_dz1 = sub(Ev(En, 1, rh, PAD - 1, fN), ey);
+          float d_ex_dy1 = sub(Ev(Ec, 0, rh + 1, PAD - 1, fC), ex);
+          float d_ez_dy1 = sub(Ev(Ec, 2, rh + 1, PAD - 1, fC), ez);
+          constexpr bool U = SD::k16;
           if (AXX && hh.sx >= 0) {
-            d_ez_dx1 = pml_corr<FMA>(d_ez_dx1, pf.b(0, hh.sx), pf.a(0, hh.sx), pf.ik(0, hh.sx), hh.x0);
-            d_ey_dx1 = pml_corr<FMA>(d_ey_dx1, pf.b(0, hh.sx), pf.a(0, hh.sx), pf.ik(0, hh.sx), hh.x1);
+            const float b = pf.b(0, hh.sx), a_ = pf.a(0, hh.sx), ik = pf.ik(0, hh.sx);
+            d_ez_dx1 = corr_u<FMA, U>(d_ez_dx1, b, a_, ik, hh.x0, un);
+            d_ey_dx1 = corr_u<FMA, U>(d_ey_dx1, b, a_, ik, hh.x1, un);
           }
           if (AXY && hh.sy >= 0) {
-            d_ez_dy1 = pml_corr<FMA>(d_ez_dy1, pf.b(1, hh.sy), pf.a(1, hh.sy), pf.ik(1, hh.sy), hh.y0);
-            d_ex_dy1 = pml_corr<FMA>(d_ex_dy1, pf.b(1, hh.sy), pf.a(1, hh.sy), pf.ik(1, hh.sy), hh.y1);
+            const float b = pf.b(1, hh.sy), a_ = pf.a(1, hh.sy), ik = pf.ik(1, hh.sy);
+            d_ez_dy1 = corr_u<FMA, U>(d_ez_dy1, b, a_, ik, hh.y0, un);
+            d_ex_dy1 = corr_u<FMA, U>(d_ex_dy1, b, a_, ik, hh.y1, un);
           }
           if (AXZ && hh.sz >= 0) {
-            d_ey_dz1 = pml_corr<FMA>(d_ey_dz1, pf.b(2, hh.sz), pf.a(2, hh.sz), pf.ik(2, hh.sz), hh.z0);
-            d_ex_dz1 = pml_corr<FMA>(d_ex_dz1, pf.b(2, hh.sz), pf.a(2, hh.sz), pf.ik(2, hh.sz), hh.z1);
+            const float b = pf.b(2, hh.sz), a_ = pf.a(2, hh.sz), ik = pf.ik(2, hh.sz);
+            d_ey_dz1 = corr_u<FMA, U>(d_ey_dz1, b, a_, ik, hh.z0, un);
+            d_ex_dz1 = corr_u<FMA, U>(d_ex_dz1, b, a_, ik, hh.z1, un);
           }
           const float4 cf = s_coef[Mc[rh * L::MW + 15]];
-          hyv = h_new<FMA>(cf.z, SD::ld1(Hc + (1 * L::HH + rh) * L::HW + PAD - 1, sHc), cf.w,
-                           sub(d_ex_dz1, d_ez_dx1));
-          hzv = h_new<FMA>(cf.z, SD::ld1(Hc + (2 * L::HH + rh) * L::HW + PAD - 1, sHc), cf.w,
-                           sub(d_ey_dx1, d_ex_dy1));
-          hyv = SD::rt(hyv, iHw, sHw);
-          hzv = SD::rt(hzv, iHw, sHw);
+          auto Hv = [&](int c) {
+            return SD::template ld1<SD::k16>(Hc + (c * L::HH + rh) * L::HW + PAD - 1, fC);
+          };
+          hyv = SD::rt(h_new<FMA>(cf.z, Hv(1), cf.w, sub(d_ex_dz1, d_ez_dx1)));
+          hzv = SD::rt(h_new<FMA>(cf.z, Hv(2), cf.w, sub(d_ey_dx1, d_ex_dy1)));
         }
         pl_hzh[rh] = hzv;
         pl_hyh[rh] = hyv;
       }
     }
+    have_nx = active;
     if (PML && cell_ok && j + 1 < np - 1) prefetch(p + 1);  // next plane's H terms
     if (xhalo && j + 1 < np - 1) prefetch_halo(p + 1);
 
@@ -584,23 +618,25 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         if (PML && cell_ok) {
           if (AXX && lp.xmode == 1) {
             const PmlAxis &P = g.pml[0];
-            corr4_x<FMA>(d_hz_dx, d_hy_dx, ex_, pf, lp.sx);
+            corr4_x<FMA, SD::k16>(d_hz_dx, d_hy_dx, ex_, pf, lp.sx, un);
             stg4(P.psi_nxt + 2 * P.cells + lp.ix, ex_.p0);
             stg4(P.psi_nxt + 3 * P.cells + lp.ix, ex_.p1);
           } else if (AXX && lp.xmode == 2) {
 #pragma unroll
             for (int q = 0; q < 4; ++q)
-              corr_x_cell<FMA>(g, pf, 2, xg + q, y, p, d_hz_dx[q], d_hy_dx[q], true);
+              corr_x_cell<FMA, SD::k16>(g, pf, 2, xg + q, y, p, d_hz_dx[q], d_hy_dx[q], true, un);
           }
           if (AXY && lp.y) {
             const PmlAxis &P = g.pml[1];
-            corr4_uniform<FMA>(d_hz_dy, d_hx_dy, ey_, pf.b(1, lp.sy), pf.a(1, lp.sy), pf.ik(1, lp.sy));
+            corr4_uniform<FMA, SD::k16>(d_hz_dy, d_hx_dy, ey_, pf.b(1, lp.sy), pf.a(1, lp.sy),
+                                        pf.ik(1, lp.sy), un);
             stg4(P.psi_nxt + 2 * P.cells + lp.iy, ey_.p0);
             stg4(P.psi_nxt + 3 * P.cells + lp.iy, ey_.p1);
           }
           if (AXZ && lp.z) {
             const PmlAxis &P = g.pml[2];
-            corr4_uniform<FMA>(d_hy_dz, d_hx_dz, ez_, pf.b(2, lp.sz), pf.a(2, lp.sz), pf.ik(2, lp.sz));
+            corr4_uniform<FMA, SD::k16>(d_hy_dz, d_hx_dz, ez_, pf.b(2, lp.sz), pf.a(2, lp.sz),
+                                        pf.ik(2, lp.sz), un);
             stg4(P.psi_nxt + 2 * P.cells + lp.iz, ez_.p0);
             stg4(P.psi_nxt + 3 * P.cells + lp.iz, ez_.p1);
           }
@@ -616,8 +652,7 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
             eo[2][q] = e_new<FMA>(cf.x, comp(ez4, q), cf.y, sub(d_hy_dx[q], d_hx_dy[q]));
           }
           ST *Ep = nxt + (static_cast<long long>(p) * ny + y) * nx + xg;
-          const typename SD::Word w0 = SD::enc4(eo[0], iEw), w1 = SD::enc4(eo[1], iEw),
-                                   w2 = SD::enc4(eo[2], iEw);
+          const typename SD::Word w0 = SD::enc4(eo[0]), w1 = SD::enc4(eo[1]), w2 = SD::enc4(eo[2]);
           SD::st4(Ep, w0);
           SD::st4(Ep + N, w1);
           SD::st4(Ep + 2 * N, w2);
@@ -645,13 +680,19 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   }
 }
 
-// One launch handles one class of work items: interior items (AX = 0: no
-// CPML code, lean registers), items meeting only the x, only the y or only
-// the z slab (AX = 1, 2, 4), or items meeting several (AX = 7).  The host
-// lists each class's items (tile x, tile y, z chunk); the launches
-// partition the grid.
+// One launch handles one class of work items, named by the mask of the CPML
+// slabs its items meet (1 x, 2 y, 4 z): interior items (AX = 0: no CPML
+// code, lean registers) and one instantiation per combination, so that each
+// item runs only the psi code of its own axes.  The host lists each class's
+// items (tile x, tile y, z chunk); the launches partition the grid.
+// Three CTAs per SM at 4 tile rows, except for items on two or three CPML
+// axes, whose psi registers (prefetched H terms, in-flight E terms) need
+// more than a third of the register file: two CTAs there, without spills.
+template <int AX>
+constexpr int kMultiAxis = (AX & (AX - 1)) != 0;
+
 template <int TY, int S, bool FMA, int AX, typename ST>
-__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 3 : 1)
+__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? (kMultiAxis<AX> ? 2 : 3) : 1)
     k_fused(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
             const __grid_constant__ CUtensorMap tmM, const FusedArgs a, const int *items) {
   using L = Layout<TY, S, ST>;
@@ -693,7 +734,7 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 3 : 1)
 // mbarrier ring is re-initialised per item (every copy of the previous item
 // has completed: the body consumes or drains all it issued).
 template <int TY, int S>
-__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 3 : 1)
+__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 2 : 1)
     k_fused_batch(const BatchScene *scenes, const int2 *items, int n_items, int *counter,
                   int parity) {
   using L = Layout<TY, S, float>;
@@ -774,7 +815,7 @@ int batch_ctas_per_sm_t() {
   return n;
 }
 
-#define WF_AX_CLASSES(X) X(0) X(1) X(2) X(4) X(7)
+#define WF_AX_CLASSES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
 
 template <int TY, int S, bool FMA, typename ST>
 cudaError_t prepare_t() {

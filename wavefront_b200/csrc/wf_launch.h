@@ -67,10 +67,10 @@ bool fused_supported(const FusedConfig &c, int prec);
 int fused_smem_bytes(const FusedConfig &c, int prec);
 // Sets the kernels' dynamic shared-memory limit (call outside graph capture).
 cudaError_t fused_prepare(const FusedConfig &c, int prec);
-// Kernel class of work item `item` (tile x, tile y, z chunk): 0 interior,
-// 1 / 2 / 4 meets only the x / y / z CPML slab, 7 meets several.
+// Kernel class of work item `item` (tile x, tile y, z chunk): the mask of
+// the CPML slabs it meets (1 x, 2 y, 4 z; 0 interior).
 int fused_item_class(const FusedArgs &a, int ty, int item);
-constexpr int kFusedClasses[5] = {0, 1, 2, 4, 7};
+constexpr int kFusedClassCount = 8;
 // Launches the kernel of class `ax` over a device list of n_items items.
 cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                          const int *items, int n_items, int ax, bool fma, cudaStream_t s);

@@ -150,12 +150,12 @@ __global__ void k_split_e(GridArgs g) {
   En[2 * N + i] = e_new<FMA>(cf.x, E[2 * N + i], cf.y, curl_ez);
 }
 
-// One stored value of a 16-bit state: decode / encode with a shift.
+// One stored value of a 16-bit state in field units: decode / encode with a
+// shift.
 __device__ __forceinline__ float dec16(const void *f, long long i, int prec, int shift) {
   const unsigned b = static_cast<const unsigned short *>(f)[i];
-  return prec == kPrecF16 ? __fmul_rn(Store<__half>::dec_lo(b), Store<__half>::dscale(shift))
-                          : __fmul_rn(Store<__nv_bfloat16>::dec_lo(b),
-                                      Store<__nv_bfloat16>::dscale(shift));
+  return __fmul_rn(prec == kPrecF16 ? Store<__half>::dec_lo(b) : Store<__nv_bfloat16>::dec_lo(b),
+                   pow2f(shift));
 }
 // stores v; returns the decoded stored value
 __device__ __forceinline__ float enc16(void *f, long long i, int prec, int shift, float v) {
@@ -171,7 +171,8 @@ __device__ __forceinline__ float enc16(void *f, long long i, int prec, int shift
 // through the largest Cb/Db times 8 (four raw differences, each at most
 // doubled by the CPML correction), and the soft-source amplitudes that
 // step adds:  bh = 2*NH + kh*NE,  be = 2*NE + ke*bh + src  (f32, this
-// order); shift = store_shift_bits(bound).  Whole CTA; s_src >= nslab.
+// order); the slab's shift (E and H alike) = store_shift_bits(max(be, bh)).
+// Whole CTA; s_src >= nslab.
 // count_sat (after a step, binary16): every slab and kind whose maximum is
 // binary16's largest finite magnitude (where .satfinite puts overflowing
 // values) adds one to *ovf.
@@ -210,8 +211,9 @@ __device__ void next_shifts(const TailArgs &t, long long next, float *s_src, boo
     const float ne = __uint_as_float(me), nh = __uint_as_float(mh);
     const float bh = __fadd_rn(__fmul_rn(2.0f, nh), __fmul_rn(t.kh, ne));
     const float be = __fadd_rn(__fadd_rn(__fmul_rn(2.0f, ne), __fmul_rn(t.ke, bh)), s_src[b]);
-    t.shift_next[2 * b] = store_shift_bits(__float_as_uint(be));
-    t.shift_next[2 * b + 1] = store_shift_bits(__float_as_uint(bh));
+    const int sh = store_shift_bits(__float_as_uint(fmaxf(be, bh)));
+    t.shift_next[2 * b] = sh;
+    t.shift_next[2 * b + 1] = sh;
   }
   __syncthreads();
   for (int b = threadIdx.x; b < 2 * t.nslab; b += blockDim.x) t.slab_max[b] = 0u;
@@ -301,7 +303,8 @@ __global__ void k_next_shifts(TailArgs t, long long next) {
 }
 
 // 16-bit state from FP32 values, in three passes: slab maxima of the input,
-// the shifts they give, then the encoding (whose maxima remain).
+// the shift they give each slab (from the larger of its E and H maxima),
+// then the encoding (whose maxima remain).
 __global__ void k_slab_max_f32(const float *in, long long N, int nxy, unsigned *slab_max) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= 6 * N) return;
@@ -310,11 +313,13 @@ __global__ void k_slab_max_f32(const float *in, long long N, int nxy, unsigned *
   const unsigned v = __float_as_uint(fabsf(in[i]));
   if (v) atomicMax(slab_max + 2 * b + (c >= 3), v);
 }
-__global__ void k_shift_from_max(unsigned *slab_max, int *shift, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  shift[i] = store_shift_bits(slab_max[i]);
-  slab_max[i] = 0u;
+__global__ void k_shift_from_max(unsigned *slab_max, int *shift, int nslab) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nslab) return;
+  const int sh = store_shift_bits(max(slab_max[2 * b], slab_max[2 * b + 1]));
+  shift[2 * b] = sh;
+  shift[2 * b + 1] = sh;
+  slab_max[2 * b] = slab_max[2 * b + 1] = 0u;
 }
 __global__ void k_encode(const float *in, void *out, int prec, long long N, int nxy,
                          const int *shift, unsigned *slab_max) {
@@ -408,7 +413,7 @@ cudaError_t launch_encode_state(const float *in, void *out, int prec, int nx, in
   cudaError_t e = cudaMemsetAsync(slab_max, 0, sizeof(unsigned) * 2 * nslab, s);
   if (e != cudaSuccess) return e;
   k_slab_max_f32<<<blocks, 256, 0, s>>>(in, N, nx * ny, slab_max);
-  k_shift_from_max<<<(2 * nslab + 255) / 256, 256, 0, s>>>(slab_max, shift, 2 * nslab);
+  k_shift_from_max<<<(nslab + 255) / 256, 256, 0, s>>>(slab_max, shift, nslab);
   (void)ovf;  // encoding a given state saturates nothing it has to report
   k_encode<<<blocks, 256, 0, s>>>(in, out, prec, N, nx * ny, shift, slab_max);
   return cudaGetLastError();
