@@ -187,14 +187,18 @@ bool encode(CUtensorMap *m, CUtensorMapDataType t, int rank, void *base, const c
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tiling used unless the caller set one (best measured at 512^3 on B200).
+FusedConfig default_cfg(const wf_handle *h) {
+  return store16(h) ? FusedConfig{4, 12, 4} : FusedConfig{4, 12, 3};
+}
+
 // TMA descriptors per state buffer: fields as a 4D tensor {nx, ny, nz, 6},
 // ids as {nx, ny, nz} with a 16-byte-multiple row pitch, and each CPML
 // axis's psi slab as a 4D tensor {.., .., .., 4 terms}.
 wf_status build_maps(wf_handle *h) {
   h->maps_ok = false;
   if (!encode_fn()) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
-  if (!h->cfg_user_set) h->cfg = FusedConfig{4, 12, 3};  // best measured at 512^3 on B200
-  if (store16(h) && !h->cfg_user_set) h->cfg = FusedConfig{4, 12, 4};
+  if (!h->cfg_user_set) h->cfg = default_cfg(h);
   unsigned eb[4], hb[4], mb[3];
   wf::fused_boxes(h->cfg.ty, h->precision, eb, hb, mb);
   const cuuint64_t es = elem_bytes(h);
@@ -1218,9 +1222,10 @@ wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches) {
 
 wf_status wf_get_tiling(const wf_handle *h, wf_tiling *out) {
   if (!h || !out) return WF_ERR_ARG;
-  out->tile_rows = h->cfg.ty;
-  out->z_chunk = h->cfg.zchunk;
-  out->stages = h->cfg.stages;
+  const FusedConfig c = h->cfg_user_set ? h->cfg : default_cfg(h);
+  out->tile_rows = c.ty;
+  out->z_chunk = c.zchunk;
+  out->stages = c.stages;
   return WF_OK;
 }
 
