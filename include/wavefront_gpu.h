@@ -47,7 +47,8 @@ typedef enum {
   WF_ERR_TIMEOUT = 4,     /* a bounded device wait gave up (flag latched)    */
   WF_ERR_DEVICE_FLAG = 5, /* another device-side error flag was set          */
   WF_ERR_STATE = 6,       /* call not valid in the handle's current state    */
-  WF_ERR_UNSUPPORTED = 7  /* option not supported on this device/build       */
+  WF_ERR_UNSUPPORTED = 7, /* option not supported on this device/build       */
+  WF_ERR_IO = 8           /* a file could not be opened, read or written     */
 } wf_status;
 
 typedef enum { WF_BOUNDARY_ZERO = 0, WF_BOUNDARY_PERIODIC = 1 } wf_boundary;
@@ -183,15 +184,51 @@ wf_status wf_set_fields(wf_handle *h, const float *in6);
  * src/engine.rs:622-640): blocks (bz*nby+by)*nbx+bx, each ex..hz x 512. */
 wf_status wf_download_blocks(wf_handle *h, void *out);
 wf_status wf_upload_blocks(wf_handle *h, const void *in);
+
+/* ---- trajectory snapshots (src/engine.rs:617-640, 688-802) --------------- */
+
+/* A writer of the reference's wave_trajectory.bin: each capture appends the
+ * current state's FieldBlock bytes (wf_download_blocks' layout, nblocks *
+ * 12288 bytes, no header) at offset k * that size, the stream
+ * src/bin/wavefront-view.rs:280-305 reads.  The device reorders the state
+ * into a staging buffer, a copy stream moves it into one of two pinned host
+ * buffers, and a host thread writes that buffer to the file (O_DIRECT where
+ * the file system allows it) while the handle keeps stepping.  A capture
+ * waits only when both host buffers are still being written, the point at
+ * which src/engine.rs:784-802 stalls too; the next capture's reorder waits
+ * on the device for the previous copy out of the staging buffer.  Close the
+ * writer before destroying its handle. */
+typedef struct wf_snapshot_writer wf_snapshot_writer;
+wf_status wf_snapshot_open(wf_handle *h, const char *path, wf_snapshot_writer **out);
+wf_status wf_snapshot_capture(wf_snapshot_writer *w);
+/* Waits until every capture is in the file, closes it and frees the writer
+ * (also after an error); bytes_written (may be NULL) receives the bytes
+ * written.  Returns the first error of any capture's write. */
+wf_status wf_snapshot_close(wf_snapshot_writer *w, uint64_t *bytes_written);
+
+/* ---- checkpoint / resume (no reference counterpart) --------------------- */
+
+/* The complete stepping state in one file: the fields as stored (16-bit words
+ * and their shifts included), every CPML psi array, probe sums and traces,
+ * the step count and the binary16 saturation count, with the handle's
+ * configuration (dimensions, storage, arithmetic, boundaries, CPML
+ * thicknesses, source count, probe shapes) and a checksum.  Loading it into
+ * a handle configured the same way (materials, CPML, sources, probes)
+ * resumes the run bit for bit.  A configuration mismatch returns WF_ERR_ARG
+ * before anything is changed; a damaged payload returns WF_ERR_IO and leaves
+ * the handle's state undefined. */
+wf_status wf_checkpoint_save(wf_handle *h, const char *path);
+wf_status wf_checkpoint_load(wf_handle *h, const char *path);
 /* psi of the reference PmlAux array `which` (0..11 in the declaration order
  * of src/layout.rs:545-558), as an nz*ny*nx grid, zero where none is kept. */
 wf_status wf_get_psi(wf_handle *h, int which, float *out);
 /* Device pointers of the current six field arrays (FP32 precision only). */
 wf_status wf_device_fields(wf_handle *h, float **out6);
 /* 16-bit storage: the shifts the next step stores E and H with, per z slab
- * (nz/8 entries each; either may be NULL), and a saturation count: one per
- * step, slab and kind whose largest stored binary16 magnitude was 65504 (where
- * larger values saturate).  FP32 and bfloat16 storage report 0. */
+ * (nz/8 entries each; either may be NULL; a slab's E and H share one shift,
+ * so both arrays receive it), and a saturation count: one per step, slab and
+ * kind whose largest stored binary16 magnitude was 65504 (where larger
+ * values saturate).  FP32 and bfloat16 storage report 0. */
 wf_status wf_storage_info(wf_handle *h, int *shift_e, int *shift_h, uint64_t *overflows);
 
 /* The handle's CUDA stream (cudaStream_t) for event timing and interop. */

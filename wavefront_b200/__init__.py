@@ -14,7 +14,7 @@ from .source import FieldComponent, Source, Waveform, default_waveform
 from .probe import FrequencyResponse, Probe
 from .probe import FieldComponent as ProbeComponent
 from .scene import Scene, SceneError, demo_sphere
-from .engine import DeviceBatch, DeviceFieldGrid, EngineConfig, PSI_NAMES, run
+from .engine import DeviceBatch, DeviceFieldGrid, EngineConfig, PSI_NAMES, SnapshotWriter, run
 from ._lib import WfError, lib
 
 __all__ = [
@@ -22,5 +22,5 @@ __all__ = [
     "PmlConfig", "PmlContext", "PmlProfile1D", "effective_pml_thickness_blocks",
     "material_coeffs", "FieldComponent", "Source", "Waveform", "default_waveform",
     "FrequencyResponse", "Probe", "ProbeComponent", "Scene", "SceneError", "demo_sphere",
-    "DeviceBatch", "DeviceFieldGrid", "EngineConfig", "PSI_NAMES", "run", "WfError", "lib",
+    "DeviceBatch", "DeviceFieldGrid", "EngineConfig", "PSI_NAMES", "SnapshotWriter", "run", "WfError", "lib",
 ]

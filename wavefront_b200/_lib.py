@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libwavefront_gpu.so")
 
 WF_OK, WF_ERR_ARG, WF_ERR_CUDA, WF_ERR_OOM, WF_ERR_TIMEOUT, WF_ERR_DEVICE_FLAG, \
-    WF_ERR_STATE, WF_ERR_UNSUPPORTED = range(8)
+    WF_ERR_STATE, WF_ERR_UNSUPPORTED, WF_ERR_IO = range(9)
 
 # Every symbol include/wavefront_gpu.h declares (checked by tests).
 EXPORTS = [
@@ -27,6 +27,8 @@ EXPORTS = [
     "wf_nn_gelu_backward", "wf_nn_mse", "wf_nn_adam",
     "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
     "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
+    "wf_snapshot_open", "wf_snapshot_capture", "wf_snapshot_close",
+    "wf_checkpoint_save", "wf_checkpoint_load",
     "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
     "wf_material_coeffs", "wf_effective_pml_thickness_blocks", "wf_pml_profile",
     "wf_waveform_eval", "wf_source_values", "wf_probe_first_step", "wf_probe_tables",
@@ -95,6 +97,16 @@ def lib() -> C.CDLL:
         L.wf_steps_done.restype = C.c_int64
         L.wf_kernel_launches.argtypes = [_h]
         L.wf_kernel_launches.restype = C.c_int64
+        L.wf_snapshot_open.argtypes = [_h, C.c_char_p, C.POINTER(C.c_void_p)]
+        L.wf_snapshot_open.restype = S
+        L.wf_snapshot_capture.argtypes = [C.c_void_p]
+        L.wf_snapshot_capture.restype = S
+        L.wf_snapshot_close.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        L.wf_snapshot_close.restype = S
+        L.wf_checkpoint_save.argtypes = [_h, C.c_char_p]
+        L.wf_checkpoint_save.restype = S
+        L.wf_checkpoint_load.argtypes = [_h, C.c_char_p]
+        L.wf_checkpoint_load.restype = S
         L.wf_storage_info.argtypes = [_h, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_uint64)]
         L.wf_storage_info.restype = S

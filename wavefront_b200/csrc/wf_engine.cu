@@ -6,11 +6,19 @@
 // E everywhere, then every source in order, then every probe.
 #include <cudaTypedefs.h>
 
+#include <errno.h>
+#include <fcntl.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/wavefront_gpu.h"
@@ -605,6 +613,7 @@ const char *wf_status_string(wf_status s) {
     case WF_ERR_DEVICE_FLAG: return "device error flag";
     case WF_ERR_STATE: return "invalid state";
     case WF_ERR_UNSUPPORTED: return "unsupported";
+    case WF_ERR_IO: return "file I/O error";
   }
   return "unknown";
 }
@@ -1430,6 +1439,380 @@ wf_status wf_nn_mse(const float *y, const float *t, float *dy, float *loss, int6
 wf_status wf_nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, int64_t n,
                      float lr, float b1, float b2, float eps, int t, void *stream) {
   WF_CUDA(nullptr, static_cast<cudaError_t>(wf::nn_adam(w, w_bf16, g, m1, m2, n, lr, b1, b2, eps, t, stream)));
+  return WF_OK;
+}
+
+/* ---- trajectory snapshots ---------------------------------------------- */
+
+struct wf_snapshot_writer {
+  wf_handle *h = nullptr;
+  int fd = -1;
+  bool direct = false;
+  size_t bytes = 0;          // one snapshot
+  float *d_stage = nullptr;  // the state in FieldBlock order (FP32)
+  float *d_soa = nullptr;    // 16-bit storage: the decoded state
+  void *host[2] = {nullptr, nullptr};  // pinned
+  cudaStream_t copy = nullptr;
+  cudaEvent_t staged = nullptr, copied[2] = {nullptr, nullptr};
+  int last_slot = -1;  // slot of the latest copy out of d_stage
+  int next_slot = 0;
+  uint64_t offset = 0;   // file offset of the next capture
+  uint64_t written = 0;  // bytes the writer thread has written
+  std::thread thr;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::pair<int, uint64_t>> jobs;  // (slot, file offset)
+  bool busy[2] = {false, false};               // slot queued or being written
+  bool stop = false;
+  std::string err;  // first error of the writer thread
+};
+
+namespace {
+
+// pwrite of n bytes at off in chunks of at most 1 GiB (src/engine.rs:602 caps
+// a single O_DIRECT write the same way).  A file system that refuses
+// O_DIRECT at write time gets buffered writes from then on.
+std::string write_all(wf_snapshot_writer *w, const unsigned char *p, size_t n, uint64_t off) {
+  while (n > 0) {
+    const size_t len = std::min<size_t>(n, size_t(1) << 30);
+    const ssize_t r = pwrite(w->fd, p, len, static_cast<off_t>(off));
+    if (r < 0 && errno == EINTR) continue;
+    if (r < 0 && errno == EINVAL && w->direct) {
+      const int fl = fcntl(w->fd, F_GETFL);
+      if (fl >= 0 && fcntl(w->fd, F_SETFL, fl & ~O_DIRECT) == 0) {
+        w->direct = false;
+        continue;
+      }
+    }
+    if (r <= 0) return std::string("snapshot write failed: ") + std::strerror(r < 0 ? errno : EIO);
+    p += r;
+    n -= static_cast<size_t>(r);
+    off += static_cast<uint64_t>(r);
+  }
+  return std::string();
+}
+
+void snapshot_thread(wf_snapshot_writer *w) {
+  cudaSetDevice(w->h->dev);
+  for (;;) {
+    std::pair<int, uint64_t> job;
+    {
+      std::unique_lock<std::mutex> lk(w->mu);
+      w->cv.wait(lk, [w] { return w->stop || !w->jobs.empty(); });
+      if (w->jobs.empty()) return;
+      job = w->jobs.front();
+      w->jobs.pop_front();
+    }
+    const int s = job.first;
+    std::string why;
+    const cudaError_t e = cudaEventSynchronize(w->copied[s]);
+    if (e != cudaSuccess)
+      why = std::string("snapshot copy failed: ") + cudaGetErrorString(e);
+    else
+      why = write_all(w, static_cast<const unsigned char *>(w->host[s]), w->bytes, job.second);
+    {
+      std::lock_guard<std::mutex> lk(w->mu);
+      if (why.empty()) w->written += w->bytes;
+      if (!why.empty() && w->err.empty()) w->err = why;
+      w->busy[s] = false;
+    }
+    w->cv.notify_all();
+  }
+}
+
+// Frees everything a writer holds (the thread must have been joined).
+void snapshot_free(wf_snapshot_writer *w) {
+  for (void *p : w->host)
+    if (p) cudaFreeHost(p);
+  cudaFree(w->d_stage);
+  cudaFree(w->d_soa);
+  if (w->staged) cudaEventDestroy(w->staged);
+  for (cudaEvent_t e : w->copied)
+    if (e) cudaEventDestroy(e);
+  if (w->copy) cudaStreamDestroy(w->copy);
+  if (w->fd >= 0) close(w->fd);
+  delete w;
+}
+
+}  // namespace
+
+wf_status wf_snapshot_open(wf_handle *h, const char *path, wf_snapshot_writer **out) {
+  if (!h || !path || !out) return fail(h, WF_ERR_ARG, "null argument");
+  *out = nullptr;
+  DeviceGuard guard(h->dev);
+  wf_snapshot_writer *w = new wf_snapshot_writer;
+  w->h = h;
+  w->bytes = sizeof(float) * 6 * static_cast<size_t>(h->N);
+  w->fd = open(path, O_WRONLY | O_CREAT | O_TRUNC | O_DIRECT, 0644);
+  w->direct = w->fd >= 0;
+  if (w->fd < 0 && errno == EINVAL) w->fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+  if (w->fd < 0) {
+    const std::string why = std::string("cannot open ") + path + ": " + std::strerror(errno);
+    snapshot_free(w);
+    return fail(h, WF_ERR_IO, why);
+  }
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaHostAlloc(&w->host[i], w->bytes, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaMalloc(&w->d_stage, w->bytes);
+  if (e == cudaSuccess && store16(h)) e = cudaMalloc(&w->d_soa, w->bytes);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->copy, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w->staged, cudaEventDisableTiming);
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+    e = cudaEventCreateWithFlags(&w->copied[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    snapshot_free(w);
+    return cuda_fail(h, e, "snapshot writer setup");
+  }
+  w->thr = std::thread(snapshot_thread, w);
+  *out = w;
+  return WF_OK;
+}
+
+wf_status wf_snapshot_capture(wf_snapshot_writer *w) {
+  if (!w) return fail(nullptr, WF_ERR_ARG, "null writer");
+  wf_handle *h = w->h;
+  DeviceGuard guard(h->dev);
+  const int s = w->next_slot;
+  {
+    std::unique_lock<std::mutex> lk(w->mu);
+    w->cv.wait(lk, [w, s] { return !w->busy[s]; });  // the one stall point
+    if (!w->err.empty()) return fail(h, WF_ERR_IO, w->err);
+  }
+  // the staging buffer may still feed the previous copy
+  if (w->last_slot >= 0) WF_CUDA(h, cudaStreamWaitEvent(h->stream, w->copied[w->last_slot], 0));
+  const float *src = h->fld[h->cur];
+  if (store16(h)) {
+    WF_CUDA(h, wf::launch_decode_state(h->fld[h->cur], w->d_soa, h->precision, h->nx, h->ny, h->nz,
+                                       h->shift[h->cur], h->stream));
+    src = w->d_soa;
+  }
+  WF_CUDA(h, wf::launch_soa_to_blocks(src, w->d_stage, h->nx, h->ny, h->nz, h->stream));
+  WF_CUDA(h, cudaEventRecord(w->staged, h->stream));
+  WF_CUDA(h, cudaStreamWaitEvent(w->copy, w->staged, 0));
+  WF_CUDA(h, cudaMemcpyAsync(w->host[s], w->d_stage, w->bytes, cudaMemcpyDeviceToHost, w->copy));
+  WF_CUDA(h, cudaEventRecord(w->copied[s], w->copy));
+  w->last_slot = s;
+  {
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->busy[s] = true;
+    w->jobs.emplace_back(s, w->offset);
+  }
+  w->cv.notify_all();
+  w->offset += w->bytes;
+  w->next_slot ^= 1;
+  return WF_OK;
+}
+
+wf_status wf_snapshot_close(wf_snapshot_writer *w, uint64_t *bytes_written) {
+  if (!w) return fail(nullptr, WF_ERR_ARG, "null writer");
+  wf_handle *h = w->h;
+  DeviceGuard guard(h->dev);
+  {
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->stop = true;
+  }
+  w->cv.notify_all();
+  w->thr.join();  // the thread drains the queue before it returns
+  const std::string err = w->err;
+  if (bytes_written) *bytes_written = w->written;
+  snapshot_free(w);
+  return err.empty() ? WF_OK : fail(h, WF_ERR_IO, err);
+}
+
+/* ---- checkpoint / resume ------------------------------------------------ */
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'W', 'F', 'C', 'K', 'P', 'T', '\0', '\1'};
+constexpr uint32_t kCkptVersion = 1;
+
+// Fixed 256-byte header: the configuration the state belongs to.
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, header_bytes;
+  int32_t nx, ny, nz, precision, arith, periodic[3], T[3], nsrc, nprobe, nslab;
+  int64_t steps_done;
+  uint64_t ovf, payload_bytes, checksum;
+  unsigned char pad[256 - 8 - 8 - 4 * 14 - 8 * 4];
+};
+static_assert(sizeof(CkptHeader) == 256, "checkpoint header is 256 bytes");
+
+// 64-bit FNV-1a over 8-byte little-endian words (tail bytes one by one).
+struct Fnv64 {
+  uint64_t v = 1469598103934665603ull;
+  void add(const unsigned char *p, size_t n) {
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+      uint64_t w;
+      std::memcpy(&w, p + i, 8);
+      v = (v ^ w) * 1099511628211ull;
+    }
+    for (; i < n; ++i) v = (v ^ p[i]) * 1099511628211ull;
+  }
+};
+
+// One device region of the payload.
+struct CkptPiece {
+  void *dev;
+  size_t bytes;
+};
+
+// The shape records (sources, then probes) and the device regions of the
+// payload, in file order.
+void ckpt_layout(const wf_handle *h, std::vector<int32_t> *shape, std::vector<CkptPiece> *pieces) {
+  for (const SrcRec &s : h->srcs)
+    shape->insert(shape->end(), {s.d.x, s.d.y, s.d.z, s.d.comp, s.d.mode, s.d.nvals, 0, 0});
+  for (const ProbeRec &p : h->probes)
+    shape->insert(shape->end(), {p.d.x, p.d.y, p.d.z, p.d.comp, p.d.nfreq, p.d.nsteps,
+                                 p.d.first_step, p.d.record});
+  pieces->push_back({h->fld[h->cur], elem_bytes(h) * 6 * static_cast<size_t>(h->N)});
+  if (store16(h)) {
+    pieces->push_back({h->shift[h->cur], sizeof(int) * 2 * h->nslab});
+    pieces->push_back({h->shift[h->cur ^ 1], sizeof(int) * 2 * h->nslab});
+  }
+  for (const AxisState &A : h->ax)
+    if (A.T > 0) pieces->push_back({A.psi[h->cur], sizeof(float) * 4 * static_cast<size_t>(A.cells)});
+  for (const ProbeRec &p : h->probes) {
+    pieces->push_back({p.sc, sizeof(double) * 2 * p.d.nfreq});  // sc, then ss
+    pieces->push_back({p.n, sizeof(unsigned long long)});
+    if (p.d.record) pieces->push_back({p.trace, sizeof(float) * p.d.nsteps});
+  }
+}
+
+CkptHeader ckpt_header(const wf_handle *h, size_t shape_bytes, const std::vector<CkptPiece> &pieces) {
+  CkptHeader c;
+  std::memset(&c, 0, sizeof(c));
+  std::memcpy(c.magic, kCkptMagic, 8);
+  c.version = kCkptVersion;
+  c.header_bytes = sizeof(CkptHeader);
+  c.nx = h->nx;
+  c.ny = h->ny;
+  c.nz = h->nz;
+  c.precision = h->precision;
+  c.arith = h->arith;
+  for (int i = 0; i < 3; ++i) {
+    c.periodic[i] = h->periodic[i];
+    c.T[i] = h->ax[i].T;
+  }
+  c.nsrc = static_cast<int32_t>(h->srcs.size());
+  c.nprobe = static_cast<int32_t>(h->probes.size());
+  c.nslab = h->nslab;
+  c.steps_done = h->steps_done;
+  c.payload_bytes = shape_bytes;
+  for (const CkptPiece &p : pieces) c.payload_bytes += p.bytes;
+  return c;
+}
+
+struct File {
+  FILE *f = nullptr;
+  ~File() {
+    if (f) fclose(f);
+  }
+};
+
+struct PinnedBuf {
+  unsigned char *p = nullptr;
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+constexpr size_t kCkptChunk = size_t(64) << 20;
+
+}  // namespace
+
+wf_status wf_checkpoint_save(wf_handle *h, const char *path) {
+  if (!h || !path) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  wf_status st = wf_sync(h);
+  if (st != WF_OK) return st;
+  if (store16(h) && h->shifts_dirty) {  // the next step's shifts are part of the state
+    st = refresh_shifts(h);
+    if (st != WF_OK) return st;
+  }
+  unsigned long long ovf = 0;
+  if (store16(h)) WF_CUDA(h, cudaMemcpyAsync(&ovf, h->d_ovf, sizeof(ovf), cudaMemcpyDeviceToHost, h->stream));
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::vector<int32_t> shape;
+  std::vector<CkptPiece> pieces;
+  ckpt_layout(h, &shape, &pieces);
+  CkptHeader c = ckpt_header(h, sizeof(int32_t) * shape.size(), pieces);
+  c.ovf = ovf;
+  File f;
+  f.f = fopen(path, "wb");
+  if (!f.f) return fail(h, WF_ERR_IO, std::string("cannot open ") + path + ": " + std::strerror(errno));
+  PinnedBuf buf;
+  WF_CUDA(h, cudaHostAlloc(reinterpret_cast<void **>(&buf.p), kCkptChunk, cudaHostAllocDefault));
+  // header first (checksum filled in at the end), then the payload
+  Fnv64 sum;
+  bool ok = fwrite(&c, sizeof(c), 1, f.f) == 1;
+  const unsigned char *sp = reinterpret_cast<const unsigned char *>(shape.data());
+  sum.add(sp, sizeof(int32_t) * shape.size());
+  ok = ok && (shape.empty() || fwrite(sp, sizeof(int32_t), shape.size(), f.f) == shape.size());
+  for (const CkptPiece &p : pieces) {
+    for (size_t off = 0; ok && off < p.bytes; off += kCkptChunk) {
+      const size_t n = std::min(kCkptChunk, p.bytes - off);
+      WF_CUDA(h, cudaMemcpy(buf.p, static_cast<unsigned char *>(p.dev) + off, n, cudaMemcpyDeviceToHost));
+      sum.add(buf.p, n);
+      ok = fwrite(buf.p, 1, n, f.f) == n;
+    }
+  }
+  c.checksum = sum.v;
+  ok = ok && fseek(f.f, 0, SEEK_SET) == 0 && fwrite(&c, sizeof(c), 1, f.f) == 1;
+  ok = ok && fflush(f.f) == 0;
+  if (!ok) return fail(h, WF_ERR_IO, std::string("checkpoint write failed: ") + path);
+  return WF_OK;
+}
+
+wf_status wf_checkpoint_load(wf_handle *h, const char *path) {
+  if (!h || !path) return fail(h, WF_ERR_ARG, "null argument");
+  DeviceGuard guard(h->dev);
+  wf_status st = wf_sync(h);
+  if (st != WF_OK) return st;
+  File f;
+  f.f = fopen(path, "rb");
+  if (!f.f) return fail(h, WF_ERR_IO, std::string("cannot open ") + path + ": " + std::strerror(errno));
+  CkptHeader c;
+  if (fread(&c, sizeof(c), 1, f.f) != 1 || std::memcmp(c.magic, kCkptMagic, 8) != 0 ||
+      c.version != kCkptVersion || c.header_bytes != sizeof(CkptHeader))
+    return fail(h, WF_ERR_IO, "not a checkpoint of this library version");
+  std::vector<int32_t> shape;
+  std::vector<CkptPiece> pieces;
+  ckpt_layout(h, &shape, &pieces);
+  const CkptHeader mine = ckpt_header(h, sizeof(int32_t) * shape.size(), pieces);
+  const bool same = c.nx == mine.nx && c.ny == mine.ny && c.nz == mine.nz &&
+                    c.precision == mine.precision && c.arith == mine.arith &&
+                    std::equal(c.periodic, c.periodic + 3, mine.periodic) &&
+                    std::equal(c.T, c.T + 3, mine.T) && c.nsrc == mine.nsrc &&
+                    c.nprobe == mine.nprobe && c.nslab == mine.nslab &&
+                    c.payload_bytes == mine.payload_bytes;
+  if (!same) return fail(h, WF_ERR_ARG, "checkpoint of a differently configured grid");
+  std::vector<int32_t> file_shape(shape.size());
+  if (!shape.empty() && fread(file_shape.data(), sizeof(int32_t), shape.size(), f.f) != shape.size())
+    return fail(h, WF_ERR_IO, "checkpoint truncated");
+  if (file_shape != shape) return fail(h, WF_ERR_ARG, "checkpoint sources or probes differ");
+  Fnv64 sum;
+  sum.add(reinterpret_cast<const unsigned char *>(file_shape.data()), sizeof(int32_t) * shape.size());
+  PinnedBuf buf;
+  WF_CUDA(h, cudaHostAlloc(reinterpret_cast<void **>(&buf.p), kCkptChunk, cudaHostAllocDefault));
+  for (const CkptPiece &p : pieces) {
+    for (size_t off = 0; off < p.bytes; off += kCkptChunk) {
+      const size_t n = std::min(kCkptChunk, p.bytes - off);
+      if (fread(buf.p, 1, n, f.f) != n) return fail(h, WF_ERR_IO, "checkpoint truncated");
+      sum.add(buf.p, n);
+      WF_CUDA(h, cudaMemcpy(static_cast<unsigned char *>(p.dev) + off, buf.p, n, cudaMemcpyHostToDevice));
+    }
+  }
+  if (sum.v != c.checksum) return fail(h, WF_ERR_IO, "checkpoint checksum mismatch");
+  h->steps_done = c.steps_done;
+  const long long step = c.steps_done;
+  WF_CUDA(h, cudaMemcpy(h->d_step, &step, sizeof(step), cudaMemcpyHostToDevice));
+  if (store16(h)) {
+    const unsigned long long ovf = c.ovf;
+    WF_CUDA(h, cudaMemcpy(h->d_ovf, &ovf, sizeof(ovf), cudaMemcpyHostToDevice));
+    WF_CUDA(h, cudaMemset(h->slab_max, 0, sizeof(unsigned) * 2 * h->nslab));
+    h->shifts_dirty = false;
+  }
   return WF_OK;
 }
 

@@ -10,6 +10,7 @@ reference's FieldBlock byte order (the host writer stays with the caller).
 from __future__ import annotations
 
 import ctypes as C
+import os
 import time
 from dataclasses import dataclass
 from typing import Callable, Optional, Sequence
@@ -247,14 +248,71 @@ class DeviceFieldGrid:
         self._chk(_L.lib().wf_device_fields(self._h, arr))
         return [int(v) for v in arr]
 
+    # -- checkpoint / resume ----------------------------------------------------
+    def checkpoint(self, path) -> None:
+        """Saves the complete stepping state (wf_checkpoint_save)."""
+        self._chk(_L.lib().wf_checkpoint_save(self._h, os.fsencode(path)))
+
+    def restore(self, path) -> None:
+        """Loads a checkpoint into this grid, which must be configured like the
+        one that saved it (wf_checkpoint_load); the run then continues bit for
+        bit."""
+        self._chk(_L.lib().wf_checkpoint_load(self._h, os.fsencode(path)))
+
+    def snapshot_writer(self, path) -> "SnapshotWriter":
+        return SnapshotWriter(self, path)
+
+
+class SnapshotWriter:
+    """wave_trajectory.bin writer (src/engine.rs:688-802): each capture()
+    appends the current state's FieldBlock bytes; the device-to-host copy and
+    the file write overlap the following steps.  Use as a context manager or
+    call close()."""
+
+    def __init__(self, grid: DeviceFieldGrid, path):
+        self._grid = grid
+        self._w = C.c_void_p()
+        grid._chk(_L.lib().wf_snapshot_open(grid._h, os.fsencode(path), C.byref(self._w)))
+        self.captures = 0
+
+    def capture(self) -> None:
+        self._grid._chk(_L.lib().wf_snapshot_capture(self._w))
+        self.captures += 1
+
+    def close(self) -> int:
+        """Waits for every capture to reach the file; returns the bytes written."""
+        if not self._w:
+            return 0
+        n = C.c_uint64()
+        st = _L.lib().wf_snapshot_close(self._w, C.byref(n))
+        self._w = C.c_void_p()
+        self._grid._chk(st)
+        return int(n.value)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 @dataclass
 class EngineConfig:
-    """src/engine.rs:608-615 (output_path is the caller's snapshot sink)."""
+    """src/engine.rs:608-615.  With snapshot_every > 0 a snapshot is taken
+    after every step whose index is a multiple of it: output_path receives
+    them as wave_trajectory.bin through the pinned double-buffered writer,
+    and snapshot_sink (if given) receives (step, FieldBlock floats)."""
     num_steps: int
     dt: float
     snapshot_every: int = 0
     snapshot_sink: Optional[Callable[[int, np.ndarray], None]] = None
+    output_path: Optional[str] = None
 
 
 def run(grid: DeviceFieldGrid, sources: Sequence, probes: Sequence, config: EngineConfig,
@@ -271,7 +329,9 @@ def run(grid: DeviceFieldGrid, sources: Sequence, probes: Sequence, config: Engi
                               p.record_trace)
     grid.sync()
     t0 = time.perf_counter()
-    every = max(config.snapshot_every, 1) if config.snapshot_sink else 0
+    snap = config.snapshot_sink is not None or config.output_path is not None
+    every = max(config.snapshot_every, 1) if snap else 0
+    writer = grid.snapshot_writer(config.output_path) if config.output_path is not None else None
     done = 0
     while done < n:
         if every:
@@ -283,7 +343,12 @@ def run(grid: DeviceFieldGrid, sources: Sequence, probes: Sequence, config: Engi
         grid.step(chunk)
         done += chunk
         if every and (done - 1) % every == 0:
-            config.snapshot_sink(done - 1, grid.download_blocks())
+            if writer is not None:
+                writer.capture()
+            if config.snapshot_sink is not None:
+                config.snapshot_sink(done - 1, grid.download_blocks())
+    if writer is not None:
+        writer.close()
     grid.sync()
     wall = time.perf_counter() - t0
     for i, p in enumerate(probes):
