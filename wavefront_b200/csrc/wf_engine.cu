@@ -195,9 +195,11 @@ bool encode(CUtensorMap *m, CUtensorMapDataType t, int rank, void *base, const c
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Tiling used unless the caller set one (best measured at 512^3 on B200).
+// Tiling used unless the caller set one (best measured at 512^3 and 1024^3 on
+// B200, for every storage type).
 FusedConfig default_cfg(const wf_handle *h) {
-  return store16(h) ? FusedConfig{4, 12, 4} : FusedConfig{4, 12, 3};
+  (void)h;
+  return FusedConfig{4, 12, 3};
 }
 
 // TMA descriptors per state buffer: fields as a 4D tensor {nx, ny, nz, 6},
@@ -1998,7 +2000,7 @@ wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int tys[] = {4, 8, 16}, stg[] = {3, 4}, zcs[] = {8, 16, 32, 64, 128};
+  const int tys[] = {4, 8, 16}, stg[] = {3, 4}, zcs[] = {8, 12, 16, 24, 32, 64, 128};
   for (int ty : tys)
     for (int sg : stg)
       for (int zc : zcs) {

@@ -685,14 +685,18 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
 // code, lean registers) and one instantiation per combination, so that each
 // item runs only the psi code of its own axes.  The host lists each class's
 // items (tile x, tile y, z chunk); the launches partition the grid.
-// Three CTAs per SM at 4 tile rows, except for items on two or three CPML
+// CTAs per SM at 4 tile rows: three, except for items on two or three CPML
 // axes, whose psi registers (prefetched H terms, in-flight E terms) need
-// more than a third of the register file: two CTAs there, without spills.
+// more than a third of the register file (two there, without spills), and
+// the 16-bit interior, which fits 96 registers without spills and gains
+// from a fourth CTA (its shared memory allows four at 3 stages).
 template <int AX>
 constexpr int kMultiAxis = (AX & (AX - 1)) != 0;
+template <int AX, typename ST>
+constexpr int kCtasPerSm4 = kMultiAxis<AX> ? 2 : (sizeof(ST) == 2 && AX == 0 ? 4 : 3);
 
 template <int TY, int S, bool FMA, int AX, typename ST>
-__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? (kMultiAxis<AX> ? 2 : 3) : 1)
+__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, ST> : 1)
     k_fused(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
             const __grid_constant__ CUtensorMap tmM, const FusedArgs a, const int *items) {
   using L = Layout<TY, S, ST>;
