@@ -118,26 +118,35 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(sc, seconds=15.0):
+def cpu_baseline(sc, seconds=15.0, seconds_one_core=6.0):
     """The oracle (C restatement of the reference, AVX2 rows, one worker
     thread per host core splitting each phase into contiguous block ranges
     like the reference's rayon Z-slabs) on a bounded sample: as many full
-    512^3 steps as fit in about `seconds`."""
+    steps of the workload as fit in about `seconds`; then the same on one
+    core for about `seconds_one_core`."""
     from oracle import oracle as O
     nt = os.cpu_count() or 1
-    sim = O.sim_from_scenario(sc, steps=64)
+    sim = O.sim_from_scenario(sc, steps=128)
+
+    def timed(threads, budget):
+        t0 = time.perf_counter()
+        n = 0
+        while n < 64:
+            sim.step(1, threads)
+            n += 1
+            if time.perf_counter() - t0 > budget:
+                break
+        return n, time.perf_counter() - t0
+
     sim.step(1, nt)  # warm-up (page-in)
-    t0 = time.perf_counter()
-    n = 0
-    while n < 64:
-        sim.step(1, nt)
-        n += 1
-        if time.perf_counter() - t0 > seconds:
-            break
-    el = time.perf_counter() - t0
+    n, el = timed(nt, seconds)
+    n1, el1 = timed(1, seconds_one_core)
     sim.close()
-    return {"value": round(sc.dims.voxel_count() * n / el / 1e6, 2), "unit": METRIC, "cores": nt,
-            "kind": "port", "sample": f"{n} full {GRID}^3 steps after 1 warm-up step, {el:.1f} s"}
+    cells = sc.dims.voxel_count()
+    return {"value": round(cells * n / el / 1e6, 2), "unit": METRIC, "cores": nt,
+            "kind": "port", "sample": f"{n} full {GRID}^3 steps after 1 warm-up step, {el:.1f} s",
+            "one_core": {"value": round(cells * n1 / el1 / 1e6, 2), "unit": METRIC,
+                         "sample": f"the next {n1} steps on 1 thread, {el1:.1f} s"}}
 
 
 def scenario(args, steps, device_voxelize=None):
@@ -147,7 +156,19 @@ def scenario(args, steps, device_voxelize=None):
     if args.workload == "random_spheres":
         dv = GRID > 256 if device_voxelize is None else device_voxelize
         return configs.random_spheres(n=GRID, steps=steps, device_voxelize=dv)
+    if args.workload == "demo_sphere":
+        return configs.demo_sphere_cube(n=GRID, steps=steps)
     return configs.two_spheres(n=GRID, steps=steps)
+
+
+def scene_config(sc, precision=None) -> dict:
+    """The workload keys both arms report (the reference arm stores FP32)."""
+    p = precision or PRECISION
+    return {"workload": WORKLOAD, "grid": [GRID] * 3,
+            "cpml_cells": sc.pml.thickness_voxels[0] if sc.pml is not None else 0,
+            "probes": len(sc.probes), "storage": p,
+            "l2": f"inputs larger than L2 ({N_CELLS * 6 * ELEM[p] / 1e9:.1f} GB of fields "
+                  "per state buffer)"}
 
 
 def run_reference(args, rank, world):
@@ -158,7 +179,7 @@ def run_reference(args, rank, world):
     nt = os.cpu_count() or 1
     sim = O.sim_from_scenario(sc, steps=args.warmup + args.steps)
     budget = float(os.environ.get("WF_REF_SECONDS", "120"))
-    for _ in range(min(args.warmup, 1)):
+    for _ in range(args.warmup):
         sim.step(1, nt)
     t0 = time.perf_counter()
     n = 0
@@ -172,11 +193,9 @@ def run_reference(args, rank, world):
     v = N_CELLS * n / el / 1e6
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": METRIC,
-        "n_gpus": world, "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": round(el / n * 1e3, 3),
+        "n_gpus": world, "steps": n, "warmup": args.warmup, "ms_per_step": round(el / n * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "grid": [GRID] * 3,
-                                        "l2": f"inputs larger than L2 ({N_CELLS * 24 / 1e9:.1f} GB "
-                                              "of fields)"},
+        "data": "synthetic", "config": scene_config(sc, "f32"),
         "cpu_baseline": {"value": round(v, 2), "unit": METRIC, "cores": nt, "kind": "port",
                          "sample": f"{n} of {args.steps} requested {GRID}^3 steps in {el:.1f} s "
                                    "(time-bounded); the Rust reference cannot be built here, so "
@@ -475,13 +494,19 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g = build()
+        g.sync()
+        t_built = time.perf_counter()
         g.step(args.steps)
         g.sync()
+        t_stepped = time.perf_counter()
         sums = [g.probe_sums(i, 1) for i in range(len(sc.probes))]
         import ctypes as C
         from wavefront_b200 import _lib as L
         L.check(L.lib().wf_download_blocks(g._h, C.c_void_p(snap.data_ptr())), g._h)
         e2e_s = time.perf_counter() - t0
+        phases = {"create_and_upload": round((t_built - t0) * 1e3, 1),
+                  "steps": round((t_stepped - t_built) * 1e3, 1),
+                  "probe_sums_and_snapshot": round((t0 + e2e_s - t_stepped) * 1e3, 1)}
         g.close()
         if dist:
             t = torch.tensor([e2e_s], device="cuda")
@@ -495,7 +520,8 @@ def run_ours(args, rank, world, local_rank):
                     "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h / args.steps),
                     "includes": "handle creation, scene + table upload, K steps, probe sums, "
-                                "one FieldBlock snapshot download (pinned host buffers)"}
+                                "one FieldBlock snapshot download (pinned host buffers)",
+                    "phases_ms": phases}
 
     if rank == 0:
         line = {
@@ -503,13 +529,9 @@ def run_ours(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [GRID] * 3, "cpml_cells": 16,
-                       "probes": 8, "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
+            "config": {**scene_config(sc), "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
                        "tiling": {"tile_rows": tiling[0], "z_chunk": tiling[1],
                                   "stages": tiling[2]},
-                       "storage": PRECISION,
-                       "l2": f"inputs larger than L2 ({N_CELLS * 6 * ELEM[PRECISION] / 1e9:.1f} GB "
-                             "of fields per state buffer)",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": e2e_line,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -539,12 +561,15 @@ def main():
     ap.add_argument("--grid", type=int, default=0,
                     help="cube edge (default 512 for two_spheres, 1024 for random_spheres)")
     ap.add_argument("--workload", default="two_spheres",
-                    choices=["two_spheres", "random_spheres", "batched", "closure"])
+                    choices=["two_spheres", "random_spheres", "batched", "closure", "demo_sphere"],
+                    help="two_spheres: the 512^3 headline; random_spheres: the mixed-precision "
+                         "scene; demo_sphere: the reference's own benchmark shape (256^3 demo "
+                         "sphere, 8-cell CPML)")
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
                     help="field storage (16-bit: per-slab power-of-two scales, FP32 math)")
     args = ap.parse_args()
     global GRID, N_CELLS, WORKLOAD, PRECISION
-    GRID = args.grid or (1024 if args.workload == "random_spheres" else 512)
+    GRID = args.grid or {"random_spheres": 1024, "demo_sphere": 256}.get(args.workload, 512)
     N_CELLS = GRID ** 3
     PRECISION = args.precision
     if args.workload == "batched":
@@ -553,6 +578,8 @@ def main():
         WORKLOAD = "learned_closure_224^3_interior_thin4_vs_cpml16_ricker"
     elif args.workload == "random_spheres":
         WORKLOAD = f"random_spheres_{GRID}^3_{PRECISION}_storage_cpml16_sinusoid_8probes"
+    elif args.workload == "demo_sphere":
+        WORKLOAD = f"demo_sphere_{GRID}^3_{PRECISION}_storage_cpml8_ricker"
     elif PRECISION == "f32":
         WORKLOAD = f"two_spheres_{GRID}^3_fp32_cpml16_gaussian_8probes"
     else:
