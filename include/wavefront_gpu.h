@@ -240,6 +240,15 @@ wf_status wf_get_stream(wf_handle *h, void **out_stream);
  * since timing was enabled. */
 wf_status wf_set_timing(wf_handle *h, int enable);
 wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches);
+/* Testing aid for the device timeout path (no reference counterpart): while
+ * extra_bytes > 0, every fused step kernel's CTAs expect extra_bytes more on
+ * their first TMA stage than its copies deliver.  The copies land, the
+ * stage's phase never completes, its bounded wait gives up after about a
+ * second, and the CTA latches the timeout flag, drains its other copies and
+ * exits; the next wf_sync returns WF_ERR_TIMEOUT.  No fault and no hang: the
+ * GPU context stays usable for other handles.  0 (the default) turns it off;
+ * the split kernels have no TMA stages and ignore it. */
+wf_status wf_set_test_stall(wf_handle *h, int extra_bytes);
 /* Device kernels this handle has launched for steps so far (step kernels of
  * every work class plus the source/probe tail), graph replays included. */
 int64_t wf_kernel_launches(const wf_handle *h);

@@ -100,6 +100,7 @@ struct wf_handle {
   long long kernel_launches = 0;       // step + tail kernels issued so far
   long long graph_kernels[2] = {0, 0};  // kernels in one replay of graph[parity]
   FusedConfig cfg{4, 12, 3};
+  int test_extra_tx = 0;      // wf_set_test_stall
   bool cfg_user_set = false;  // otherwise chosen from the grid at first use
   wf::FusedMaps maps[2];      // per state buffer (the one read by the step)
   int *d_items = nullptr;     // work items grouped by kernel class
@@ -356,6 +357,7 @@ FusedArgs fused_args(const wf_handle *h) {
   a.zchunk = h->cfg.zchunk;
   a.has_pml = has_pml(h) ? 1 : 0;
   a.prof_in_smem = (h->ax[0].W <= 64 && h->ax[1].W <= 64 && h->ax[2].W <= 64) ? 1 : 0;
+  a.test_extra_tx = h->test_extra_tx;
   return a;
 }
 
@@ -1228,6 +1230,14 @@ wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches) {
   }
   *total_ms = tot;
   *launches = static_cast<int64_t>(h->ev_used / 2);
+  return WF_OK;
+}
+
+wf_status wf_set_test_stall(wf_handle *h, int extra_bytes) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  if (extra_bytes < 0 || extra_bytes > 65536) return fail(h, WF_ERR_ARG, "extra_bytes outside [0, 65536]");
+  drop_graphs(h);  // captured launches hold the old arguments
+  h->test_extra_tx = extra_bytes;
   return WF_OK;
 }
 

@@ -258,7 +258,10 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     unsigned char *st = s_stage + slot * L::STAGE;
     const uint32_t bar = smem_u32(&s_bar[slot]);
     const bool e_only = (p == k1);
-    mbar_expect_tx(bar, e_only ? L::E_BYTES : (L::E_BYTES + L::H_BYTES + L::M_BYTES));
+    // (a nonzero test_extra_tx leaves stage 0's phase incomplete after its
+    // copies land, so its bounded wait runs out: the timeout path, tested)
+    mbar_expect_tx(bar, (e_only ? L::E_BYTES : (L::E_BYTES + L::H_BYTES + L::M_BYTES)) +
+                            (j == 0 ? static_cast<uint32_t>(a.test_extra_tx) : 0u));
     tma_load_4d(smem_u32(st), tmE, x0 - PAD, y0 - 1, p, 0, bar);
     if (!e_only) {
       tma_load_4d(smem_u32(st + L::H_OFF), tmH, x0 - PAD, y0 - 1, p, 3, bar);

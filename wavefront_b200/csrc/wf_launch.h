@@ -33,6 +33,7 @@ struct FusedArgs {
   int tiles_x, tiles_y, zchunk;
   int has_pml;
   int prof_in_smem;  // every CPML axis has at most 64 slab positions
+  int test_extra_tx;  // testing aid: bytes stage 0 expects beyond its copies (0 normally)
 };
 
 // Tiling of the fused kernel: TY rows per CTA (x width kTileX), z chunk and

@@ -248,6 +248,12 @@ class DeviceFieldGrid:
         self._chk(_L.lib().wf_device_fields(self._h, arr))
         return [int(v) for v in arr]
 
+    def set_test_stall(self, extra_bytes: int) -> None:
+        """Testing aid (wf_set_test_stall): makes every fused step's first TMA
+        stage wait run out, so the step reports WF_ERR_TIMEOUT at the next
+        sync; 0 turns it off."""
+        self._chk(_L.lib().wf_set_test_stall(self._h, int(extra_bytes)))
+
     # -- checkpoint / resume ----------------------------------------------------
     def checkpoint(self, path) -> None:
         """Saves the complete stepping state (wf_checkpoint_save)."""
