@@ -72,6 +72,92 @@ __global__ void k_conv_fwd(const float *in, const __nv_bfloat16 *w, const int *f
   }
 }
 
+// The same convolution for the network's output-channel counts (CO = 16, 6),
+// blocked for the FMA pipes: a thread computes 4 consecutive voxels of one
+// row from 6 staged inputs per (channel, dz, dy), and the weights sit in
+// shared memory output-channel fastest ([ci][27][CP], CP = CO rounded up to
+// 4, zero padded) so that 128-bit loads feed CO FMAs for each of the 4
+// voxels.  Every voxel still sums channel by channel and tap by tap in the
+// order of k_conv_fwd, skipping the same out-of-range taps, so the results
+// are identical.
+template <int CO>
+__global__ void __launch_bounds__(128) k_conv_fwd4(const float *in, const __nv_bfloat16 *w,
+                                                   const int *face, float *z, float *a, int n,
+                                                   int ci, int D, int H, int W, int act) {
+  constexpr int CP = (CO + 3) / 4 * 4;
+  extern __shared__ float s_w[];  // [ci][27][CP] of the block's sample
+  const int s = blockIdx.y;
+  const int f = face ? face[s] : 0;
+  const int nw = ci * kTaps * CP;
+  for (int i = threadIdx.x; i < nw; i += blockDim.x) {
+    const int o = i % CP, ct = i / CP;  // ct = c * 27 + t
+    const int c = ct / kTaps, t = ct % kTaps;
+    s_w[i] = o < CO ? __bfloat162float(w[((static_cast<long long>(f) * CO + o) * ci + c) * kTaps + t])
+                    : 0.0f;
+  }
+  __syncthreads();
+  const int QW = (W + 3) / 4;
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= static_cast<long long>(D) * H * QW || s >= n) return;
+  const int x0 = static_cast<int>(q % QW) * 4, y = static_cast<int>((q / QW) % H),
+            d = static_cast<int>(q / (static_cast<long long>(QW) * H));
+  bool ok[6];  // input column x0 - 1 + k inside the row
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ok[k] = x0 - 1 + k >= 0 && x0 - 1 + k < W;
+  float acc[4][CO];
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+#pragma unroll
+    for (int o = 0; o < CO; ++o) acc[v][o] = 0.0f;
+  const long long P = static_cast<long long>(D) * H * W;
+  const float *src = in + static_cast<long long>(s) * ci * P;
+  for (int c = 0; c < ci; ++c) {
+    const float *sc = src + c * P;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int dd = d + dz;
+      if (dd < 0 || dd >= D) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int yy = y + dy;
+        if (yy < 0 || yy >= H) continue;
+        const float *row = sc + (static_cast<long long>(dd) * H + yy) * W + x0 - 1;
+        float r[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) r[k] = ok[k] ? __ldg(row + k) : 0.0f;
+        const float *wt = s_w + (c * kTaps + (dz + 1) * 9 + (dy + 1) * 3) * CP;
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+          float wv[CP];
+#pragma unroll
+          for (int o4 = 0; o4 < CP / 4; ++o4) {
+            const float4 w4 = *reinterpret_cast<const float4 *>(wt + dx * CP + 4 * o4);
+            wv[4 * o4] = w4.x;
+            wv[4 * o4 + 1] = w4.y;
+            wv[4 * o4 + 2] = w4.z;
+            wv[4 * o4 + 3] = w4.w;
+          }
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            if (!ok[v + dx]) continue;  // the tap k_conv_fwd skips
+#pragma unroll
+            for (int o = 0; o < CO; ++o) acc[v][o] = __fmaf_rn(wv[o], r[v + dx], acc[v][o]);
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    if (x0 + v >= W) break;
+    const long long p = (static_cast<long long>(d) * H + y) * W + x0 + v;
+#pragma unroll
+    for (int o = 0; o < CO; ++o) {
+      const long long k = (static_cast<long long>(s) * CO + o) * P + p;
+      if (z) z[k] = acc[v][o];
+      a[k] = act ? gelu(acc[v][o]) : acc[v][o];
+    }
+  }
+}
+
 // din[n][ci][p] = sum_co sum_tap w[co][ci][tap] * dz[n][co][p - tap]
 __global__ void k_conv_bwd_data(const float *dz, const __nv_bfloat16 *w, const int *face, float *din,
                                 int n, int ci, int co, int D, int H, int W) {
@@ -296,9 +382,21 @@ int nn_conv_fwd(const float *in, const void *w_bf16, const int *face, float *z, 
                 int ci, int co, int D, int H, int W, int act, void *stream) {
   if (ci > kMaxC || co > kMaxC || ci < 1 || co < 1 || n < 1) return cudaErrorInvalidValue;
   const long long P = static_cast<long long>(D) * H * W;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const __nv_bfloat16 *wb = static_cast<const __nv_bfloat16 *>(w_bf16);
+  if (co == 16 || co == 6) {  // the network's layers: the blocked kernel
+    const long long quads = static_cast<long long>(D) * H * ((W + 3) / 4);
+    dim3 grid(blocks_for(quads, 128), n);
+    const size_t sm = sizeof(float) * ci * kTaps * (co == 16 ? 16 : 8);
+    if (co == 16)
+      k_conv_fwd4<16><<<grid, 128, sm, st>>>(in, wb, face, z, a, n, ci, D, H, W, act);
+    else
+      k_conv_fwd4<6><<<grid, 128, sm, st>>>(in, wb, face, z, a, n, ci, D, H, W, act);
+    return cudaGetLastError();
+  }
   dim3 grid(blocks_for(P, 128), n);
-  k_conv_fwd<<<grid, 128, sizeof(float) * co * ci * kTaps, static_cast<cudaStream_t>(stream)>>>(
-      in, static_cast<const __nv_bfloat16 *>(w_bf16), face, z, a, n, ci, co, D, H, W, act);
+  k_conv_fwd<<<grid, 128, sizeof(float) * co * ci * kTaps, st>>>(in, wb, face, z, a, n, ci, co, D,
+                                                                  H, W, act);
   return cudaGetLastError();
 }
 
