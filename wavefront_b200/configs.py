@@ -183,7 +183,12 @@ def device_batch(scenes: List[Scenario], steps: Optional[int] = None, device: in
     """A DeviceBatch with every scenario's materials, CPML, source values and
     probe tables loaded (tables for `steps` steps, default each scenario's)."""
     from .engine import DeviceBatch
-    b = DeviceBatch([sc.dims for sc in scenes], device=device)
+    return load_batch(DeviceBatch([sc.dims for sc in scenes], device=device), scenes, steps)
+
+
+def load_batch(b, scenes: List[Scenario], steps: Optional[int] = None):
+    """Loads every scenario's materials, CPML, source values and probe tables
+    into the grids of an allocated DeviceBatch; returns it."""
     for g, sc in zip(b.grids, scenes):
         n = sc.steps if steps is None else steps
         g.set_materials(sc.grid, sc.table)
