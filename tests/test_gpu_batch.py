@@ -44,7 +44,9 @@ def test_batch_matches_oracle_through_graph_replays(oracle):
     try:
         b.step(70)
         b.sync()
-        assert b.kernel_launches == 2 * 70
+        # per step: one persistent launch per non-empty CPML class, then the tail
+        per_step, rest = divmod(b.kernel_launches, 70)
+        assert rest == 0 and 2 <= per_step <= 9, b.kernel_launches
         _check_against_oracle(oracle, b, scenes, 70)
     finally:
         b.close()

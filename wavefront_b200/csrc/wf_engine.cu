@@ -502,14 +502,20 @@ struct wf_batch {
   std::vector<wf_handle *> h;
   FusedConfig cfg{4, 16, 3};
   wf::BatchScene *d_scenes = nullptr;
-  int2 *d_items = nullptr;
+  int2 *d_items = nullptr;  // grouped by CPML class
   int n_items = 0;
-  int *d_counter = nullptr;
+  int class_off[wf::kFusedClassCount] = {}, class_n[wf::kFusedClassCount] = {};
+  int class_ctas[wf::kFusedClassCount] = {};
+  int step_kernels = 0;    // non-empty classes: step-kernel launches per step
+  int *d_counter = nullptr;  // one work counter per class
+  // the class launches of a step run concurrently: forked from `stream` onto
+  // these and joined back before the tail
+  cudaStream_t side[wf::kFusedClassCount - 1] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[wf::kFusedClassCount - 1] = {};
   TailArgs *d_tails[2] = {nullptr, nullptr};  // per parity of the state read
   bool have_tail = false;
   std::vector<long long> versions;  // handle versions the tables were built from
   bool built = false;
-  int ctas = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   long long launches = 0;
 };
@@ -539,7 +545,7 @@ wf_status batch_build(wf_batch *b) {
   batch_drop(b);
   const size_t n = b->h.size();
   std::vector<wf::BatchScene> scenes(n);
-  std::vector<int2> items;
+  std::vector<int2> lists[wf::kFusedClassCount];
   std::vector<TailArgs> tails[2];
   b->have_tail = false;
   for (size_t i = 0; i < n; ++i) {
@@ -564,7 +570,16 @@ wf_status batch_build(wf_batch *b) {
     if (!h->srcs.empty() || !h->probes.empty()) b->have_tail = true;
     const FusedArgs &a = scenes[i].args[0];
     const int nit = a.tiles_x * a.tiles_y * ((h->nz + a.zchunk - 1) / a.zchunk);
-    for (int k = 0; k < nit; ++k) items.push_back(make_int2(static_cast<int>(i), k));
+    for (int k = 0; k < nit; ++k)
+      lists[wf::fused_item_class(a, b->cfg.ty, k)].push_back(make_int2(static_cast<int>(i), k));
+  }
+  std::vector<int2> items;
+  b->step_kernels = 0;
+  for (int k = 0; k < wf::kFusedClassCount; ++k) {
+    b->class_off[k] = static_cast<int>(items.size());
+    b->class_n[k] = static_cast<int>(lists[k].size());
+    if (b->class_n[k]) ++b->step_kernels;
+    items.insert(items.end(), lists[k].begin(), lists[k].end());
   }
   WF_CUDA(nullptr, cudaMalloc(&b->d_scenes, sizeof(wf::BatchScene) * n));
   WF_CUDA(nullptr, cudaMemcpy(b->d_scenes, scenes.data(), sizeof(wf::BatchScene) * n,
@@ -581,19 +596,34 @@ wf_status batch_build(wf_batch *b) {
   WF_CUDA(nullptr, wf::fused_batch_prepare(b->cfg));
   int sms = 0;
   WF_CUDA(nullptr, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev));
-  const int per_sm = std::max(1, wf::fused_batch_ctas_per_sm(b->cfg));
-  b->ctas = std::max(1, std::min(sms * per_sm, b->n_items));
+  for (int k = 0; k < wf::kFusedClassCount; ++k) {
+    const int per_sm = std::max(1, wf::fused_batch_ctas_per_sm(b->cfg, k));
+    b->class_ctas[k] = std::max(1, std::min(sms * per_sm, b->class_n[k]));
+  }
   b->versions.clear();
   for (wf_handle *h : b->h) b->versions.push_back(h->version);
   b->built = true;
   return WF_OK;
 }
 
-// The batched step kernel alone (reads parity `cur`).
+// The batched step kernels alone (read parity `cur`): one persistent launch
+// per non-empty class, class 0 on the batch's stream and the others on side
+// streams forked from it and joined back; the classes write disjoint cells.
 wf_status batch_kernel(wf_batch *b, int cur) {
-  WF_CUDA(nullptr, cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
-  WF_CUDA(nullptr, wf::launch_fused_batch(b->cfg, b->d_scenes, b->d_items, b->n_items,
-                                          b->d_counter, cur, b->ctas, b->stream));
+  WF_CUDA(nullptr, cudaMemsetAsync(b->d_counter, 0, sizeof(int) * wf::kFusedClassCount, b->stream));
+  WF_CUDA(nullptr, cudaEventRecord(b->fork_ev, b->stream));
+  for (int k = 0; k < wf::kFusedClassCount; ++k) {
+    if (!b->class_n[k]) continue;
+    cudaStream_t s = k == 0 ? b->stream : b->side[k - 1];
+    if (k > 0) WF_CUDA(nullptr, cudaStreamWaitEvent(s, b->fork_ev, 0));
+    WF_CUDA(nullptr, wf::launch_fused_batch(b->cfg, b->d_scenes, b->d_items + b->class_off[k],
+                                            b->class_n[k], b->d_counter + k, cur,
+                                            b->class_ctas[k], k, s));
+    if (k > 0) {
+      WF_CUDA(nullptr, cudaEventRecord(b->join_ev[k - 1], s));
+      WF_CUDA(nullptr, cudaStreamWaitEvent(b->stream, b->join_ev[k - 1], 0));
+    }
+  }
   return WF_OK;
 }
 
@@ -1852,9 +1882,18 @@ wf_status wf_batch_create(int n, const wf_grid_desc *descs, wf_batch **out) {
     delete b;
     return cuda_fail(nullptr, e, "cudaStreamCreate");
   }
-  if ((e = cudaMalloc(&b->d_counter, sizeof(int))) != cudaSuccess) {
+  if ((e = cudaMalloc(&b->d_counter, sizeof(int) * wf::kFusedClassCount)) != cudaSuccess) {
     wf_batch_destroy(b);
     return cuda_fail(nullptr, e, "cudaMalloc(counter)");
+  }
+  e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+  for (int k = 0; k < wf::kFusedClassCount - 1 && e == cudaSuccess; ++k) {
+    e = cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    wf_batch_destroy(b);
+    return cuda_fail(nullptr, e, "side stream setup");
   }
   for (int i = 0; i < n; ++i) {
     wf_grid_desc d = descs[i];
@@ -1878,6 +1917,14 @@ wf_status wf_batch_destroy(wf_batch *b) {
   batch_drop(b);
   for (wf_handle *h : b->h) wf_destroy(h);
   cudaFree(b->d_counter);
+  for (int k = 0; k < wf::kFusedClassCount - 1; ++k) {
+    if (b->side[k]) {
+      cudaStreamSynchronize(b->side[k]);
+      cudaStreamDestroy(b->side[k]);
+    }
+    if (b->join_ev[k]) cudaEventDestroy(b->join_ev[k]);
+  }
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return WF_OK;
@@ -1941,13 +1988,13 @@ wf_status wf_batch_step(wf_batch *b, int nsteps) {
       if (ec != cudaSuccess) return cuda_fail(nullptr, ec, "cudaGraphInstantiate");
     }
     WF_CUDA(nullptr, cudaGraphLaunch(ge, b->stream));
-    b->launches += static_cast<long long>(G) * (b->have_tail ? 2 : 1);
+    b->launches += static_cast<long long>(G) * (b->step_kernels + (b->have_tail ? 1 : 0));
     left -= G;
   }
   for (int i = 0; i < left; ++i) {
     st = batch_enqueue(b, cur);
     if (st != WF_OK) return st;
-    b->launches += b->have_tail ? 2 : 1;
+    b->launches += b->step_kernels + (b->have_tail ? 1 : 0);
     cur ^= 1;
   }
   for (wf_handle *h : b->h) {

@@ -71,17 +71,18 @@ cudaError_t fused_batch_prepare(const FusedConfig &c) {
 }
 
 cudaError_t launch_fused_batch(const FusedConfig &c, const BatchScene *scenes, const int2 *items,
-                               int n_items, int *counter, int parity, int ctas, cudaStream_t s) {
+                               int n_items, int *counter, int parity, int ctas, int ax,
+                               cudaStream_t s) {
 #define X(T, S_)                                                                         \
   if (c.ty == T && c.stages == S_)                                                      \
-    return batch_launch_t<T, S_>(scenes, items, n_items, counter, parity, ctas, s);
+    return batch_launch_t<T, S_>(scenes, items, n_items, counter, parity, ctas, ax, s);
   WF_FUSED_CONFIGS(X)
 #undef X
   return cudaErrorInvalidValue;
 }
 
-int fused_batch_ctas_per_sm(const FusedConfig &c) {
-#define X(T, S_) if (c.ty == T && c.stages == S_) return batch_ctas_per_sm_t<T, S_>();
+int fused_batch_ctas_per_sm(const FusedConfig &c, int ax) {
+#define X(T, S_) if (c.ty == T && c.stages == S_) return batch_ctas_per_sm_t<T, S_>(ax);
   WF_FUSED_CONFIGS(X)
 #undef X
   return 0;

@@ -735,13 +735,14 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, ST> :
   fused_body<TY, S, FMA, AX, ST>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
 }
 
-// Batched step: a persistent CTA takes (grid, item) pairs from a counter and
-// runs the all-axes CPML body (AX = 7) for each, with that grid's arguments
-// copied to shared memory and its TMA maps read from global memory.  The
-// mbarrier ring is re-initialised per item (every copy of the previous item
-// has completed: the body consumes or drains all it issued).
-template <int TY, int S>
-__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 2 : 1)
+// Batched step: one persistent launch per CPML class AX.  A CTA takes
+// (grid, item) pairs of its class from that class's counter and runs the
+// class's body for each, with that grid's arguments copied to shared memory
+// and its TMA maps read from global memory.  The mbarrier ring is
+// re-initialised per item (every copy of the previous item has completed:
+// the body consumes or drains all it issued).
+template <int TY, int S, int AX>
+__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, float> : 1)
     k_fused_batch(const BatchScene *scenes, const int2 *items, int n_items, int *counter,
                   int parity) {
   using L = Layout<TY, S, float>;
@@ -794,35 +795,66 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? 2 : 1)
     }
     first = false;
     __syncthreads();
-    fused_body<TY, S, false, 7, float>(&sc->maps[parity][0], &sc->maps[parity][1],
-                                       &sc->maps[parity][2], a, smem, x0, y0, k0, k1);
+    fused_body<TY, S, false, AX, float>(&sc->maps[parity][0], &sc->maps[parity][1],
+                                        &sc->maps[parity][2], a, smem, x0, y0, k0, k1);
   }
 }
 
+#define WF_AX_CLASSES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
+
 template <int TY, int S>
 cudaError_t batch_prepare_t() {
-  return cudaFuncSetAttribute((const void *)k_fused_batch<TY, S>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, Layout<TY, S, float>::BYTES);
+  const void *fns[] = {
+#define X(A) (const void *)k_fused_batch<TY, S, A>,
+      WF_AX_CLASSES(X)
+#undef X
+  };
+  for (const void *f : fns) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Layout<TY, S, float>::BYTES);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 template <int TY, int S>
 cudaError_t batch_launch_t(const BatchScene *scenes, const int2 *items, int n_items, int *counter,
-                           int parity, int ctas, cudaStream_t s) {
+                           int parity, int ctas, int ax, cudaStream_t s) {
   using L = Layout<TY, S, float>;
-  k_fused_batch<TY, S><<<ctas, L::THREADS, L::BYTES, s>>>(scenes, items, n_items, counter, parity);
+  switch (ax) {
+#define X(A)                                                                                    \
+  case A:                                                                                      \
+    k_fused_batch<TY, S, A><<<ctas, L::THREADS, L::BYTES, s>>>(scenes, items, n_items, counter, \
+                                                               parity);                        \
+    break;
+    WF_AX_CLASSES(X)
+#undef X
+    default:
+      return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
 template <int TY, int S>
-int batch_ctas_per_sm_t() {
+int batch_ctas_per_sm_t(int ax) {
+  using L = Layout<TY, S, float>;
+  const void *f = nullptr;
+  switch (ax) {
+#define X(A)                                 \
+  case A:                                    \
+    f = (const void *)k_fused_batch<TY, S, A>; \
+    break;
+    WF_AX_CLASSES(X)
+#undef X
+    default:
+      return 0;
+  }
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_batch<TY, S>, Layout<TY, S, float>::THREADS,
-                                                    Layout<TY, S, float>::BYTES) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, L::THREADS, L::BYTES) != cudaSuccess)
     return 0;
   return n;
 }
 
-#define WF_AX_CLASSES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
 
 template <int TY, int S, bool FMA, typename ST>
 cudaError_t prepare_t() {

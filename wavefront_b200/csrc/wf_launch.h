@@ -75,14 +75,16 @@ constexpr int kFusedClassCount = 8;
 // Launches the kernel of class `ax` over a device list of n_items items.
 cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                          const int *items, int n_items, int ax, bool fma, cudaStream_t s);
-// Batched step (FP32 storage, exact arithmetic): one persistent launch of
-// `ctas` CTAs that take (grid, item) pairs from *counter (zeroed by the
-// caller before each launch) until n_items are done.
+// Batched step (FP32 storage, exact arithmetic): one persistent launch per
+// CPML class `ax` of `ctas` CTAs that take (grid, item) pairs of that class
+// from *counter (zeroed by the caller before each launch) until n_items are
+// done.
 cudaError_t fused_batch_prepare(const FusedConfig &c);
 cudaError_t launch_fused_batch(const FusedConfig &c, const BatchScene *scenes, const int2 *items,
-                               int n_items, int *counter, int parity, int ctas, cudaStream_t s);
-// CTAs per SM the batched kernel of a tiling fits (for sizing `ctas`).
-int fused_batch_ctas_per_sm(const FusedConfig &c);
+                               int n_items, int *counter, int parity, int ctas, int ax,
+                               cudaStream_t s);
+// CTAs per SM the batched kernel of a tiling and class fits (for sizing `ctas`).
+int fused_batch_ctas_per_sm(const FusedConfig &c, int ax);
 // The step tail of n grids at once: one CTA per grid, t[i] as for launch_tail.
 cudaError_t launch_tail_batch(const TailArgs *t, int n, cudaStream_t s);
 
