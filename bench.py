@@ -206,9 +206,10 @@ def run_reference(args, rank, world):
 
 def run_batched(args, rank, world, local_rank):
     """Batched sweep: 256 independent cubes (edges 32..128, 1-4 primitives,
-    exact 10-cell CPML, Ricker source, one probe each) stepped together by one
-    persistent kernel per step (wf_batch_step, 32-step graph replays), tiling
-    from the batch autotuner.  value = total cells x steps / time."""
+    exact 10-cell CPML, Ricker source, one probe each; --scenes takes the first
+    N of them, for a small profiling case) stepped together by one persistent
+    launch per CPML class per step (wf_batch_step, 32-step graph replays),
+    tiling from the batch autotuner.  value = total cells x steps / time."""
     import torch
     from wavefront_b200 import configs
     torch.cuda.set_device(local_rank)
@@ -217,7 +218,7 @@ def run_batched(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     total = args.warmup + args.steps
-    scenes = configs.batched_sweep(256, steps=total)
+    scenes = configs.batched_sweep(256, steps=total)[:args.scenes]
     cells = sum(sc.dims.voxel_count() for sc in scenes)
     b = configs.device_batch(scenes, device=local_rank)
     if args.tiling:
@@ -587,6 +588,8 @@ def main():
                     help="two_spheres: the 512^3 headline; random_spheres: the mixed-precision "
                          "scene; demo_sphere: the reference's own benchmark shape (256^3 demo "
                          "sphere, 8-cell CPML)")
+    ap.add_argument("--scenes", type=int, default=256,
+                    help="batched workload: use the first N of its 256 scenes (profiling)")
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
                     help="field storage (16-bit: per-slab power-of-two scales, FP32 math)")
     args = ap.parse_args()
