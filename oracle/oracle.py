@@ -91,6 +91,8 @@ def _declare(L: C.CDLL) -> None:
         getattr(L, p + "probe_trace").argtypes = [C.c_void_p, C.c_int, _f64p]
         getattr(L, p + "set_storage").argtypes = [C.c_void_p, C.c_int]
         getattr(L, p + "set_storage").restype = C.c_int
+        getattr(L, p + "set_arith").argtypes = [C.c_void_p, C.c_int]
+        getattr(L, p + "set_arith").restype = C.c_int
         getattr(L, p + "storage_overflows").argtypes = [C.c_void_p]
         getattr(L, p + "storage_overflows").restype = C.c_longlong
         getattr(L, p + "get_shifts").argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -294,6 +296,13 @@ class Sim:
         self._f("probe_trace")(self._h, p, _ptr(out, _f64p))
         return out
 
+    def set_arith(self, arith: str):
+        """"exact" (the reference's operations) or "fma": the device FMA build's
+        fused forms, fma(b, psi, a*raw), fma(raw, 1/kappa, psi'),
+        fma(da, h, -(db*curl)), fma(ca, e, cb*curl) (f32, plain storage)."""
+        if self._f("set_arith")(self._h, 1 if arith == "fma" else 0) != 0:
+            raise ValueError("the FMA restatement needs the f32 oracle with plain storage")
+
     def set_storage(self, kind: str):
         """16-bit field storage emulation: "f32" (off), "f16" or "bf16" (both
         round to nearest even).  Call after the sources are added (their
@@ -325,11 +334,13 @@ def store16(v: float, kind: str, shift: int) -> float:
     return float(lib().or_store16(v, STORAGE_KINDS[kind], shift, C.byref(ov)))
 
 
-def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None, storage="f32"):
+def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None, storage="f32",
+                      arith="exact"):
     """Builds an oracle Sim for a wavefront_b200.configs.Scenario, computing every
     table (CPML profiles, source values, probe twiddles) with the oracle's own
     C code; only the scenario's description and its material ids are shared.
-    storage "f16"/"bf16" turns on the 16-bit storage emulation (f32 only)."""
+    storage "f16"/"bf16" turns on the 16-bit storage emulation (f32 only);
+    arith "fma" restates the device FMA build (f32, plain storage)."""
     steps = sc.steps if steps is None else steps
     d = sc.dims
     sim = Sim(d.nx, d.ny, d.nz, sc.grid.ids, sc.table.q16, periodic, dtype)
@@ -351,4 +362,6 @@ def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None, storage="
                       probe_first_step(p.start_recording_at_s, sc.dt), p.record_trace)
     if storage != "f32":
         sim.set_storage(storage)
+    if arith != "exact":
+        sim.set_arith(arith)
     return sim

@@ -106,6 +106,9 @@ typedef struct or_sim_f64 or_sim_f64;
   /* 16-bit field storage (f32 sim only): 0 plain, 1 f16, 2 bf16.  Re-encodes  \
    * the current state; -1 for a bad kind or on the f64 sim. */                \
   int S##_set_storage(S *s, int kind);                                          \
+  /* 1: restate the device FMA build's fused forms (f32 sim, plain storage);   \
+   * -1 otherwise. */                                                           \
+  int S##_set_arith(S *s, int fma);                                             \
   long long S##_storage_overflows(const S *s);                                  \
   /* write shifts (per 8-plane z slab) of the next step, E and H kinds */      \
   void S##_get_shifts(const S *s, int *shift_e, int *shift_h);

@@ -127,6 +127,25 @@ def test_fma_build_within_1e6_relative_l2(oracle):
         assert _rel_l2(out["fma"][c], out["exact"][c]) <= 3 * ref + 1e-7, c
 
 
+@pytest.mark.parametrize("kernel", ["fused", "split"])
+@pytest.mark.parametrize("scene", ["cube64", "two_spheres64"])
+def test_fma_build_equals_fma_restatement(oracle, kernel, scene):
+    """The FMA build computes exactly the fused forms it states:
+    psi' = fma(b, psi, a*raw), d = fma(raw, 1/kappa, psi'),
+    H' = fma(da, h, -(db*curl)), E' = fma(ca, e, cb*curl): bit for bit against
+    the oracle's restatement of those forms (fields, all psi, probe sums)."""
+    sc = (configs.plain_cube_64(steps=150) if scene == "cube64"
+          else configs.two_spheres(n=64, steps=150))
+    sim = oracle.sim_from_scenario(sc, arith="fma")
+    sim.step(sc.steps, NT)
+    g = _run_device(sc, kernel=kernel, arith="fma")
+    try:
+        _compare(g, sim, sc)
+    finally:
+        g.close()
+        sim.close()
+
+
 def test_exact_thin_cpml_10_cells(oracle):
     """Per-cell CPML of 10 cells (not rounded to blocks)."""
     sc = configs.plain_cube_64(steps=300, exact_pml=True)
