@@ -7,8 +7,8 @@ A step is one full Yee timestep of the whole grid (H, E, CPML psi, source,
 probes).  Metric: Mcell-updates/s = cells * steps / seconds / 1e6.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload two_spheres|random_spheres] [--grid N]
-                  [--precision f32|f16|bf16]
+                  [--workload two_spheres|random_spheres|demo_sphere|batched|closure]
+                  [--grid N] [--precision f32|f16|bf16] [--scenes N]
 
 --workload random_spheres --precision f16|bf16 measures the mixed-precision
 form (32 seeded random spheres, sinusoid source, 16-cell CPML; fields stored
@@ -64,6 +64,23 @@ def algorithmic_bytes(sc) -> int:
         if t:
             b += 32 * (cells // n[ax]) * min(2 * t, n[ax])
     return b
+
+
+def whole_job_value(world: int, cells: int, steps: int, seconds: float) -> float:
+    """Mcell-updates/s of the whole job: every rank's cells over the slowest
+    rank's time (ranks are replicas, so the work is world x cells x steps)."""
+    return world * cells * steps / seconds / 1e6
+
+
+def max_over_ranks(dist, value: float, device: str = "cuda") -> float:
+    """The largest value over all ranks (the slowest rank's time); every rank
+    calls it at the same point.  dist is torch.distributed or None (1 rank)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def peaks():
@@ -246,11 +263,8 @@ def run_batched(args, rank, world, local_rank):
     ms = e0.elapsed_time(e1)
     launches = b.kernel_launches - k0
     b.close()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    ms = max_over_ranks(dist, ms)
+    value = whole_job_value(world, cells, args.steps, ms / 1e3)
     alg = sum(algorithmic_bytes(sc) for sc in scenes)
     achieved = alg / (ms / args.steps / 1e3) / 1e9
     peak, peak_kind = peaks()
@@ -271,12 +285,10 @@ def run_batched(args, rank, world, local_rank):
     sums = [b.grid(i).probe_sums(0, 1) for i in range(len(scenes))]
     e2e_s = time.perf_counter() - t0
     b.close()
+    e2e_s = max_over_ranks(dist, e2e_s)
     if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
         dist.barrier()
-    e2e = world * cells * args.steps / e2e_s / 1e6
+    e2e = whole_job_value(world, cells, args.steps, e2e_s)
     h2d = cells + len(scenes) * (256 * 16 + total * (4 + 8 * 2))
     d2h = len(sums) * 24
 
@@ -479,11 +491,8 @@ def run_ours(args, rank, world, local_rank):
     g.set_timing(False)
     g.close()
     clocks = clk.summary()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * N_CELLS * args.steps / (ms / 1e3) / 1e6
+    ms = max_over_ranks(dist, ms)
+    value = whole_job_value(world, N_CELLS, args.steps, ms / 1e3)
 
     alg = algorithmic_bytes(sc)
     per_launch_ms = kern_ms / max(launches, 1)
@@ -529,12 +538,10 @@ def run_ours(args, rank, world, local_rank):
                   "steps": round((t_stepped - t_built) * 1e3, 1),
                   "probe_sums_and_snapshot": round((t0 + e2e_s - t_stepped) * 1e3, 1)}
         g.close()
+        e2e_s = max_over_ranks(dist, e2e_s)
         if dist:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
             dist.barrier()
-        e2e = world * N_CELLS * args.steps / e2e_s / 1e6
+        e2e = whole_job_value(world, N_CELLS, args.steps, e2e_s)
         h2d = (N_CELLS if sc.grid is not None else len(sc.scene_text)) + 256 * 16 + total * (4 + 8 * 16)
         d2h = len(sums) * (8 * 2 + 8) + N_CELLS * 24
         e2e_line = {"value": round(e2e, 1), "unit": METRIC,

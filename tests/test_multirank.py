@@ -1,0 +1,68 @@
+"""CPU: the N > 1 path of bench.py, with world_size-2 gloo process groups.
+
+Every rank runs its own replica (the timestep path needs no collective), the
+job's time is the slowest rank's (max over ranks), and the whole-job value
+counts every rank's cells. The reference arm under torchrun runs on rank 0
+alone and prints one line; the other ranks exit 0 without work.
+"""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out_dir):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        t = bench.max_over_ranks(dist, 1.5 + rank, device="cpu")  # rank r "took" 1.5 + r
+        with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
+            json.dump({"max": t, "value": bench.whole_job_value(world, 1000, 10, t)}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_whole_job_value_gloo(tmp_path):
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    got = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(world)]
+    for g in got:
+        assert g["max"] == 2.5  # every rank sees the slowest rank's time
+        assert g["value"] == pytest.approx(world * 1000 * 10 / 2.5 / 1e6)
+
+
+def test_whole_job_value_single_rank():
+    assert bench.max_over_ranks(None, 3.25) == 3.25
+    assert bench.whole_job_value(1, 512 ** 3, 1000, 1.5) == pytest.approx(512 ** 3 * 1000 / 1.5 / 1e6)
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    env = dict(os.environ, WF_REF_SECONDS="5")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py",
+           "--impl", "reference", "--grid", "64", "--steps", "2", "--warmup", "3"]
+    r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["steps"] == 2 and d["warmup"] == 3
+    assert d["e2e"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
