@@ -410,6 +410,10 @@ def run_closure(args, rank, world, local_rank):
     refl = {k: CL.reflection_test(**kw)["max_rel_error"] for k, kw in (
         ("thin_layer_alone", {"truncated": True}),
         ("thin_layer_with_closure_gain_0.5", {"net": net, "alpha": 0.5, "truncated": True}),
+        ("thin_layer_with_closure_gain_1_energy_guard",
+         {"net": net, "alpha": 1.0, "truncated": True, "guard": True}),
+        ("thin_layer_with_closure_gain_0.5_energy_guard",
+         {"net": net, "alpha": 0.5, "truncated": True, "guard": True}),
         ("plain_cpml_4", {"cpml": 4}), ("plain_cpml_16", {"cpml": 16}))}
     value = interior ** 3 / (closure_ms / 1e3) / 1e6
     line = {

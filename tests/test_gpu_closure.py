@@ -90,6 +90,57 @@ def test_closure_in_step_equals_explicit_pipeline():
         g2.close()
 
 
+def test_energy_guard_in_step_and_never_raises_band_energy():
+    """With the guard on, a step equals the explicit pipeline with the guard
+    applied by hand, and each face's correction can only lower the energy of
+    its band's six fields (sum of squares in the gained units)."""
+    sc = configs.plain_cube_64(steps=1, n=32)
+    net = CL.ClosureNet(seed=4)
+    net.w[2].mul_(400.0)  # a correction large enough that the guard must act
+    net.wb[2].copy_(net.w[2].to(torch.bfloat16))
+    dims = wf.GridDims(32, 32, 32)
+    rng = np.random.default_rng(6)
+    f0 = (rng.standard_normal((6, 32, 32, 32)) * 0.01).astype(np.float32)
+    g1 = wf.DeviceFieldGrid(dims, kernel="fused")
+    g2 = wf.DeviceFieldGrid(dims, kernel="fused")
+    try:
+        for g in (g1, g2):
+            g.set_materials(wf.MaterialGrid(dims), wf.MaterialTable.vacuum_filled(sc.dt, sc.dx))
+            CL.set_thin_cpml(g, sc.dt, sc.dx)
+            g.set_fields(f0)
+        net.attach(g1, guard=True)
+        g1.step(1)
+        g2.step(1)
+        g2.sync()
+        P = 8 * 32 * 32
+        X = torch.empty(6, 10, 8, 32, 32, device=net.dev)
+        L.check(L.lib().wf_band_gather(g2._h, CL._p(X), net.gain_e, net.gain_h))
+        torch.cuda.synchronize()
+        s = torch.sqrt(torch.sum(X[:, :3].reshape(6, -1) ** 2, dim=1) / (3 * P)) + 1e-30
+        Xs = (X / s.view(6, 1, 1, 1, 1)).contiguous()
+        faces = torch.arange(6, dtype=torch.int32, device=net.dev)
+        y, _ = net.forward(Xs, faces)
+        Y = y * s.view(6, 1, 1, 1, 1)
+        F = X[:, :6]
+        a = torch.sum((F * Y).reshape(6, -1).double(), dim=1)
+        b = torch.sum((Y * Y).reshape(6, -1).double(), dim=1)
+        grow = 2 * a + b > 0
+        lam = torch.where(grow, torch.clamp(-2 * a / torch.clamp(b, min=1e-300), 0, 1),
+                          torch.ones_like(a))
+        assert bool(grow.any())  # the guard has work to do in this case
+        Yg = (Y * lam.view(6, 1, 1, 1, 1).float()).contiguous()
+        e_before = torch.sum((F * F).reshape(6, -1).double(), dim=1)
+        e_after = torch.sum(((F + Yg) ** 2).reshape(6, -1).double(), dim=1)
+        assert bool(torch.all(e_after <= e_before * (1 + 1e-6)))
+        L.check(L.lib().wf_band_scatter_add(g2._h, CL._p(Yg), net.gain_e, net.gain_h))
+        torch.cuda.synchronize()
+        got, want = g1.fields(), g2.fields()
+        assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
+    finally:
+        g1.close()
+        g2.close()
+
+
 @pytest.fixture(scope="module")
 def trained():
     X, R, F, _ = CL.generate(96, seed=1)
@@ -118,3 +169,6 @@ def test_ablation_closure_on_the_thin_layer(trained):
           f"plain 4-cell CPML {steep4['max_rel_error']:.3f}, 16-cell CPML {thick16['max_rel_error']:.4f}")
     assert np.isfinite(closed["max_rel_error"])
     assert closed["max_rel_error"] < 0.5 * thin["max_rel_error"]
+    guarded = CL.reflection_test(net=net, alpha=1.0, truncated=True, guard=True)
+    print(f"closure at gain 1 with the energy guard {guarded['max_rel_error']:.3f}")
+    assert np.isfinite(guarded["max_rel_error"])

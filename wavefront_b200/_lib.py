@@ -22,7 +22,8 @@ EXPORTS = [
     "wf_batch_create", "wf_batch_destroy", "wf_batch_size", "wf_batch_handle", "wf_batch_step",
     "wf_batch_sync", "wf_batch_get_stream", "wf_batch_kernel_launches", "wf_batch_get_tiling",
     "wf_batch_set_tiling", "wf_batch_autotune",
-    "wf_set_closure", "wf_band_gather", "wf_band_scatter_add", "wf_restrict_state",
+    "wf_set_closure", "wf_set_closure_guard", "wf_band_gather", "wf_band_scatter_add",
+    "wf_restrict_state",
     "wf_nn_conv3d_forward", "wf_nn_conv3d_backward_data", "wf_nn_conv3d_backward_weight",
     "wf_nn_gelu_backward", "wf_nn_mse", "wf_nn_adam",
     "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
@@ -140,6 +141,7 @@ def lib() -> C.CDLL:
         L.wf_batch_autotune.restype = S
         vp = C.c_void_p
         L.wf_set_closure.argtypes = [_h, vp, vp, vp, C.c_float, C.c_float]
+        L.wf_set_closure_guard.argtypes = [_h, C.c_int]
         L.wf_band_gather.argtypes = [_h, vp, C.c_float, C.c_float]
         L.wf_band_scatter_add.argtypes = [_h, vp, C.c_float, C.c_float]
         L.wf_restrict_state.argtypes = [_h, _h, C.c_int]
@@ -150,7 +152,7 @@ def lib() -> C.CDLL:
         L.wf_nn_mse.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
         L.wf_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float,
                                  C.c_float, C.c_int, vp]
-        for name in ("wf_set_closure", "wf_band_gather", "wf_band_scatter_add", "wf_restrict_state",
+        for name in ("wf_set_closure", "wf_set_closure_guard", "wf_band_gather", "wf_band_scatter_add", "wf_restrict_state",
                      "wf_nn_conv3d_forward", "wf_nn_conv3d_backward_data",
                      "wf_nn_conv3d_backward_weight", "wf_nn_gelu_backward", "wf_nn_mse",
                      "wf_nn_adam"):

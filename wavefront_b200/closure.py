@@ -141,13 +141,16 @@ class ClosureNet:
         self.adam_step(lr)
         return loss
 
-    def attach(self, grid: DeviceFieldGrid, alpha: float = 1.0):
+    def attach(self, grid: DeviceFieldGrid, alpha: float = 1.0, guard: bool = False):
         """The network as grid's closure (applied after every step kernel),
-        its correction scaled by alpha (folded into the last layer)."""
+        its correction scaled by alpha (folded into the last layer); guard
+        scales each face's correction so that it cannot raise the band's
+        energy (wf_set_closure_guard)."""
         torch = _torch()
         w3 = self.wb[2] if alpha == 1.0 else (self.w[2] * alpha).to(torch.bfloat16)
         _chk(_L.lib().wf_set_closure(grid._h, _p(self.wb[0]), _p(self.wb[1]), _p(w3),
                                      self.gain_e, self.gain_h))
+        _chk(_L.lib().wf_set_closure_guard(grid._h, 1 if guard else 0))
 
     @staticmethod
     def detach(grid: DeviceFieldGrid):
@@ -360,7 +363,7 @@ def residual_loss(net: Optional[ClosureNet], X, R, F, batch: int = 256) -> float
 
 def reflection_test(interior: int = 48, steps: int = 260, net: Optional[ClosureNet] = None,
                     cpml: int = THIN, device: int = 0, seed: int = 3, alpha: float = 1.0,
-                    truncated: bool = False) -> dict:
+                    truncated: bool = False, guard: bool = False) -> dict:
     """Reflection of the boundary of an interior^3 region with a `cpml`-cell
     CPML (plus `net` as its closure), against a reference run in a domain
     large enough that nothing returns within `steps`: a Ricker Ez source
@@ -394,7 +397,7 @@ def reflection_test(interior: int = 48, steps: int = 260, net: Optional[ClosureN
                 g.add_probe_tables(p[0] + off, p[1] + off, p[2] + off, PC.Ez,
                                    np.zeros((steps, 0)), np.zeros((steps, 0)), 0, record_trace=True)
             if closure:
-                net.attach(g, alpha)
+                net.attach(g, alpha, guard)
             g.step(steps)
             g.sync()
             return np.stack([g.probe_trace(i, steps) for i in range(len(probes_i))]).astype(np.float64)

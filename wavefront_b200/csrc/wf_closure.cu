@@ -365,6 +365,40 @@ __global__ void k_face_rms(const float *X, int C, long long P, float *s) {
   if (threadIdx.x == 0) s[f] = sqrtf(s_sum[0] / static_cast<float>(3 * P)) + 1e-30f;
 }
 
+// Energy guard of a face's correction Y (field units times the gains) on its
+// band fields F = X * s[f] (X normalised, channels 0-5 the fields): with
+// a = <F, Y> and b = <Y, Y> over the six field channels, the band energy
+// changes by 2a + b; if that is positive, lam[f] = clamp(-2a / b, 0, 1) is the
+// largest factor that keeps it from growing, else lam[f] = 1.
+__global__ void k_face_guard(const float *X, int C, const float *Y, long long P, const float *s,
+                             float *lam) {
+  __shared__ float s_a[256], s_b[256];
+  const int f = blockIdx.x;
+  const float *x = X + static_cast<long long>(f) * C * P;
+  const float *y = Y + static_cast<long long>(f) * 6 * P;
+  float a = 0.0f, b = 0.0f;
+  for (long long i = threadIdx.x; i < 6 * P; i += blockDim.x) {
+    a += x[i] * y[i];
+    b += y[i] * y[i];
+  }
+  s_a[threadIdx.x] = a;
+  s_b[threadIdx.x] = b;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) {
+      s_a[threadIdx.x] += s_a[threadIdx.x + k];
+      s_b[threadIdx.x] += s_b[threadIdx.x + k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const float aa = s_a[0] * s[f], bb = s_b[0];
+    float l = 1.0f;
+    if (2.0f * aa + bb > 0.0f) l = (aa < 0.0f && bb > 0.0f) ? fminf(1.0f, -2.0f * aa / bb) : 0.0f;
+    lam[f] = l;
+  }
+}
+
 // X[f][c][p] *= s[f] (or / s[f])
 __global__ void k_face_scale(float *X, int C, long long P, const float *s, int divide) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -454,6 +488,12 @@ int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, 
 
 int face_rms(const float *X, int C, long long P, float *s, void *stream) {
   k_face_rms<<<6, 256, 0, static_cast<cudaStream_t>(stream)>>>(X, C, P, s);
+  return cudaGetLastError();
+}
+
+int face_guard(const float *X, int C, const float *Y, long long P, const float *s, float *lam,
+               void *stream) {
+  k_face_guard<<<6, 256, 0, static_cast<cudaStream_t>(stream)>>>(X, C, Y, P, s, lam);
   return cudaGetLastError();
 }
 

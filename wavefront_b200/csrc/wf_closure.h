@@ -44,6 +44,10 @@ int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, 
 // s[f] = RMS of face f's E channels in X[6][C][P]; X[f] *= s[f] (or /=).
 int face_rms(const float *X, int C, long long P, float *s, void *stream);
 int face_scale(float *X, int C, long long P, const float *s, int divide, void *stream);
+// Per face, the factor lam[f] in [0, 1] that keeps the correction Y from
+// raising the energy of the band fields X * s[f] (see k_face_guard).
+int face_guard(const float *X, int C, const float *Y, long long P, const float *s, float *lam,
+               void *stream);
 // student = teacher restricted at offset `off` (fields and each axis's psi).
 int band_restrict(const BandGrid &teacher, const BandGrid &student, int off, void *stream);
 

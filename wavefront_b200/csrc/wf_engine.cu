@@ -95,6 +95,7 @@ struct wf_handle {
   void *cl_w[3] = {nullptr, nullptr, nullptr};  // bf16 weights, 6 faces per layer
   float *cl_buf = nullptr;                      // X, A1, A2, Y band tensors
   float cl_ge = 1.0f, cl_gh = 1.0f;
+  bool cl_guard = false;  // wf_set_closure_guard
   int *cl_face = nullptr;                       // device {0, 1, ..., 5}
   long long version = 0;               // bumped when device tables are reallocated
   long long kernel_launches = 0;       // step + tail kernels issued so far
@@ -315,7 +316,7 @@ cudaError_t closure_enqueue(wf_handle *h) {
   float *X = h->cl_buf, *A1 = X + 6 * wf::kBandIn * P, *A2 = A1 + 6 * kClHidden * P,
         *Y = A2 + 6 * kClHidden * P;
   const wf::BandGrid g = band_grid(h, h->cur ^ 1);
-  float *scale = Y + 6 * 6 * P;
+  float *scale = Y + 6 * 6 * P, *lam = scale + 8;
   int e = wf::band_gather(g, X, n, n, h->cl_ge, h->cl_gh, h->stream);
   if (!e) e = wf::face_rms(X, wf::kBandIn, P, scale, h->stream);
   if (!e) e = wf::face_scale(X, wf::kBandIn, P, scale, 1, h->stream);
@@ -324,6 +325,8 @@ cudaError_t closure_enqueue(wf_handle *h) {
   if (!e) e = wf::nn_conv_fwd(A1, h->cl_w[1], h->cl_face, nullptr, A2, 6, kClHidden, kClHidden, D, n, n, 1, h->stream);
   if (!e) e = wf::nn_conv_fwd(A2, h->cl_w[2], h->cl_face, nullptr, Y, 6, kClHidden, 6, D, n, n, 0, h->stream);
   if (!e) e = wf::face_scale(Y, 6, P, scale, 0, h->stream);
+  if (!e && h->cl_guard) e = wf::face_guard(X, wf::kBandIn, Y, P, scale, lam, h->stream);
+  if (!e && h->cl_guard) e = wf::face_scale(Y, 6, P, lam, 0, h->stream);
   if (!e) e = wf::band_scatter_add(g, Y, n, n, h->cl_ge, h->cl_gh, h->stream);
   return static_cast<cudaError_t>(e);
 }
@@ -1401,7 +1404,7 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
   }
   if (!h->cl_buf) {
     const long long P = static_cast<long long>(wf::kBandDepth) * h->nx * h->nx;
-    WF_CUDA(h, cudaMalloc(&h->cl_buf, sizeof(float) * (6 * P * (wf::kBandIn + 2 * kClHidden + 6) + 8)));
+    WF_CUDA(h, cudaMalloc(&h->cl_buf, sizeof(float) * (6 * P * (wf::kBandIn + 2 * kClHidden + 6) + 16)));
     const int faces[6] = {0, 1, 2, 3, 4, 5};
     WF_CUDA(h, cudaMalloc(&h->cl_face, sizeof(faces)));
     WF_CUDA(h, cudaMemcpy(h->cl_face, faces, sizeof(faces), cudaMemcpyHostToDevice));
@@ -1409,6 +1412,15 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
   h->cl_ge = gain_e;
   h->cl_gh = gain_h;
   h->closure = true;
+  return WF_OK;
+}
+
+wf_status wf_set_closure_guard(wf_handle *h, int on) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  drop_graphs(h);
+  h->cl_guard = on != 0;
   return WF_OK;
 }
 
