@@ -283,10 +283,11 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms);
 wf_status wf_set_closure(wf_handle *h, const void *w1_bf16, const void *w2_bf16,
                          const void *w3_bf16, float gain_e, float gain_h);  /* w1 NULL: off */
 /* Energy guard of the closure (off by default): per face, the correction is
- * scaled by the largest factor in [0, 1] that keeps it from raising the
- * energy of the band's six fields (sum of squares in the gained units; with
- * gain_h = 377 gain_e that is the electromagnetic energy up to a constant),
- * so the closure can only take energy out of the band. */
+ * scaled by the largest factor in [0, 1] that keeps it from raising the sum
+ * of squares of the band's six fields in the gained units (with gain_h = 377
+ * gain_e, the field energy density up to a constant).  It is not a stability
+ * guarantee: the Yee scheme's conserved energy pairs E and H at staggered
+ * times, and the CPML's psi is not covered. */
 wf_status wf_set_closure_guard(wf_handle *h, int on);
 /* The current state's bands into device X[6][10][8][n][n] (scaled as above). */
 wf_status wf_band_gather(wf_handle *h, float *X, float gain_e, float gain_h);

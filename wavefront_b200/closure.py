@@ -253,7 +253,8 @@ def _grids(run: Run, dx: float, dt: float, steps: int, device: int):
 
 
 def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, crop: int = 16,
-             seed: int = 1, device: int = 0, net: Optional["ClosureNet"] = None, max_lead: int = 12):
+             seed: int = 1, device: int = 0, net: Optional["ClosureNet"] = None, max_lead: int = 12,
+             guard: bool = False):
     """Teacher-forced one-step samples: returns (X [M][10][8][c][c],
     R [M][6][8][c][c], face [M] int32, 1.0) on the device.  H-side values
     are times ETA0, and every sample is divided by the RMS of the E channels
@@ -264,7 +265,8 @@ def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, cr
     1..max_lead steps with `net` as its closure from the teacher's state
     (the last of them without the closure, whose input is the sample): the
     target is the teacher's state at the same time, so the network also
-    learns to pull a drifting student back (a DAgger-style round)."""
+    learns to pull a drifting student back (a DAgger-style round).  guard
+    runs those closure steps with the energy guard on."""
     torch = _torch()
     dev = torch.device("cuda", device)
     rng = np.random.default_rng(seed)
@@ -286,7 +288,7 @@ def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, cr
                 done = k - lead + 1
                 _chk(_L.lib().wf_restrict_state(teacher._h, s1._h, OFFSET))
                 if lead > 1:
-                    net.attach(s1)
+                    net.attach(s1, guard=guard)
                     for _ in range(lead - 1):
                         s1.step(1)
                         teacher.step(1)
