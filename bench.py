@@ -429,7 +429,8 @@ def run_closure(args, rank, world, local_rank):
         "comparison_ms_per_step": {"cpml16_256^3": round(thick_ms, 4),
                                    "thin4_232^3_with_closure": round(closure_ms, 4),
                                    "thin4_232^3_alone": round(thin_ms, 4)},
-        "reflection_test_max_rel_error": {k: round(v, 5) for k, v in refl.items()},
+        "reflection_test_max_rel_error": {k: (round(v, 5) if np.isfinite(v) else None)
+                                          for k, v in refl.items()},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
