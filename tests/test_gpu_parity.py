@@ -160,6 +160,48 @@ def test_exact_thin_cpml_10_cells(oracle):
             g.close()
 
 
+@pytest.mark.parametrize("shape", [(8, 8, 8), (8, 136, 16), (264, 16, 16), (16, 16, 200)])
+def test_extreme_grid_shapes(oracle, shape):
+    """The smallest grid, a tile with 2 of its 32 lanes inside the domain, a
+    last x tile 8 cells wide, and a long thin z axis: fused under two tilings
+    and split, bit for bit (fields, psi, probe sums).  The CPML thickness
+    follows the reference's rounding, so grids one block thick get none."""
+    nx, ny, nz = shape
+    dims = wf.GridDims(nx, ny, nz)
+    dx = 1e-3
+    dt = configs.courant_dt(dx)
+    grid = wf.MaterialGrid(dims)
+    table = wf.MaterialTable.vacuum_filled(dt, dx)
+    wf.Scene.parse(f"sphere 3.0 1.0 0.01 {nx / 2} {ny / 2} {nz / 2} {min(nx, ny, nz) / 3}\n").voxelize(
+        grid, table, dt, dx)
+    pml = wf.PmlContext.build(dims, wf.PmlConfig(thickness=8), dt, dx)
+    f = float(np.float32(3e8 / (12 * dx)))
+    srcs = [wf.Source(nx // 2, ny // 2, nz // 2, wf.FieldComponent.Ez, 1.0,
+                      wf.default_waveform("ricker", f)),
+            wf.Source(nx - 1, ny - 1, nz - 1, wf.FieldComponent.Ex, 0.5,
+                      wf.default_waveform("gaussian", f))]
+    prbs = [wf.Probe(nx // 4, ny // 3, nz // 2, wf.ProbeComponent(c), [f], 0.0) for c in (2, 4)]
+    sc = configs.Scenario("extreme", dims, dx, dt, grid, table, pml, srcs, prbs, 60)
+    sim = oracle.sim_from_scenario(sc)
+    sim.step(sc.steps, NT)
+    for kernel, tiling in (("fused", (4, 12, 3)), ("fused", (16, 5, 3)), ("split", None)):
+        g = configs.device_grid(sc, kernel=kernel)
+        try:
+            if tiling:
+                g.set_tiling(*tiling)
+            for s_ in srcs:
+                g.add_source_values(s_.x, s_.y, s_.z, s_.component, s_.values(dt, sc.steps))
+            for p in prbs:
+                c, si = p.tables(dt, sc.steps)
+                g.add_probe_tables(p.x, p.y, p.z, p.component, c, si, p.first_step(dt))
+            g.step(sc.steps)
+            g.sync()
+            _compare(g, sim, sc)
+        finally:
+            g.close()
+    sim.close()
+
+
 def test_ragged_grid_materials_h_probes_and_late_start(oracle):
     """nx not a multiple of the 128-cell tile, ny not a multiple of the tile
     rows, a thin z axis, a lossy scene, several sources and H-component
