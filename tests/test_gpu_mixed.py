@@ -103,6 +103,36 @@ def test_ragged_grid_tilings_match_storage_emulation(oracle, prec):
             g.close()
 
 
+@pytest.mark.parametrize("prec", ["f16", "bf16"])
+@pytest.mark.parametrize("shape", [(8, 136, 16), (264, 16, 16), (16, 16, 72)])
+def test_extreme_shapes_match_storage_emulation(oracle, prec, shape):
+    """A tile with 2 of its 32 lanes in the domain, a last x tile 8 cells wide,
+    and a thin grid with 9 z slabs, in 16-bit storage: bit for bit against the
+    emulation (fields, psi, probe sums, next shifts)."""
+    nx, ny, nz = shape
+    dims = wf.GridDims(nx, ny, nz)
+    dx = 1e-3
+    dt = configs.courant_dt(dx)
+    grid = wf.MaterialGrid(dims)
+    table = wf.MaterialTable.vacuum_filled(dt, dx)
+    wf.Scene.parse(f"sphere 3.0 1.0 0.01 {nx / 2} {ny / 2} {nz / 2} {min(nx, ny, nz) / 3}\n").voxelize(
+        grid, table, dt, dx)
+    pml = wf.PmlContext.build(dims, wf.PmlConfig(thickness=8), dt, dx)
+    f = float(np.float32(3e8 / (12 * dx)))
+    srcs = [wf.Source(nx // 2, ny // 2, nz // 2, wf.FieldComponent.Ez, 1.0,
+                      wf.default_waveform("ricker", f))]
+    prbs = [wf.Probe(nx // 4, ny // 3, nz // 2, wf.ProbeComponent(c), [f], 0.0) for c in (2, 4)]
+    sc = configs.Scenario("extreme16", dims, dx, dt, grid, table, pml, srcs, prbs, 60)
+    sim = oracle.sim_from_scenario(sc, storage=prec)
+    sim.step(sc.steps, NT)
+    for tiling in (None, (8, 5, 3)):
+        g = _run(sc, prec, tiling=tiling)
+        try:
+            _compare(g, sim, sc)
+        finally:
+            g.close()
+
+
 def test_random_spheres_128_f16_matches_emulation_and_fields_round_trip(oracle):
     """The mixed-precision scene at 128^3 for 300 steps; then the FP32 view
     (get_fields / snapshot) re-encodes losslessly into a fresh handle."""
