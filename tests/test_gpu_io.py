@@ -3,8 +3,8 @@
 1. engine.run with output_path writes wave_trajectory.bin: one FieldBlock
    snapshot (src/engine.rs:617-640) after every step whose index is a
    multiple of snapshot_every, appended back to back; each equals the oracle's
-   blocks at that step bit for bit (FP32, and binary16 against the storage
-   emulation), and voxels read the way src/bin/wavefront-view.rs:280-305
+   blocks at that step bit for bit (FP32, and binary16 and bfloat16 against
+   the storage emulation), and voxels read the way src/bin/wavefront-view.rs:280-305
    reads them equal the oracle's fields.
 2. The writer overlaps stepping: captures taken between steps on a larger
    grid equal wf_download_blocks at the same steps.
@@ -54,7 +54,7 @@ def _read_component(snap, dims, x, y, z, field):
     return snap[b * BLOCK_FLOATS + field * 512 + local]
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16"])
+@pytest.mark.parametrize("prec", ["f32", "f16", "bf16"])
 def test_trajectory_file_matches_oracle(tmp_path, prec):
     steps, every = 40, 10
     sc = configs.plain_cube_64(steps=steps)
@@ -112,7 +112,7 @@ def test_writer_overlaps_stepping(tmp_path):
         ref.close()
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16"])
+@pytest.mark.parametrize("prec", ["f32", "f16", "bf16"])
 def test_checkpoint_resume_is_bit_exact(tmp_path, prec):
     steps = 90
     sc = configs.random_spheres(n=64, steps=steps, pml_cells=10)
