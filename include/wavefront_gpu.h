@@ -130,6 +130,13 @@ wf_status wf_set_materials(wf_handle *h, const uint8_t *ids,
  * reference's message. */
 wf_status wf_set_scene(wf_handle *h, const char *text, float dt, float dx,
                        int32_t (*table_q16)[4], int *n_materials);
+/* wf_set_scene for the z window [z_offset, z_offset + nz) of a scene on an
+ * nx x ny x nz_global grid: the primitives are placed and clamped in the
+ * global grid and the handle receives that window's planes, the ids the
+ * global grid holds there (one z slab of a decomposed grid). */
+wf_status wf_set_scene_window(wf_handle *h, const char *text, float dt, float dx,
+                              int nz_global, int z_offset, int32_t (*table_q16)[4],
+                              int *n_materials);
 /* The material ids on the device, nz*ny*nx bytes (MaterialGrid order). */
 wf_status wf_get_materials(wf_handle *h, uint8_t *ids);
 
@@ -230,6 +237,21 @@ wf_status wf_device_fields(wf_handle *h, float **out6);
  * kind whose largest stored binary16 magnitude was 65504 (where larger
  * values saturate).  FP32 and bfloat16 storage report 0. */
 wf_status wf_storage_info(wf_handle *h, int *shift_e, int *shift_h, uint64_t *overflows);
+
+/* ---- z-slab decomposition (no reference counterpart) ------------------- */
+
+/* A grid split along z runs one handle per slab: the slab's own planes plus
+ * a ghost block of neighbouring planes on each inner side.  These copy the
+ * complete stepping state of the planes [z0, z0 + nplanes) (six field
+ * components and the x and y CPML psi of those planes) between the current
+ * state and a packed device buffer of wf_slab_floats(h, nplanes) floats
+ * (16-byte aligned), enqueued on the handle's stream without waiting.
+ * z CPML psi is not part of a slab: a decomposition keeps the z-CPML planes
+ * out of every ghost block.  FP32 storage only (WF_ERR_UNSUPPORTED
+ * otherwise).  wf_slab_floats returns -1 for bad arguments. */
+int64_t wf_slab_floats(const wf_handle *h, int nplanes);
+wf_status wf_slab_pack(wf_handle *h, int z0, int nplanes, float *dst_device);
+wf_status wf_slab_unpack(wf_handle *h, int z0, int nplanes, const float *src_device);
 
 /* The handle's CUDA stream (cudaStream_t) for event timing and interop. */
 wf_status wf_get_stream(wf_handle *h, void **out_stream);

@@ -1,0 +1,136 @@
+"""GPU: the z-slab decomposition in one process against the whole grid.
+
+A grid split into 2-4 z slabs (SlabDomain: one handle per slab on one device
+and one stream, ghost blocks moved every 8 steps by the pack/unpack kernels)
+must give the whole grid's fields and probe sums, with +0 and -0 treated as
+equal (the slabs holding the z CPML run its interior-valued profile on their
+other side, where the correction can flip the sign of a zero).  The scenes
+have CPML on every axis, so the x and y psi of the ghost planes move too,
+and sources on ghost planes.
+"""
+import numpy as np
+import pytest
+
+from wavefront_b200 import configs
+from wavefront_b200 import slabs as S
+from wavefront_b200._lib import WF_ERR_UNSUPPORTED, WfError
+from wavefront_b200.engine import DeviceFieldGrid
+from wavefront_b200.source import FieldComponent, Source, default_waveform
+
+pytestmark = pytest.mark.gpu
+STEPS = 61
+
+
+def _eq(got, want, what):
+    bad = got != want
+    assert not bad.any(), f"{what}: {bad.sum()} cells differ, first {np.argwhere(bad)[:4].tolist()}"
+
+
+def _scene(n=128, device_voxelize=False):
+    if device_voxelize:
+        sc = configs.random_spheres(n, steps=STEPS, device_voxelize=True)
+    else:
+        sc = configs.two_spheres(n, steps=STEPS)
+    f = sc.meta["f"]
+    # sources on planes that are ghost planes of the 2- and 4-way plans
+    sc.sources.append(Source(40, 50, 60, FieldComponent.Ex, 0.25, default_waveform("ricker", f)))
+    sc.sources.append(Source(70, 61, 66, FieldComponent.Ey, -0.5, default_waveform("ricker", f)))
+    return sc
+
+
+def _whole(sc, **kw):
+    g = configs.device_grid(sc, **kw)
+    for s in sc.sources:
+        g.add_source_values(s.x, s.y, s.z, s.component, s.values(sc.dt, STEPS), s.mode)
+    for p in sc.probes:
+        c, si = p.tables(sc.dt, STEPS)
+        g.add_probe_tables(p.x, p.y, p.z, p.component, c, si, p.first_step(sc.dt))
+    g.step(STEPS)
+    g.sync()
+    return g
+
+
+def _check(sc, parts, **kw):
+    whole = _whole(sc, **kw)
+    want = whole.fields()
+    assert np.abs(want).max() > 0
+    d = S.SlabDomain(sc, parts, steps=STEPS, **kw)
+    try:
+        d.step(3)
+        d.step(STEPS - 3)
+        assert d.exchanges == (STEPS - 1) // S.GHOST
+        _eq(d.fields(), want, f"fields, {parts} slabs")
+        for i, p in enumerate(sc.probes):
+            nf = len(p.frequencies_hz)
+            gc, gs, gn = d.probe_sums(i, nf)
+            wc, ws, wn = whole.probe_sums(i, nf)
+            assert gn == wn and np.array_equal(gc, wc) and np.array_equal(gs, ws), i
+    finally:
+        d.close()
+        whole.close()
+
+
+@pytest.mark.parametrize("parts", [2, 3, 4])
+def test_slab_domain_equals_whole_grid(parts):
+    _check(_scene(), parts)
+
+
+def test_slab_domain_split_kernel():
+    _check(_scene(), 2, kernel="split")
+
+
+def test_scene_window_voxelizer_and_device_scene():
+    sc = _scene(device_voxelize=True)
+    whole = DeviceFieldGrid(sc.dims)
+    whole.set_scene(sc.scene_text, sc.table, sc.dt, sc.dx)
+    ids = whole.materials().reshape(sc.dims.nz, -1)
+    whole.close()
+    for s in S.plan(sc.dims.nz, 3, 16):
+        g = DeviceFieldGrid(configs.GridDims(sc.dims.nx, sc.dims.ny, s.nz))
+        g.set_scene_window(sc.scene_text, configs.MaterialTable(sc.table.q16.copy()), sc.dt,
+                           sc.dx, sc.dims.nz, s.lo)
+        assert np.array_equal(g.materials().reshape(s.nz, -1), ids[s.lo:s.hi])
+        g.close()
+    _check(sc, 3)
+
+
+def test_pack_unpack_round_trip_moves_fields_and_psi():
+    sc = configs.two_spheres(64, steps=20)
+    a = _whole(sc)
+    b = configs.device_grid(sc)
+    import torch
+    n = a.slab_floats(8)
+    nx = ny = 64
+    row_x = ny * ((32 + 3) // 4 * 4)  # x psi: 2 x 16 slab positions per row
+    assert n == 6 * 8 * nx * ny + 4 * 8 * row_x + 4 * 8 * 32 * nx
+    buf = torch.empty(n, dtype=torch.float32, device="cuda")
+    a.pack_planes(24, 8, buf.data_ptr())
+    b.unpack_planes(8, 8, buf.data_ptr())
+    a.sync()
+    b.sync()
+    fa, fb = a.fields(), b.fields()
+    assert np.array_equal(fb[:, 8:16].view(np.uint32), fa[:, 24:32].view(np.uint32))
+    assert not fb[:, :8].any() and not fb[:, 16:].any()
+    for w in (0, 1, 2, 3, 6, 7, 8, 9):  # x and y psi arrays
+        pa, pb = a.psi(w), b.psi(w)
+        assert np.array_equal(pb[8:16].view(np.uint32), pa[24:32].view(np.uint32)), w
+    a.close()
+    b.close()
+
+
+def test_slab_copies_reject_bad_arguments():
+    import torch
+    g = DeviceFieldGrid(configs.GridDims(32, 32, 32), precision="f16")
+    buf = torch.empty(1 << 16, dtype=torch.float32, device="cuda")
+    with pytest.raises(WfError) as e:
+        g.pack_planes(0, 8, buf.data_ptr())
+    assert e.value.status == WF_ERR_UNSUPPORTED
+    g.close()
+    g = DeviceFieldGrid(configs.GridDims(32, 32, 32))
+    with pytest.raises(WfError):
+        g.pack_planes(30, 8, buf.data_ptr())  # past nz
+    with pytest.raises(WfError):
+        g.pack_planes(0, 8, buf.data_ptr() + 4)  # not 16-byte aligned
+    with pytest.raises(ValueError):
+        g.slab_floats(0)
+    g.close()

@@ -30,6 +30,7 @@ EXPORTS = [
     "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
     "wf_snapshot_open", "wf_snapshot_capture", "wf_snapshot_close", "wf_set_test_stall",
     "wf_checkpoint_save", "wf_checkpoint_load",
+    "wf_set_scene_window", "wf_slab_floats", "wf_slab_pack", "wf_slab_unpack",
     "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
     "wf_material_coeffs", "wf_effective_pml_thickness_blocks", "wf_pml_profile",
     "wf_waveform_eval", "wf_source_values", "wf_probe_first_step", "wf_probe_tables",
@@ -117,6 +118,15 @@ def lib() -> C.CDLL:
         L.wf_set_scene.restype = S
         L.wf_get_materials.argtypes = [_h, _u8p]
         L.wf_get_materials.restype = S
+        L.wf_set_scene_window.argtypes = [_h, C.c_char_p, C.c_float, C.c_float, C.c_int, C.c_int,
+                                          _i32p, C.POINTER(C.c_int)]
+        L.wf_set_scene_window.restype = S
+        L.wf_slab_floats.argtypes = [_h, C.c_int]
+        L.wf_slab_floats.restype = C.c_int64
+        L.wf_slab_pack.argtypes = [_h, C.c_int, C.c_int, C.c_void_p]
+        L.wf_slab_pack.restype = S
+        L.wf_slab_unpack.argtypes = [_h, C.c_int, C.c_int, C.c_void_p]
+        L.wf_slab_unpack.restype = S
         L.wf_batch_create.argtypes = [C.c_int, C.POINTER(GridDesc), C.POINTER(_h)]
         L.wf_batch_create.restype = S
         L.wf_batch_destroy.argtypes = [_h]

@@ -842,18 +842,78 @@ wf_status wf_set_materials(wf_handle *h, const uint8_t *ids, const int32_t (*tab
 
 wf_status wf_set_scene(wf_handle *h, const char *text, float dt, float dx,
                        int32_t (*table)[4], int *n_materials) {
+  if (!h) return fail(h, WF_ERR_ARG, "null argument");
+  return wf_set_scene_window(h, text, dt, dx, h->nz, 0, table, n_materials);
+}
+
+wf_status wf_set_scene_window(wf_handle *h, const char *text, float dt, float dx, int nz_global,
+                              int z_offset, int32_t (*table)[4], int *n_materials) {
   if (!h || !text || !table) return fail(h, WF_ERR_ARG, "null argument");
+  if (nz_global < h->nz || z_offset < 0 || z_offset > nz_global - h->nz)
+    return fail(h, WF_ERR_ARG, "the window [z_offset, z_offset + nz) must lie in [0, nz_global)");
   std::vector<wf::RasterOp> ops;
   std::string msg;
-  if (!wf::scene_parse(text, h->nx, h->ny, h->nz, dt, dx, &ops, table, n_materials, &msg))
+  if (!wf::scene_parse(text, h->nx, h->ny, nz_global, dt, dx, &ops, table, n_materials, &msg))
     return fail(h, WF_ERR_ARG, msg);
   DeviceGuard guard(h->dev);
   wf_status st = upload_coef(h, table);
   if (st != WF_OK) return st;
-  WF_CUDA(h, static_cast<cudaError_t>(
-                 wf::launch_voxelize(ops, h->mat, h->nx, h->ny, h->nz, h->mat_pitch, 0, h->stream)));
+  WF_CUDA(h, static_cast<cudaError_t>(wf::launch_voxelize(ops, h->mat, h->nx, h->ny, h->nz,
+                                                          h->mat_pitch, 0, h->stream, z_offset)));
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   return WF_OK;
+}
+
+namespace {
+
+// The state of planes [z0, z0 + np) as segments of the packed slab layout:
+// Ex Ey Ez Hx Hy Hz [np][ny][nx], then the x psi slots [4][np][ny][pitch],
+// then the y psi slots [4][np][W][nx] (each present when that axis has CPML).
+wf::SlabSegments slab_segments(const wf_handle *h, int z0, int np) {
+  wf::SlabSegments sg{};
+  long long off = 0;
+  auto add = [&](float *dev, long long n) {
+    sg.seg[sg.n++] = wf::SlabSegment{dev, off, n};
+    off += n;
+  };
+  const long long plane = static_cast<long long>(h->nx) * h->ny;
+  for (int c = 0; c < 6; ++c) add(h->fld[h->cur] + c * h->N + z0 * plane, np * plane);
+  const AxisState &X = h->ax[0], &Y = h->ax[1];
+  if (X.T > 0) {
+    const long long row = static_cast<long long>(h->ny) * X.pitch;
+    for (int k = 0; k < 4; ++k) add(X.psi[h->cur] + k * X.cells + z0 * row, np * row);
+  }
+  if (Y.T > 0) {
+    const long long row = static_cast<long long>(Y.W) * h->nx;
+    for (int k = 0; k < 4; ++k) add(Y.psi[h->cur] + k * Y.cells + z0 * row, np * row);
+  }
+  return sg;
+}
+
+wf_status slab_copy(wf_handle *h, int z0, int np, float *buf, bool unpack) {
+  if (!h || !buf) return fail(h, WF_ERR_ARG, "null argument");
+  if (store16(h)) return fail(h, WF_ERR_UNSUPPORTED, "slab copies need FP32 storage");
+  if (np < 1 || z0 < 0 || z0 > h->nz - np) return fail(h, WF_ERR_ARG, "planes outside the grid");
+  if (reinterpret_cast<uintptr_t>(buf) & 15) return fail(h, WF_ERR_ARG, "buffer not 16-byte aligned");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, wf::launch_slab_copy(slab_segments(h, z0, np), buf, unpack, h->stream));
+  return WF_OK;
+}
+
+}  // namespace
+
+int64_t wf_slab_floats(const wf_handle *h, int nplanes) {
+  if (!h || nplanes < 1 || nplanes > h->nz) return -1;
+  const wf::SlabSegments sg = slab_segments(h, 0, nplanes);
+  return sg.seg[sg.n - 1].off + sg.seg[sg.n - 1].n;
+}
+
+wf_status wf_slab_pack(wf_handle *h, int z0, int nplanes, float *dst) {
+  return slab_copy(h, z0, nplanes, dst, false);
+}
+
+wf_status wf_slab_unpack(wf_handle *h, int z0, int nplanes, const float *src) {
+  return slab_copy(h, z0, nplanes, const_cast<float *>(src), true);
 }
 
 wf_status wf_get_materials(wf_handle *h, uint8_t *ids) {

@@ -111,4 +111,18 @@ cudaError_t launch_state_max(const void *in, int prec, int nx, int ny, int nz, c
 // Write shifts of the step with index `next` into t.shift_next (see k_tail).
 cudaError_t launch_next_shifts(const TailArgs &t, long long next, cudaStream_t s);
 
+// z-slab ghost blocks: contiguous device segments of a grid's state and their
+// offsets in a packed buffer (floats; all multiples of 4, 16-byte aligned).
+struct SlabSegment {
+  float *dev;
+  long long off, n;
+};
+constexpr int kSlabMaxSegments = 14;  // 6 field components + 4 x psi + 4 y psi
+struct SlabSegments {
+  SlabSegment seg[kSlabMaxSegments];
+  int n;
+};
+// One launch: every segment copied into the packed buffer, or out of it.
+cudaError_t launch_slab_copy(const SlabSegments &segs, float *buf, bool unpack, cudaStream_t s);
+
 }  // namespace wf

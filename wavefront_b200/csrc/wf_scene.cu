@@ -13,7 +13,9 @@ namespace wf {
 
 namespace {
 
-__global__ void k_raster(RasterOp op, uint8_t *ids, int nx, int ny, int pitch) {
+// op's z range is already clipped to the window; z_lo is the window's first
+// plane, so the id of global plane z lands in row plane z - z_lo.
+__global__ void k_raster(RasterOp op, uint8_t *ids, int nx, int ny, int pitch, long long z_lo) {
   const long long wx = op.x1 - op.x0, wy = op.y1 - op.y0, wz = op.z1 - op.z0;
   const long long n = wx * wy * wz;
   for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
@@ -26,7 +28,7 @@ __global__ void k_raster(RasterOp op, uint8_t *ids, int nx, int ny, int pitch) {
       const float ddz = __fsub_rn(__fadd_rn(static_cast<float>(z), 0.5f), op.cz);
       in = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz)) <= op.r2;
     }
-    if (in) ids[(z * ny + y) * pitch + x] = op.id;
+    if (in) ids[((z - z_lo) * ny + y) * pitch + x] = op.id;
   }
   (void)nx;
 }
@@ -34,16 +36,19 @@ __global__ void k_raster(RasterOp op, uint8_t *ids, int nx, int ny, int pitch) {
 }  // namespace
 
 int launch_voxelize(const std::vector<RasterOp> &ops, uint8_t *ids, int nx, int ny, int nz,
-                    int pitch, uint8_t fill, void *stream) {
+                    int pitch, uint8_t fill, void *stream, int z_lo) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(ids, fill, static_cast<size_t>(pitch) * ny * nz, s);
   if (e != cudaSuccess) return e;
-  for (const RasterOp &op : ops) {
+  for (RasterOp op : ops) {
+    // keep the planes of the window [z_lo, z_lo + nz)
+    if (op.z0 < z_lo) op.z0 = z_lo;
+    if (op.z1 > static_cast<long long>(z_lo) + nz) op.z1 = static_cast<long long>(z_lo) + nz;
+    if (op.x1 <= op.x0 || op.y1 <= op.y0 || op.z1 <= op.z0) continue;
     const long long n = (op.x1 - op.x0) * (op.y1 - op.y0) * (op.z1 - op.z0);
-    if (op.x1 <= op.x0 || op.y1 <= op.y0 || op.z1 <= op.z0 || n <= 0) continue;
     const long long want = (n + 255) / 256;
     const unsigned blocks = static_cast<unsigned>(want < 148 * 64 ? want : 148 * 64);
-    k_raster<<<blocks, 256, 0, s>>>(op, ids, nx, ny, pitch);
+    k_raster<<<blocks, 256, 0, s>>>(op, ids, nx, ny, pitch, z_lo);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;

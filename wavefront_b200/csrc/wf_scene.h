@@ -30,8 +30,9 @@ bool scene_parse(const char *text, int nx, int ny, int nz, float dt, float dx,
                  std::string *err);
 
 // Device voxelizer: ids (pitch bytes per row, nz*ny rows) set to `fill`, then
-// every op applied in order on `stream`.
+// every op applied in order on `stream`.  The ids hold the planes
+// [z_lo, z_lo + nz) of the scene's grid (ops carry that grid's coordinates).
 int launch_voxelize(const std::vector<RasterOp> &ops, uint8_t *ids, int nx, int ny, int nz,
-                    int pitch, uint8_t fill, void *stream);
+                    int pitch, uint8_t fill, void *stream, int z_lo = 0);
 
 }  // namespace wf

@@ -105,6 +105,17 @@ class DeviceFieldGrid:
         table.q16[:] = q
         return n.value
 
+    def set_scene_window(self, text: str, table: MaterialTable, dt: float, dx: float,
+                         nz_global: int, z_offset: int) -> int:
+        """set_scene for the planes [z_offset, z_offset + nz) of the scene on
+        an nx x ny x nz_global grid (one z slab of a decomposed grid)."""
+        q = np.ascontiguousarray(table.q16, np.int32)
+        n = C.c_int()
+        self._chk(_L.lib().wf_set_scene_window(self._h, text.encode(), dt, dx, nz_global,
+                                               z_offset, _L.ptr(q, _L.i32p), C.byref(n)))
+        table.q16[:] = q
+        return n.value
+
     def materials(self) -> np.ndarray:
         """The device material ids, nz*ny*nx bytes."""
         out = np.empty(self.dims.voxel_count(), np.uint8)
@@ -247,6 +258,24 @@ class DeviceFieldGrid:
         arr = (C.c_void_p * 6)()
         self._chk(_L.lib().wf_device_fields(self._h, arr))
         return [int(v) for v in arr]
+
+    # -- z-slab copies ---------------------------------------------------------
+    def slab_floats(self, nplanes: int) -> int:
+        """Floats of the packed state of `nplanes` z planes (wf_slab_floats)."""
+        n = int(_L.lib().wf_slab_floats(self._h, nplanes))
+        if n < 0:
+            raise ValueError(f"bad plane count {nplanes} for nz = {self.dims.nz}")
+        return n
+
+    def pack_planes(self, z0: int, nplanes: int, dst_ptr: int) -> None:
+        """Enqueues the copy of planes [z0, z0 + nplanes) of the current state
+        into the device buffer at dst_ptr (wf_slab_pack)."""
+        self._chk(_L.lib().wf_slab_pack(self._h, z0, nplanes, C.c_void_p(dst_ptr)))
+
+    def unpack_planes(self, z0: int, nplanes: int, src_ptr: int) -> None:
+        """Enqueues the copy of a packed buffer into planes [z0, z0 + nplanes)
+        of the current state (wf_slab_unpack)."""
+        self._chk(_L.lib().wf_slab_unpack(self._h, z0, nplanes, C.c_void_p(src_ptr)))
 
     def set_test_stall(self, extra_bytes: int) -> None:
         """Testing aid (wf_set_test_stall): makes every fused step's first TMA

@@ -1,0 +1,350 @@
+"""Z-slab decomposition of one grid: one handle per slab, ghost blocks between.
+
+The reference splits its grid into z slabs of whole blocks for its rayon
+threads (src/engine.rs:8-13), all in one address space, each thread reading
+its neighbours' planes directly.  Here a slab is a separate grid (on its own
+GPU, or several on one GPU) that holds its own planes [z0, z1) plus a ghost
+block of GHOST planes on each inner side, [lo, hi).
+
+Why the ghost blocks stay exact for GHOST steps: H(k) reads E(k) and E(k+1),
+E(k) reads H(k) and H(k-1).  A slab's outer ghost planes see zero fields
+beyond [lo, hi) where the whole grid has real ones, so each step the wrong
+values advance one plane inward from lo and from hi - 1.  After s steps the
+planes [lo, lo + s) and [hi - s, hi) may be wrong; the owned planes read
+the ghost planes next to them, z0 - 1 and z1, which stay exact while
+s <= GHOST.  So every GHOST steps each slab receives both ghost blocks
+(the six field components and the x and y CPML psi of those planes) from
+its neighbours' owned planes, and runs GHOST more steps.  Sources on a
+ghost plane are applied by both slabs that hold it (the ghost must evolve
+exactly); probes only by the owner.
+
+z CPML: the slab holding a real z-CPML layer gets the global profile sliced
+to its planes, with the same thickness, so its other z side carries the
+profile's interior values (b 1, a 0, 1/kappa 1): psi stays exactly +0 there
+and the curl passes through unchanged.  `plan` keeps the real layer off
+every ghost block, so z psi never has to move between slabs.
+
+Transports: `SlabDomain` runs all slabs in one process on one device, one
+CUDA stream, moving ghost blocks with the pack/unpack kernels through a
+device staging buffer; `SlabRank` runs one slab per rank of a
+torch.distributed group and moves ghost blocks with batched point-to-point
+sends (NCCL over NVLink between GPUs).  FP32 storage only.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional
+
+import numpy as np
+
+from .layout import GridDims, MaterialGrid, MaterialTable
+
+GHOST = 8  # planes per ghost block, and steps between exchanges
+_HARD_SHEET_X = 1  # WF_SRC_HARD_SHEET_X: writes every (y, z) of its plane x
+
+
+@dataclass(frozen=True)
+class Slab:
+    index: int
+    z0: int  # first owned plane of the whole grid
+    z1: int  # one past the last owned plane
+    lo: int  # first plane held (z0 - GHOST, or 0)
+    hi: int  # one past the last plane held (z1 + GHOST, or nz)
+
+    @property
+    def nz(self) -> int:
+        return self.hi - self.lo
+
+    def owns(self, z: int) -> bool:
+        return self.z0 <= z < self.z1
+
+    def holds(self, z: int) -> bool:
+        return self.lo <= z < self.hi
+
+
+def plan(nz: int, parts: int, pml_z: int = 0) -> List[Slab]:
+    """Splits nz planes into `parts` slabs of whole 8-plane blocks, the first
+    nz/8 % parts slabs one block larger.  With more than one slab the first
+    and last must own at least pml_z + GHOST planes, so that no ghost block
+    reaches a real z-CPML plane."""
+    if nz <= 0 or nz % 8:
+        raise ValueError("nz must be a positive multiple of 8")
+    blocks = nz // 8
+    if parts < 1 or parts > blocks:
+        raise ValueError(f"cannot split {blocks} z blocks into {parts} slabs")
+    base, extra = divmod(blocks, parts)
+    out, z = [], 0
+    for i in range(parts):
+        z1 = z + 8 * (base + (1 if i < extra else 0))
+        out.append(Slab(i, z, z1, max(z - GHOST, 0), min(z1 + GHOST, nz)))
+        z = z1
+    if parts > 1 and pml_z > 0:
+        for s in (out[0], out[-1]):
+            if s.z1 - s.z0 < pml_z + GHOST:
+                raise ValueError(f"slab {s.index} owns {s.z1 - s.z0} planes; with a {pml_z}-plane "
+                                 f"z CPML the end slabs need at least {pml_z + GHOST}")
+    return out
+
+
+@dataclass
+class SlabSpec:
+    """Everything one slab's grid is loaded with, in slab coordinates."""
+    slab: Slab
+    dims: GridDims
+    ids: Optional[np.ndarray]       # nz*ny*nx material ids, or None (scene window)
+    scene_text: Optional[str]
+    table: MaterialTable
+    pml: list                       # per axis (thickness, b, a, inv_kappa) or None
+    sources: list = field(default_factory=list)  # (x, y, z, comp, values, mode)
+    probes: list = field(default_factory=list)   # (global index, x, y, z, comp, cos, sin, first, trace)
+
+
+def slab_spec(sc, slab: Slab, steps: int) -> SlabSpec:
+    """The slab's share of a Scenario: its planes of the material ids (or the
+    scene text for a device window), the CPML profiles (x, y whole; z sliced),
+    every source on a plane it holds (sheet sources everywhere) and every
+    probe on a plane it owns, with tables for `steps` steps."""
+    d = sc.dims
+    dims = GridDims(d.nx, d.ny, slab.nz)
+    ids = None
+    if sc.grid is not None:
+        plane = d.nx * d.ny
+        ids = np.ascontiguousarray(sc.grid.ids[slab.lo * plane:slab.hi * plane])
+    table = MaterialTable(np.array(sc.table.q16, np.int32, copy=True))
+    pml = [None, None, None]
+    if sc.pml is not None:
+        for ax in range(3):
+            p = sc.pml.profiles[ax]
+            t = int(sc.pml.thickness_voxels[ax])
+            if t == 0:
+                continue
+            if ax < 2:
+                pml[ax] = (t, p.b, p.a, p.inv_kappa)
+            elif slab.lo < t or slab.hi > d.nz - t:
+                sl = slice(slab.lo, slab.hi)
+                pml[ax] = (t, p.b[sl].copy(), p.a[sl].copy(), p.inv_kappa[sl].copy())
+    spec = SlabSpec(slab, dims, ids, None if ids is not None else sc.scene_text, table, pml)
+    for s in sc.sources:
+        vals = s.values(sc.dt, steps)
+        if s.mode == _HARD_SHEET_X:
+            spec.sources.append((s.x, s.y, 0, int(s.component), vals, s.mode))
+        elif slab.holds(s.z):
+            spec.sources.append((s.x, s.y, s.z - slab.lo, int(s.component), vals, s.mode))
+    for i, p in enumerate(sc.probes):
+        if slab.owns(p.z):
+            c, si = p.tables(sc.dt, steps)
+            spec.probes.append((i, p.x, p.y, p.z - slab.lo, int(p.component), c, si,
+                                p.first_step(sc.dt), bool(p.record_trace)))
+    return spec
+
+
+class DeviceSlabState:
+    """A slab's grid on the device (DeviceFieldGrid) behind the interface the
+    transports use: step, floats/pack/unpack of plane ranges into torch
+    device tensors, owned fields and probe sums."""
+
+    def __init__(self, spec: SlabSpec, nz_global: int, sc, stream: int, device: int = 0,
+                 arith: str = "exact", kernel: str = "auto"):
+        from .engine import DeviceFieldGrid
+        self.spec = spec
+        g = DeviceFieldGrid(spec.dims, arith=arith, kernel=kernel, device=device, stream=stream)
+        self.grid = g
+        if spec.ids is not None:
+            g.set_materials(MaterialGrid(spec.dims, spec.ids), spec.table)
+        else:
+            g.set_scene_window(spec.scene_text, spec.table, sc.dt, sc.dx, nz_global,
+                               spec.slab.lo)
+        for ax, p in enumerate(spec.pml):
+            if p is not None:
+                g.set_pml_axis(ax, *p)
+        for (x, y, z, comp, vals, mode) in spec.sources:
+            g.add_source_values(x, y, z, comp, vals, mode)
+        self.probe_index = {}
+        for (gi, x, y, z, comp, c, si, first, trace) in spec.probes:
+            self.probe_index[gi] = g.add_probe_tables(x, y, z, comp, c, si, first, trace)
+
+    def step(self, n: int) -> None:
+        self.grid.step(n)
+
+    def floats(self, nplanes: int) -> int:
+        return self.grid.slab_floats(nplanes)
+
+    def pack(self, z0: int, nplanes: int, out) -> None:
+        self.grid.pack_planes(z0, nplanes, out.data_ptr())
+
+    def unpack(self, z0: int, nplanes: int, src) -> None:
+        self.grid.unpack_planes(z0, nplanes, src.data_ptr())
+
+    def owned_fields(self) -> np.ndarray:
+        s = self.spec.slab
+        return self.grid.fields()[:, s.z0 - s.lo:s.z1 - s.lo]
+
+    def probe_sums(self, global_index: int, nfreq: int):
+        return self.grid.probe_sums(self.probe_index[global_index], nfreq)
+
+    def close(self) -> None:
+        self.grid.close()
+
+
+def _pml_z(sc) -> int:
+    """The scenario's z-CPML thickness (0 without CPML)."""
+    return int(sc.pml.thickness_voxels[2]) if sc.pml is not None else 0
+
+
+class SlabDomain:
+    """All slabs of a grid in this process on one device and one CUDA stream.
+    step(n) runs every slab in lockstep, exchanging ghost blocks every GHOST
+    steps through the pack/unpack kernels; fields() and probe_sums() read the
+    owning slabs.  Results equal the whole grid's bit for bit."""
+
+    def __init__(self, sc, parts: int, steps: Optional[int] = None, device: int = 0,
+                 arith: str = "exact", kernel: str = "auto"):
+        import torch
+        self.sc = sc
+        steps = sc.steps if steps is None else steps
+        self.slabs = plan(sc.dims.nz, parts, _pml_z(sc))
+        self._torch = torch
+        self.stream = torch.cuda.Stream(device=device)
+        self.states = [DeviceSlabState(slab_spec(sc, s, steps), sc.dims.nz, sc,
+                                       self.stream.cuda_stream, device, arith, kernel)
+                       for s in self.slabs]
+        n = self.states[0].floats(GHOST) if parts > 1 else 4
+        self._buf = torch.empty(n, dtype=torch.float32, device=f"cuda:{device}")
+        self._since = 0  # steps since the last exchange
+        self.exchanges = 0
+
+    def exchange(self) -> None:
+        """Refreshes every ghost block from its owner (stream-ordered)."""
+        for a, b in zip(self.states, self.states[1:]):
+            sa, sb = a.spec.slab, b.spec.slab
+            # b's lowest owned block -> a's upper ghost block
+            b.pack(sb.z0 - sb.lo, GHOST, self._buf)
+            a.unpack(sa.z1 - sa.lo, GHOST, self._buf)
+            # a's highest owned block -> b's lower ghost block
+            a.pack(sa.z1 - GHOST - sa.lo, GHOST, self._buf)
+            b.unpack(0, GHOST, self._buf)
+        self.exchanges += 1
+
+    def step(self, n: int = 1) -> None:
+        while n > 0:
+            if self._since == GHOST:
+                if len(self.states) > 1:
+                    self.exchange()
+                self._since = 0
+            k = min(GHOST - self._since, n)
+            for s in self.states:
+                s.step(k)
+            self._since += k
+            n -= k
+
+    def sync(self) -> None:
+        self.stream.synchronize()
+        for s in self.states:
+            s.grid.sync()
+
+    def fields(self) -> np.ndarray:
+        self.sync()
+        return np.concatenate([s.owned_fields() for s in self.states], axis=1)
+
+    def probe_sums(self, p: int, nfreq: int):
+        self.sync()
+        for s in self.states:
+            if p in s.probe_index:
+                return s.probe_sums(p, nfreq)
+        raise IndexError(f"no probe {p}")
+
+    def close(self) -> None:
+        for s in self.states:
+            s.close()
+        self.states = []
+
+
+class SlabRank:
+    """This rank's slab of a grid split over the ranks of a torch.distributed
+    group (one process per GPU).  step(n) exchanges ghost blocks with the two
+    neighbouring ranks every GHOST steps through batched point-to-point
+    sends and receives of packed device buffers; every rank calls step with
+    the same n.  `make_state(spec)` builds the slab's state (default: a
+    DeviceSlabState on the current CUDA device and stream)."""
+
+    def __init__(self, sc, group=None, steps: Optional[int] = None,
+                 make_state: Optional[Callable] = None, arith: str = "exact",
+                 kernel: str = "auto"):
+        import torch
+        import torch.distributed as dist
+        self._dist, self._torch, self.group = dist, torch, group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        steps = sc.steps if steps is None else steps
+        self.slabs = plan(sc.dims.nz, self.world, _pml_z(sc))
+        self.slab = self.slabs[self.rank]
+        spec = slab_spec(sc, self.slab, steps)
+        if make_state is None:
+            dev = torch.cuda.current_device()
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            self.state = DeviceSlabState(spec, sc.dims.nz, sc, stream, dev, arith, kernel)
+            where = torch.device("cuda", dev)
+        else:
+            self.state = make_state(spec)
+            where = torch.device("cpu")
+        n = self.state.floats(GHOST)
+        self._bufs = [torch.empty(n, dtype=torch.float32, device=where) for _ in range(4)]
+        self._since = 0
+        self.exchanges = 0
+
+    def _peer(self, r: int) -> int:
+        return r if self.group is None else self._dist.get_global_rank(self.group, r)
+
+    def exchange(self) -> None:
+        dist, s = self._dist, self.slab
+        send_lo, recv_lo, send_hi, recv_hi = self._bufs
+        ops = []
+        if self.rank > 0:
+            self.state.pack(s.z0 - s.lo, GHOST, send_lo)
+            ops += [dist.P2POp(dist.isend, send_lo, self._peer(self.rank - 1), self.group),
+                    dist.P2POp(dist.irecv, recv_lo, self._peer(self.rank - 1), self.group)]
+        if self.rank < self.world - 1:
+            self.state.pack(s.z1 - GHOST - s.lo, GHOST, send_hi)
+            ops += [dist.P2POp(dist.isend, send_hi, self._peer(self.rank + 1), self.group),
+                    dist.P2POp(dist.irecv, recv_hi, self._peer(self.rank + 1), self.group)]
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        if self.rank > 0:
+            self.state.unpack(0, GHOST, recv_lo)
+        if self.rank < self.world - 1:
+            self.state.unpack(s.z1 - s.lo, GHOST, recv_hi)
+        self.exchanges += 1
+
+    def step(self, n: int = 1) -> None:
+        while n > 0:
+            if self._since == GHOST:
+                if self.world > 1:
+                    self.exchange()
+                self._since = 0
+            k = min(GHOST - self._since, n)
+            self.state.step(k)
+            self._since += k
+            n -= k
+
+    def gather_fields(self, dst: int = 0) -> Optional[np.ndarray]:
+        """The whole grid's fields on rank `dst` (None elsewhere)."""
+        part = self.state.owned_fields()
+        got = [None] * self.world if self.rank == dst else None
+        self._dist.gather_object(part, got, dst=self._peer(dst), group=self.group)
+        return np.concatenate(got, axis=1) if self.rank == dst else None
+
+    def gather_probe_sums(self, nfreq: int, dst: int = 0) -> Optional[dict]:
+        """{global probe index: (cos sums, sin sums, samples)} on rank `dst`."""
+        mine = {p: self.state.probe_sums(p, nfreq) for p in self.state.probe_index}
+        got = [None] * self.world if self.rank == dst else None
+        self._dist.gather_object(mine, got, dst=self._peer(dst), group=self.group)
+        if self.rank != dst:
+            return None
+        out = {}
+        for d in got:
+            out.update(d)
+        return out
+
+    def close(self) -> None:
+        self.state.close()
