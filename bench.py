@@ -583,6 +583,53 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_slabs(args, local_rank):
+    """The workload split into `--slabs` z slabs on one GPU (SlabDomain: one
+    handle per slab, 8-plane ghost blocks refreshed every 8 steps by the
+    pack/unpack kernels, all on one stream).  value counts the whole grid's
+    cells once; the ghost planes are the decomposition's extra work."""
+    import torch
+    from wavefront_b200 import slabs as S
+    torch.cuda.set_device(local_rank)
+    total = args.warmup + args.steps
+    sc = scenario(args, total)
+    d = S.SlabDomain(sc, args.slabs, steps=total, device=local_rank)
+    if args.tiling:
+        for st in d.states:
+            st.grid.set_tiling(*[int(v) for v in args.tiling.split(",")])
+    d.step(args.warmup)
+    d.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k_before = sum(st.grid.kernel_launches for st in d.states)
+    x_before = d.exchanges
+    with ClockSampler(local_rank) as clk:
+        e0.record(d.stream)
+        d.step(args.steps)
+        e1.record(d.stream)
+        d.sync()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    # each exchange: two packs and two unpacks per neighbouring pair
+    launches = (sum(st.grid.kernel_launches for st in d.states) - k_before
+                + 4 * (args.slabs - 1) * (d.exchanges - x_before))
+    planes = sum(s.nz for s in d.slabs)
+    d.close()
+    value = whole_job_value(1, N_CELLS, args.steps, ms / 1e3)
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {**scene_config(sc), "slabs": args.slabs, "ghost_planes": S.GHOST,
+                   "exchange_every_steps": S.GHOST, "planes_stepped_per_step": planes,
+                   "parallelism": f"z slabs x{args.slabs} on 1 GPU"},
+        "e2e": {"value": None, "unit": METRIC, "skipped": "--slabs measures the decomposition"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -602,6 +649,9 @@ def main():
                          "sphere, 8-cell CPML)")
     ap.add_argument("--scenes", type=int, default=256,
                     help="batched workload: use the first N of its 256 scenes (profiling)")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="two_spheres/random_spheres/demo_sphere on one GPU split into this many "
+                         "z slabs with ghost-block exchange (FP32)")
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
                     help="field storage (16-bit: per-slab power-of-two scales, FP32 math)")
     args = ap.parse_args()
@@ -632,6 +682,10 @@ def main():
         run_batched(args, rank, world, local_rank)
     elif args.workload == "closure":
         run_closure(args, rank, world, local_rank)
+    elif args.slabs:
+        if world > 1 or PRECISION != "f32":
+            raise SystemExit("--slabs runs on one GPU with FP32 storage")
+        run_slabs(args, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 
