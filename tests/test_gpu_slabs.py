@@ -8,14 +8,20 @@ other side, where the correction can flip the sign of a zero).  The scenes
 have CPML on every axis, so the x and y psi of the ghost planes move too,
 and sources on ghost planes.
 """
+import os
+import socket
+import sys
+
 import numpy as np
 import pytest
 
-from wavefront_b200 import configs
-from wavefront_b200 import slabs as S
-from wavefront_b200._lib import WF_ERR_UNSUPPORTED, WfError
-from wavefront_b200.engine import DeviceFieldGrid
-from wavefront_b200.source import FieldComponent, Source, default_waveform
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+from wavefront_b200 import configs  # noqa: E402
+from wavefront_b200 import slabs as S  # noqa: E402
+from wavefront_b200._lib import WF_ERR_UNSUPPORTED, WfError  # noqa: E402
+from wavefront_b200.engine import DeviceFieldGrid  # noqa: E402
+from wavefront_b200.source import FieldComponent, Source, default_waveform  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 STEPS = 61
@@ -79,6 +85,10 @@ def test_slab_domain_split_kernel():
     _check(_scene(), 2, kernel="split")
 
 
+def test_slab_domain_fma_build():
+    _check(_scene(), 3, arith="fma")
+
+
 def test_scene_window_voxelizer_and_device_scene():
     sc = _scene(device_voxelize=True)
     whole = DeviceFieldGrid(sc.dims)
@@ -134,3 +144,53 @@ def test_slab_copies_reject_bad_arguments():
     with pytest.raises(ValueError):
         g.slab_floats(0)
     g.close()
+
+
+def _rank_main(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        r = S.SlabRank(_scene(), steps=STEPS)
+        r.step(5)
+        r.step(STEPS - 5)
+        f = r.gather_fields()
+        pr = r.gather_probe_sums(1)
+        if rank == 0:
+            np.savez(out, fields=f, exchanges=r.exchanges,
+                     **{f"p{k}": np.array([v[0][0], v[1][0], v[2]]) for k, v in pr.items()})
+        r.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_ranks_gloo_host_staging_on_one_gpu(tmp_path, world):
+    """SlabRank in separate processes (gloo, blocks staged through pinned
+    host buffers), every rank's slab on the one GPU: the gathered fields and
+    probe sums equal the whole grid's.  No kernel waits on another rank: the
+    exchange happens on the host between launches."""
+    import torch.multiprocessing as mp
+    out = str(tmp_path / "ranks.npz")
+    mp.start_processes(_rank_main, args=(world, _free_port(), out), nprocs=world,
+                       start_method="spawn", join=True)
+    got = np.load(out)
+    sc = _scene()
+    whole = _whole(sc)
+    try:
+        assert int(got["exchanges"]) == (STEPS - 1) // S.GHOST
+        _eq(got["fields"], whole.fields(), f"fields, {world} ranks")
+        for i in range(len(sc.probes)):
+            c, si, n = whole.probe_sums(i, 1)
+            assert np.array_equal(got[f"p{i}"], np.array([c[0], si[0], n])), i
+    finally:
+        whole.close()

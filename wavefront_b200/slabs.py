@@ -209,7 +209,8 @@ class SlabDomain:
                                        self.stream.cuda_stream, device, arith, kernel)
                        for s in self.slabs]
         n = self.states[0].floats(GHOST) if parts > 1 else 4
-        self._buf = torch.empty(n, dtype=torch.float32, device=f"cuda:{device}")
+        with torch.cuda.stream(self.stream):  # the staging buffer belongs to the slabs' stream
+            self._buf = torch.empty(n, dtype=torch.float32, device=f"cuda:{device}")
         self._since = 0  # steps since the last exchange
         self.exchanges = 0
 
@@ -265,7 +266,13 @@ class SlabRank:
     neighbouring ranks every GHOST steps through batched point-to-point
     sends and receives of packed device buffers; every rank calls step with
     the same n.  `make_state(spec)` builds the slab's state (default: a
-    DeviceSlabState on the current CUDA device and stream)."""
+    DeviceSlabState on the current CUDA device, on a stream of its own that
+    the exchange's copies and communication are ordered on as well).
+
+    With an NCCL group the packed device buffers travel as they are.  With
+    another backend (gloo) a device slab's blocks are staged through pinned
+    host buffers: packed on the device, copied to the host, sent, received,
+    copied back and unpacked, all ordered on the slab's stream."""
 
     def __init__(self, sc, group=None, steps: Optional[int] = None,
                  make_state: Optional[Callable] = None, arith: str = "exact",
@@ -279,42 +286,73 @@ class SlabRank:
         self.slabs = plan(sc.dims.nz, self.world, _pml_z(sc))
         self.slab = self.slabs[self.rank]
         spec = slab_spec(sc, self.slab, steps)
+        self.stream = None
         if make_state is None:
             dev = torch.cuda.current_device()
-            stream = torch.cuda.current_stream(dev).cuda_stream
-            self.state = DeviceSlabState(spec, sc.dims.nz, sc, stream, dev, arith, kernel)
+            self.stream = torch.cuda.Stream(dev)
+            self.state = DeviceSlabState(spec, sc.dims.nz, sc, self.stream.cuda_stream, dev,
+                                         arith, kernel)
             where = torch.device("cuda", dev)
         else:
             self.state = make_state(spec)
             where = torch.device("cpu")
         n = self.state.floats(GHOST)
-        self._bufs = [torch.empty(n, dtype=torch.float32, device=where) for _ in range(4)]
+        with self._on_stream():
+            self._bufs = [torch.empty(n, dtype=torch.float32, device=where) for _ in range(4)]
+        # host staging for a device slab in a group whose backend is not NCCL
+        self._host = None
+        if where.type == "cuda" and dist.get_backend(group) != "nccl":
+            self._host = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(4)]
         self._since = 0
         self.exchanges = 0
+
+    def _on_stream(self):
+        """Makes the slab's stream torch's current stream (a device slab), so
+        that torch copies and NCCL calls are ordered with its kernels."""
+        import contextlib
+        return self._torch.cuda.stream(self.stream) if self.stream is not None \
+            else contextlib.nullcontext()
 
     def _peer(self, r: int) -> int:
         return r if self.group is None else self._dist.get_global_rank(self.group, r)
 
     def exchange(self) -> None:
+        with self._on_stream():
+            self._exchange()
+        self.exchanges += 1
+
+    def _exchange(self) -> None:
         dist, s = self._dist, self.slab
         send_lo, recv_lo, send_hi, recv_hi = self._bufs
-        ops = []
-        if self.rank > 0:
+        wire = self._host or self._bufs  # what travels: device or pinned host buffers
+        lower, upper = self.rank > 0, self.rank < self.world - 1
+        if lower:
             self.state.pack(s.z0 - s.lo, GHOST, send_lo)
-            ops += [dist.P2POp(dist.isend, send_lo, self._peer(self.rank - 1), self.group),
-                    dist.P2POp(dist.irecv, recv_lo, self._peer(self.rank - 1), self.group)]
-        if self.rank < self.world - 1:
+        if upper:
             self.state.pack(s.z1 - GHOST - s.lo, GHOST, send_hi)
-            ops += [dist.P2POp(dist.isend, send_hi, self._peer(self.rank + 1), self.group),
-                    dist.P2POp(dist.irecv, recv_hi, self._peer(self.rank + 1), self.group)]
+        if self._host:  # device -> host on the slab's stream, then wait for it
+            for k, on in ((0, lower), (2, upper)):
+                if on:
+                    wire[k].copy_(self._bufs[k], non_blocking=True)
+            self.stream.synchronize()
+        ops = []
+        if lower:
+            ops += [dist.P2POp(dist.isend, wire[0], self._peer(self.rank - 1), self.group),
+                    dist.P2POp(dist.irecv, wire[1], self._peer(self.rank - 1), self.group)]
+        if upper:
+            ops += [dist.P2POp(dist.isend, wire[2], self._peer(self.rank + 1), self.group),
+                    dist.P2POp(dist.irecv, wire[3], self._peer(self.rank + 1), self.group)]
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
-        if self.rank > 0:
+        if self._host:  # host -> device, ordered before the unpacks on the same stream
+            for k, on in ((1, lower), (3, upper)):
+                if on:
+                    self._bufs[k].copy_(wire[k], non_blocking=True)
+        if lower:
             self.state.unpack(0, GHOST, recv_lo)
-        if self.rank < self.world - 1:
+        if upper:
             self.state.unpack(s.z1 - s.lo, GHOST, recv_hi)
-        self.exchanges += 1
 
     def step(self, n: int = 1) -> None:
         while n > 0:
