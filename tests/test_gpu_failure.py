@@ -1,4 +1,4 @@
-"""GPU: the device timeout path, exercised without a fault.
+"""GPU: failure paths, exercised without a fault.
 
 wf_set_test_stall makes each fused step CTA expect more bytes on its first
 TMA stage than its copies deliver: the copies land, the stage's phase never
@@ -6,6 +6,11 @@ completes, and the kernel's bounded wait (about one second) runs out. The
 step must then report WF_ERR_TIMEOUT at the next sync, within a bounded
 time, and the GPU context must stay usable: a fresh handle on the same device
 steps and matches the oracle bit for bit.
+
+The host-side failures: a grid larger than the device (its cudaMalloc
+fails, which is not a sticky error) must return WF_ERR_OOM with nothing left
+allocated, and a snapshot file whose writes fail (/dev/full) must surface as
+WF_ERR_IO from the writer without stalling it.
 """
 import os
 import time
@@ -70,6 +75,47 @@ def test_stall_argument_checks():
         g.set_test_stall(0)  # off: a normal step
         _configure(g, sc, 2)
         g.step(2)
+        g.sync()
+    finally:
+        g.close()
+
+
+def test_device_allocation_failure_is_reported_and_context_survives():
+    # 4096^3 cells: 1.6 TB per FP32 state buffer, far beyond any GPU
+    with pytest.raises(wf.WfError) as e:
+        wf.DeviceFieldGrid(wf.GridDims(4096, 4096, 4096))
+    assert e.value.status == L.WF_ERR_OOM
+    sc = configs.plain_cube_64(steps=4)
+    g = configs.device_grid(sc)
+    try:
+        _configure(g, sc, 4)
+        g.step(4)
+        g.sync()
+        assert np.abs(g.fields()).max() > 0
+    finally:
+        g.close()
+
+
+def test_snapshot_write_failure_surfaces_as_io_error():
+    if not os.path.exists("/dev/full"):
+        pytest.skip("no /dev/full on this host")
+    sc = configs.plain_cube_64(steps=8)
+    g = configs.device_grid(sc)
+    statuses = []
+    try:
+        _configure(g, sc, 8)
+        w = g.snapshot_writer("/dev/full")
+        try:
+            for _ in range(3):
+                g.step(2)
+                w.capture()
+        except wf.WfError as err:  # a later capture may see the first failure
+            statuses.append(err.status)
+        with pytest.raises(wf.WfError) as e:
+            w.close()
+        statuses.append(e.value.status)
+        assert statuses and all(st == L.WF_ERR_IO for st in statuses)
+        g.step(1)  # the handle keeps working
         g.sync()
     finally:
         g.close()
