@@ -630,6 +630,68 @@ def run_slabs(args, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_slab_ranks(args, rank, world, local_rank):
+    """The workload split into one z slab per rank (SlabRank): each rank
+    steps its slab and exchanges 8-plane ghost blocks with its neighbours
+    every 8 steps (NCCL by default; --backend gloo stages them through pinned
+    host buffers).  Strong scaling: the whole grid is fixed, value counts its
+    cells once over the slowest rank's time."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from wavefront_b200 import slabs as S
+    dev = local_rank % torch.cuda.device_count()
+    torch.cuda.set_device(dev)
+    dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=300))
+    try:
+        total = args.warmup + args.steps
+        sc = scenario(args, total)
+        r = S.SlabRank(sc, steps=total)
+        if args.tiling:
+            r.state.grid.set_tiling(*[int(v) for v in args.tiling.split(",")])
+        r.step(args.warmup)
+        r.stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k_before, x_before = r.state.grid.kernel_launches, r.exchanges
+        dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(dev) as clk:
+            e0.record(r.stream)
+            r.step(args.steps)
+            e1.record(r.stream)
+            r.stream.synchronize()
+            torch.cuda.synchronize()
+        dist.barrier()
+        ms = max_over_ranks(dist, e0.elapsed_time(e1),
+                            device="cuda" if args.backend == "nccl" else "cpu")
+        # this rank's step kernels plus its packs and unpacks (one each per neighbour)
+        nbrs = (rank > 0) + (rank < world - 1)
+        launches = r.state.grid.kernel_launches - k_before + 2 * nbrs * (r.exchanges - x_before)
+        planes = r.slab.nz
+        r.close()
+        value = whole_job_value(1, N_CELLS, args.steps, ms / 1e3)
+        if rank == 0:
+            gpus = min(world, torch.cuda.device_count())  # ranks may share a GPU under gloo
+            line = {
+                "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": gpus,
+                "ranks": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {**scene_config(sc), "slabs": world, "ghost_planes": S.GHOST,
+                           "exchange_every_steps": S.GHOST,
+                           "rank0_planes_stepped_per_step": planes,
+                           "parallelism": f"z slabs x{world}, {args.backend} exchange"},
+                "e2e": {"value": None, "unit": METRIC,
+                        "skipped": "--slabs measures the decomposition"},
+                "gpu_launches": int(launches),
+                "clocks": clk.summary(),
+            }
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -652,6 +714,8 @@ def main():
     ap.add_argument("--slabs", type=int, default=0,
                     help="two_spheres/random_spheres/demo_sphere on one GPU split into this many "
                          "z slabs with ghost-block exchange (FP32)")
+    ap.add_argument("--backend", default="nccl", choices=["nccl", "gloo"],
+                    help="--slabs under torchrun: how ghost blocks travel between ranks")
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
                     help="field storage (16-bit: per-slab power-of-two scales, FP32 math)")
     args = ap.parse_args()
@@ -683,9 +747,14 @@ def main():
     elif args.workload == "closure":
         run_closure(args, rank, world, local_rank)
     elif args.slabs:
-        if world > 1 or PRECISION != "f32":
-            raise SystemExit("--slabs runs on one GPU with FP32 storage")
-        run_slabs(args, local_rank)
+        if PRECISION != "f32":
+            raise SystemExit("--slabs needs FP32 storage")
+        if world > 1:
+            if args.slabs != world:
+                raise SystemExit("under torchrun --slabs must equal the number of ranks")
+            run_slab_ranks(args, rank, world, local_rank)
+        else:
+            run_slabs(args, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 
