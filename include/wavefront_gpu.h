@@ -262,6 +262,11 @@ wf_status wf_get_stream(wf_handle *h, void **out_stream);
  * since timing was enabled. */
 wf_status wf_set_timing(wf_handle *h, int enable);
 wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches);
+/* Steps per captured CUDA graph (even, 2..1024; default 32): wf_step replays
+ * graphs for whole multiples of it and launches the remainder directly, so a
+ * caller that steps in chunks of k (a z slab exchanging ghost blocks every k
+ * steps) sets k.  Drops the graphs captured so far. */
+wf_status wf_set_graph_steps(wf_handle *h, int steps);
 /* Testing aid for the device timeout path (no reference counterpart): while
  * extra_bytes > 0, every fused step kernel's CTAs expect extra_bytes more on
  * their first TMA stage than its copies deliver.  The copies land, the

@@ -194,3 +194,26 @@ def test_slab_ranks_gloo_host_staging_on_one_gpu(tmp_path, world):
             assert np.array_equal(got[f"p{i}"], np.array([c[0], si[0], n])), i
     finally:
         whole.close()
+
+
+def test_graph_steps_change_only_the_launch_grouping():
+    sc = configs.two_spheres(64, steps=50)
+    out = []
+    for gs in (None, 8, 2):
+        g = configs.device_grid(sc)
+        if gs:
+            g.set_graph_steps(gs)
+        for s in sc.sources:
+            g.add_source_values(s.x, s.y, s.z, s.component, s.values(sc.dt, 50), s.mode)
+        g.step(21)
+        g.step(29)
+        g.sync()
+        out.append(g.fields())
+        if gs == 8:
+            for bad in (0, 3, 2048):
+                with pytest.raises(WfError):
+                    g.set_graph_steps(bad)
+        g.close()
+    assert np.abs(out[0]).max() > 0
+    for f in out[1:]:
+        assert np.array_equal(f.view(np.uint32), out[0].view(np.uint32))

@@ -29,6 +29,7 @@ EXPORTS = [
     "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
     "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
     "wf_snapshot_open", "wf_snapshot_capture", "wf_snapshot_close", "wf_set_test_stall",
+    "wf_set_graph_steps",
     "wf_checkpoint_save", "wf_checkpoint_load",
     "wf_set_scene_window", "wf_slab_floats", "wf_slab_pack", "wf_slab_unpack",
     "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
@@ -107,6 +108,8 @@ def lib() -> C.CDLL:
         L.wf_snapshot_close.restype = S
         L.wf_set_test_stall.argtypes = [_h, C.c_int]
         L.wf_set_test_stall.restype = S
+        L.wf_set_graph_steps.argtypes = [_h, C.c_int]
+        L.wf_set_graph_steps.restype = S
         L.wf_checkpoint_save.argtypes = [_h, C.c_char_p]
         L.wf_checkpoint_save.restype = S
         L.wf_checkpoint_load.argtypes = [_h, C.c_char_p]

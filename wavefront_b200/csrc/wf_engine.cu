@@ -1329,6 +1329,17 @@ wf_status wf_get_timing(wf_handle *h, double *total_ms, int64_t *launches) {
   return WF_OK;
 }
 
+wf_status wf_set_graph_steps(wf_handle *h, int steps) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  if (steps < 2 || steps > 1024 || steps % 2)
+    return fail(h, WF_ERR_ARG, "graph steps must be even, in [2, 1024]");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  drop_graphs(h);
+  h->graph_steps = steps;
+  return WF_OK;
+}
+
 wf_status wf_set_test_stall(wf_handle *h, int extra_bytes) {
   if (!h) return fail(h, WF_ERR_ARG, "null handle");
   if (extra_bytes < 0 || extra_bytes > 65536) return fail(h, WF_ERR_ARG, "extra_bytes outside [0, 65536]");

@@ -277,6 +277,10 @@ class DeviceFieldGrid:
         of the current state (wf_slab_unpack)."""
         self._chk(_L.lib().wf_slab_unpack(self._h, z0, nplanes, C.c_void_p(src_ptr)))
 
+    def set_graph_steps(self, steps: int) -> None:
+        """Steps per captured CUDA graph (even, default 32; wf_set_graph_steps)."""
+        self._chk(_L.lib().wf_set_graph_steps(self._h, int(steps)))
+
     def set_test_stall(self, extra_bytes: int) -> None:
         """Testing aid (wf_set_test_stall): makes every fused step's first TMA
         stage wait run out, so the step reports WF_ERR_TIMEOUT at the next

@@ -24,9 +24,9 @@ profile's interior values (b 1, a 0, 1/kappa 1): psi stays exactly +0 there
 and the curl passes through unchanged.  `plan` keeps the real layer off
 every ghost block, so z psi never has to move between slabs.
 
-Transports: `SlabDomain` runs all slabs in one process on one device, one
-CUDA stream, moving ghost blocks with the pack/unpack kernels through a
-device staging buffer; `SlabRank` runs one slab per rank of a
+Transports: `SlabDomain` runs all slabs in one process on one device, each
+on its own CUDA stream, moving ghost blocks with the pack/unpack kernels
+through device staging buffers; `SlabRank` runs one slab per rank of a
 torch.distributed group and moves ghost blocks with batched point-to-point
 sends (NCCL over NVLink between GPUs).  FP32 storage only.
 """
@@ -192,10 +192,17 @@ def _pml_z(sc) -> int:
 
 
 class SlabDomain:
-    """All slabs of a grid in this process on one device and one CUDA stream.
-    step(n) runs every slab in lockstep, exchanging ghost blocks every GHOST
-    steps through the pack/unpack kernels; fields() and probe_sums() read the
-    owning slabs.  Results equal the whole grid's bit for bit."""
+    """All slabs of a grid in this process on one device, each slab on a CUDA
+    stream of its own so that the slabs' steps run concurrently.  step(n)
+    runs every slab in lockstep, exchanging ghost blocks every GHOST steps
+    through the pack/unpack kernels: a block is packed on its owner's stream
+    into a staging buffer of its own, and the receiving slab's stream waits
+    for that before unpacking (and the next pack into the buffer waits for
+    the unpack).  `stream` is the domain's own stream: every step(n) starts
+    after the work already on it and ends with it waiting for every slab, so
+    events recorded on it bracket the domain's work.  fields() and
+    probe_sums() read the owning slabs.  Results equal the whole grid's bit
+    for bit."""
 
     def __init__(self, sc, parts: int, steps: Optional[int] = None, device: int = 0,
                  arith: str = "exact", kernel: str = "auto"):
@@ -205,28 +212,52 @@ class SlabDomain:
         self.slabs = plan(sc.dims.nz, parts, _pml_z(sc))
         self._torch = torch
         self.stream = torch.cuda.Stream(device=device)
+        self.streams = [torch.cuda.Stream(device=device) for _ in self.slabs]
         self.states = [DeviceSlabState(slab_spec(sc, s, steps), sc.dims.nz, sc,
-                                       self.stream.cuda_stream, device, arith, kernel)
-                       for s in self.slabs]
+                                       st.cuda_stream, device, arith, kernel)
+                       for s, st in zip(self.slabs, self.streams)]
+        for s in self.states:
+            s.grid.set_graph_steps(GHOST)  # every step call is one exchange period
         n = self.states[0].floats(GHOST) if parts > 1 else 4
-        with torch.cuda.stream(self.stream):  # the staging buffer belongs to the slabs' stream
-            self._buf = torch.empty(n, dtype=torch.float32, device=f"cuda:{device}")
+        with torch.cuda.stream(self.stream):
+            # per neighbouring pair: [block moving down, block moving up]
+            self._bufs = [[torch.empty(n, dtype=torch.float32, device=f"cuda:{device}")
+                           for _ in range(2)] for _ in range(parts - 1)]
+        self._unpacked = [[None, None] for _ in range(parts - 1)]
         self._since = 0  # steps since the last exchange
         self.exchanges = 0
 
+    def _move(self, pair: int, way: int, src: int, z_src: int, dst: int, z_dst: int) -> None:
+        torch = self._torch
+        buf = self._bufs[pair][way]
+        s_src, s_dst = self.streams[src], self.streams[dst]
+        if self._unpacked[pair][way] is not None:  # the buffer's last unpack is done
+            s_src.wait_event(self._unpacked[pair][way])
+        self.states[src].pack(z_src, GHOST, buf)
+        packed = torch.cuda.Event()
+        packed.record(s_src)
+        s_dst.wait_event(packed)
+        self.states[dst].unpack(z_dst, GHOST, buf)
+        done = torch.cuda.Event()
+        done.record(s_dst)
+        self._unpacked[pair][way] = done
+
     def exchange(self) -> None:
-        """Refreshes every ghost block from its owner (stream-ordered)."""
-        for a, b in zip(self.states, self.states[1:]):
-            sa, sb = a.spec.slab, b.spec.slab
-            # b's lowest owned block -> a's upper ghost block
-            b.pack(sb.z0 - sb.lo, GHOST, self._buf)
-            a.unpack(sa.z1 - sa.lo, GHOST, self._buf)
-            # a's highest owned block -> b's lower ghost block
-            a.pack(sa.z1 - GHOST - sa.lo, GHOST, self._buf)
-            b.unpack(0, GHOST, self._buf)
+        """Refreshes every ghost block from its owner."""
+        for i in range(len(self.states) - 1):
+            sa, sb = self.slabs[i], self.slabs[i + 1]
+            # i+1's lowest owned block -> i's upper ghost block
+            self._move(i, 0, i + 1, sb.z0 - sb.lo, i, sa.z1 - sa.lo)
+            # i's highest owned block -> i+1's lower ghost block
+            self._move(i, 1, i, sa.z1 - GHOST - sa.lo, i + 1, 0)
         self.exchanges += 1
 
     def step(self, n: int = 1) -> None:
+        torch = self._torch
+        start = torch.cuda.Event()
+        start.record(self.stream)
+        for st in self.streams:
+            st.wait_event(start)
         while n > 0:
             if self._since == GHOST:
                 if len(self.states) > 1:
@@ -237,9 +268,15 @@ class SlabDomain:
                 s.step(k)
             self._since += k
             n -= k
+        for st in self.streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            self.stream.wait_event(ev)
 
     def sync(self) -> None:
         self.stream.synchronize()
+        for st in self.streams:
+            st.synchronize()
         for s in self.states:
             s.grid.sync()
 
@@ -255,6 +292,7 @@ class SlabDomain:
         raise IndexError(f"no probe {p}")
 
     def close(self) -> None:
+        self.sync()
         for s in self.states:
             s.close()
         self.states = []
@@ -292,6 +330,7 @@ class SlabRank:
             self.stream = torch.cuda.Stream(dev)
             self.state = DeviceSlabState(spec, sc.dims.nz, sc, self.stream.cuda_stream, dev,
                                          arith, kernel)
+            self.state.grid.set_graph_steps(GHOST)  # every step call is one exchange period
             where = torch.device("cuda", dev)
         else:
             self.state = make_state(spec)
