@@ -393,21 +393,25 @@ wf_status enqueue_one(wf_handle *h) {
     }
     const FusedArgs a = fused_args(h);
     // class 0 (interior) on the main stream, the CPML classes on side
-    // streams forked from it; they touch disjoint cells of the next state
+    // streams forked from it; they touch disjoint cells of the next state.
+    // Launched costliest items first (three axes ... one axis, interior
+    // last), so that the cheap interior items fill the end of the step.
+    static constexpr int kOrder[wf::kFusedClassCount] = {7, 5, 3, 6, 1, 4, 2, 0};
     WF_CUDA(h, cudaEventRecord(h->fork_ev, h->stream));
     e = cudaSuccess;
-    for (int k = 0; k < wf::kFusedClassCount && e == cudaSuccess; ++k) {
+    for (int i = 0; i < wf::kFusedClassCount && e == cudaSuccess; ++i) {
+      const int k = kOrder[i];
       if (h->class_n[k] == 0) continue;
       cudaStream_t s = k == 0 ? h->stream : h->side[k - 1];
       if (k > 0) WF_CUDA(h, cudaStreamWaitEvent(s, h->fork_ev, 0));
       e = wf::launch_fused(h->cfg, h->maps[h->cur], a, h->d_items + h->class_off[k],
                            h->class_n[k], k, fma, s);
       if (e == cudaSuccess) h->kernel_launches += 1;
-      if (e == cudaSuccess && k > 0) {
-        WF_CUDA(h, cudaEventRecord(h->join_ev[k - 1], s));
-        WF_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_ev[k - 1], 0));
-      }
+      if (e == cudaSuccess && k > 0) WF_CUDA(h, cudaEventRecord(h->join_ev[k - 1], s));
     }
+    // the main stream waits for every side class only after all are launched
+    for (int k = 1; k < wf::kFusedClassCount && e == cudaSuccess; ++k)
+      if (h->class_n[k] > 0) WF_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_ev[k - 1], 0));
   } else {
     e = wf::launch_split(g, fma, h->stream);
     if (e == cudaSuccess) h->kernel_launches += 2;  // H pass, E pass
