@@ -619,18 +619,20 @@ wf_status batch_build(wf_batch *b) {
 wf_status batch_kernel(wf_batch *b, int cur) {
   WF_CUDA(nullptr, cudaMemsetAsync(b->d_counter, 0, sizeof(int) * wf::kFusedClassCount, b->stream));
   WF_CUDA(nullptr, cudaEventRecord(b->fork_ev, b->stream));
-  for (int k = 0; k < wf::kFusedClassCount; ++k) {
+  // costliest items first, interior last (as in the single-grid step)
+  static constexpr int kOrder[wf::kFusedClassCount] = {7, 5, 3, 6, 1, 4, 2, 0};
+  for (int i = 0; i < wf::kFusedClassCount; ++i) {
+    const int k = kOrder[i];
     if (!b->class_n[k]) continue;
     cudaStream_t s = k == 0 ? b->stream : b->side[k - 1];
     if (k > 0) WF_CUDA(nullptr, cudaStreamWaitEvent(s, b->fork_ev, 0));
     WF_CUDA(nullptr, wf::launch_fused_batch(b->cfg, b->d_scenes, b->d_items + b->class_off[k],
                                             b->class_n[k], b->d_counter + k, cur,
                                             b->class_ctas[k], k, s));
-    if (k > 0) {
-      WF_CUDA(nullptr, cudaEventRecord(b->join_ev[k - 1], s));
-      WF_CUDA(nullptr, cudaStreamWaitEvent(b->stream, b->join_ev[k - 1], 0));
-    }
+    if (k > 0) WF_CUDA(nullptr, cudaEventRecord(b->join_ev[k - 1], s));
   }
+  for (int k = 1; k < wf::kFusedClassCount; ++k)
+    if (b->class_n[k]) WF_CUDA(nullptr, cudaStreamWaitEvent(b->stream, b->join_ev[k - 1], 0));
   return WF_OK;
 }
 
