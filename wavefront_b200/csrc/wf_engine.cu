@@ -204,7 +204,12 @@ bool encode(CUtensorMap *m, CUtensorMapDataType t, int rank, void *base, const c
 FusedConfig default_cfg(const wf_handle *h) {
   const bool big = h->nz >= 1024;
   if (store16(h)) return FusedConfig{4, big ? 48 : 32, 3};
-  return FusedConfig{4, big ? 24 : 12, 3};
+  // FP32: 24-plane chunks (fewer warm-up planes) while they still give at
+  // least four waves of work items at three CTAs per SM, else 12
+  const long long tiles = static_cast<long long>((h->nx + wf::kTileX - 1) / wf::kTileX) *
+                          ((h->ny + 3) / 4);
+  const long long items24 = tiles * ((h->nz + 23) / 24);
+  return FusedConfig{4, items24 >= 4LL * 148 * 3 ? 24 : 12, 3};
 }
 
 // TMA descriptors per state buffer: fields as a 4D tensor {nx, ny, nz, 6},
