@@ -143,6 +143,13 @@ def test_slab_copies_reject_bad_arguments():
         g.pack_planes(0, 8, buf.data_ptr() + 4)  # not 16-byte aligned
     with pytest.raises(ValueError):
         g.slab_floats(0)
+    text = "sphere 4.0 1.0 0.0 16 16 16 6\n"
+    table = configs.MaterialTable.vacuum_filled(1e-12, 1e-3)
+    for nz_global, off in ((24, 0), (64, 40), (64, -8)):  # window outside the global grid
+        with pytest.raises(WfError):
+            g.set_scene_window(text, table, 1e-12, 1e-3, nz_global, off)
+    g.set_scene_window(text, table, 1e-12, 1e-3, 64, 32)  # planes 32..63: the sphere misses
+    assert not g.materials().any()
     g.close()
 
 
