@@ -8,6 +8,7 @@ other side, where the correction can flip the sign of a zero).  The scenes
 have CPML on every axis, so the x and y psi of the ghost planes move too,
 and sources on ghost planes.
 """
+import datetime
 import os
 import socket
 import sys
@@ -159,7 +160,8 @@ def _rank_main(rank, world, port, out):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     torch.cuda.set_device(0)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
     try:
         r = S.SlabRank(_scene(), steps=STEPS)
         r.step(5)

@@ -6,6 +6,7 @@ counts every rank's cells. The reference arm under torchrun runs on rank 0
 alone and prints one line; the other ranks exit 0 without work.
 """
 import json
+import datetime
 import os
 import socket
 import subprocess
@@ -29,7 +30,8 @@ def _rank_main(rank, world, port, out_dir):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
     try:
         t = bench.max_over_ranks(dist, 1.5 + rank, device="cpu")  # rank r "took" 1.5 + r
         with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:

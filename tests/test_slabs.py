@@ -8,6 +8,7 @@ decomposed run must equal the whole grid's bit for bit.  The device
 transport (pack/unpack kernels, one process) is covered by
 test_gpu_slabs.py.
 """
+import datetime
 import os
 import socket
 import sys
@@ -149,7 +150,8 @@ def _rank_main(rank, world, port, out):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
     try:
         sc = _scenario()
         r = S.SlabRank(sc, make_state=OracleSlabState)
