@@ -215,3 +215,31 @@ def test_two_spheres_plan_keeps_cpml_off_ghosts():
                 ghost = slice(0, s.z0 - s.lo) if s.lo > 0 else slice(s.z1 - s.lo, s.nz)
                 np.testing.assert_array_equal(k[ghost], 1.0)
                 assert t == 16
+
+
+def test_plan_properties_over_random_splits():
+    """Every plan covers [0, nz) with disjoint owned ranges of whole blocks,
+    holds at most GHOST planes beyond them on each inner side, keeps every
+    held range inside the grid, and keeps the z CPML off all ghost blocks."""
+    rng = np.random.default_rng(7)
+    checked = 0
+    for _ in range(400):
+        nz = 8 * int(rng.integers(1, 160))
+        parts = int(rng.integers(1, 12))
+        t = int(rng.choice([0, 8, 10, 16, 32]))
+        try:
+            p = S.plan(nz, parts, pml_z=t)
+        except ValueError:
+            continue
+        checked += 1
+        assert p[0].z0 == 0 and p[-1].z1 == nz
+        for a, b in zip(p, p[1:]):
+            assert a.z1 == b.z0
+        for s in p:
+            assert s.z0 % 8 == 0 and s.z1 % 8 == 0 and s.z1 - s.z0 >= 8
+            assert s.lo == max(s.z0 - S.GHOST, 0) and s.hi == min(s.z1 + S.GHOST, nz)
+            assert 0 <= s.lo and s.hi <= nz and s.nz % 8 == 0
+            if len(p) > 1 and t:
+                for z in list(range(s.lo, s.z0)) + list(range(s.z1, s.hi)):
+                    assert t <= z < nz - t  # a ghost plane is never a real z-CPML plane
+    assert checked > 200
