@@ -280,10 +280,16 @@ def run_batched(args, rank, world, local_rank):
     t0 = time.perf_counter()
     configs.load_batch(b, scenes)
     b.set_tiling(*tiling)
+    b.sync()
+    t_loaded = time.perf_counter()
     b.step(args.steps)
     b.sync()
+    t_stepped = time.perf_counter()
     sums = [b.grid(i).probe_sums(0, 1) for i in range(len(scenes))]
     e2e_s = time.perf_counter() - t0
+    phases = {"upload": round((t_loaded - t0) * 1e3, 1),
+              "steps": round((t_stepped - t_loaded) * 1e3, 1),
+              "probe_sums": round((t0 + e2e_s - t_stepped) * 1e3, 1)}
     b.close()
     e2e_s = max_over_ranks(dist, e2e_s)
     if dist:
@@ -311,7 +317,8 @@ def run_batched(args, rank, world, local_rank):
                     "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h / args.steps),
                     "includes": "every scene's ids + tables uploaded, K steps, every probe's "
-                                "sums read back; the batch's device allocation is untimed set-up"},
+                                "sums read back; the batch's device allocation is untimed set-up",
+                    "phases_ms": phases},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": None, "algorithmic_bytes_per_launch": alg,
