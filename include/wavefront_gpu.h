@@ -246,12 +246,16 @@ wf_status wf_storage_info(wf_handle *h, int *shift_e, int *shift_h, uint64_t *ov
  * components and the x and y CPML psi of those planes) between the current
  * state and a packed device buffer of wf_slab_floats(h, nplanes) floats
  * (16-byte aligned), enqueued on the handle's stream without waiting.
+ * capacity_floats is the buffer's size: a buffer smaller than the planes
+ * need returns WF_ERR_ARG before anything is launched.
  * z CPML psi is not part of a slab: a decomposition keeps the z-CPML planes
  * out of every ghost block.  FP32 storage only (WF_ERR_UNSUPPORTED
  * otherwise).  wf_slab_floats returns -1 for bad arguments. */
 int64_t wf_slab_floats(const wf_handle *h, int nplanes);
-wf_status wf_slab_pack(wf_handle *h, int z0, int nplanes, float *dst_device);
-wf_status wf_slab_unpack(wf_handle *h, int z0, int nplanes, const float *src_device);
+wf_status wf_slab_pack(wf_handle *h, int z0, int nplanes, float *dst_device,
+                       int64_t capacity_floats);
+wf_status wf_slab_unpack(wf_handle *h, int z0, int nplanes, const float *src_device,
+                         int64_t capacity_floats);
 
 /* The handle's CUDA stream (cudaStream_t) for event timing and interop. */
 wf_status wf_get_stream(wf_handle *h, void **out_stream);

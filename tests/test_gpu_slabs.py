@@ -115,8 +115,8 @@ def test_pack_unpack_round_trip_moves_fields_and_psi():
     row_x = ny * ((32 + 3) // 4 * 4)  # x psi: 2 x 16 slab positions per row
     assert n == 6 * 8 * nx * ny + 4 * 8 * row_x + 4 * 8 * 32 * nx
     buf = torch.empty(n, dtype=torch.float32, device="cuda")
-    a.pack_planes(24, 8, buf.data_ptr())
-    b.unpack_planes(8, 8, buf.data_ptr())
+    a.pack_planes(24, 8, buf.data_ptr(), n)
+    b.unpack_planes(8, 8, buf.data_ptr(), n)
     a.sync()
     b.sync()
     fa, fb = a.fields(), b.fields()
@@ -133,15 +133,22 @@ def test_slab_copies_reject_bad_arguments():
     import torch
     g = DeviceFieldGrid(configs.GridDims(32, 32, 32), precision="f16")
     buf = torch.empty(1 << 16, dtype=torch.float32, device="cuda")
+    cap = buf.numel()
     with pytest.raises(WfError) as e:
-        g.pack_planes(0, 8, buf.data_ptr())
+        g.pack_planes(0, 8, buf.data_ptr(), cap)
     assert e.value.status == WF_ERR_UNSUPPORTED
     g.close()
     g = DeviceFieldGrid(configs.GridDims(32, 32, 32))
     with pytest.raises(WfError):
-        g.pack_planes(30, 8, buf.data_ptr())  # past nz
+        g.pack_planes(30, 8, buf.data_ptr(), cap)  # past nz
     with pytest.raises(WfError):
-        g.pack_planes(0, 8, buf.data_ptr() + 4)  # not 16-byte aligned
+        g.pack_planes(0, 8, buf.data_ptr() + 4, cap - 1)  # not 16-byte aligned
+    need = g.slab_floats(8)
+    for bad in (need - 4, 0):  # a buffer smaller than the planes need
+        with pytest.raises(WfError) as e:
+            g.unpack_planes(0, 8, buf.data_ptr(), bad)
+        assert "floats" in str(e.value)
+    g.pack_planes(0, 8, buf.data_ptr(), need)
     with pytest.raises(ValueError):
         g.slab_floats(0)
     text = "sphere 4.0 1.0 0.0 16 16 16 6\n"

@@ -126,9 +126,9 @@ def lib() -> C.CDLL:
         L.wf_set_scene_window.restype = S
         L.wf_slab_floats.argtypes = [_h, C.c_int]
         L.wf_slab_floats.restype = C.c_int64
-        L.wf_slab_pack.argtypes = [_h, C.c_int, C.c_int, C.c_void_p]
+        L.wf_slab_pack.argtypes = [_h, C.c_int, C.c_int, C.c_void_p, C.c_int64]
         L.wf_slab_pack.restype = S
-        L.wf_slab_unpack.argtypes = [_h, C.c_int, C.c_int, C.c_void_p]
+        L.wf_slab_unpack.argtypes = [_h, C.c_int, C.c_int, C.c_void_p, C.c_int64]
         L.wf_slab_unpack.restype = S
         L.wf_batch_create.argtypes = [C.c_int, C.POINTER(GridDesc), C.POINTER(_h)]
         L.wf_batch_create.restype = S

@@ -901,13 +901,18 @@ wf::SlabSegments slab_segments(const wf_handle *h, int z0, int np) {
   return sg;
 }
 
-wf_status slab_copy(wf_handle *h, int z0, int np, float *buf, bool unpack) {
+wf_status slab_copy(wf_handle *h, int z0, int np, float *buf, int64_t capacity, bool unpack) {
   if (!h || !buf) return fail(h, WF_ERR_ARG, "null argument");
   if (store16(h)) return fail(h, WF_ERR_UNSUPPORTED, "slab copies need FP32 storage");
   if (np < 1 || z0 < 0 || z0 > h->nz - np) return fail(h, WF_ERR_ARG, "planes outside the grid");
   if (reinterpret_cast<uintptr_t>(buf) & 15) return fail(h, WF_ERR_ARG, "buffer not 16-byte aligned");
+  const wf::SlabSegments sg = slab_segments(h, z0, np);
+  const long long need = sg.seg[sg.n - 1].off + sg.seg[sg.n - 1].n;
+  if (capacity < need)
+    return fail(h, WF_ERR_ARG, "buffer holds " + std::to_string(capacity) + " floats, the planes need " +
+                                   std::to_string(need));
   DeviceGuard guard(h->dev);
-  WF_CUDA(h, wf::launch_slab_copy(slab_segments(h, z0, np), buf, unpack, h->stream));
+  WF_CUDA(h, wf::launch_slab_copy(sg, buf, unpack, h->stream));
   return WF_OK;
 }
 
@@ -919,12 +924,12 @@ int64_t wf_slab_floats(const wf_handle *h, int nplanes) {
   return sg.seg[sg.n - 1].off + sg.seg[sg.n - 1].n;
 }
 
-wf_status wf_slab_pack(wf_handle *h, int z0, int nplanes, float *dst) {
-  return slab_copy(h, z0, nplanes, dst, false);
+wf_status wf_slab_pack(wf_handle *h, int z0, int nplanes, float *dst, int64_t capacity) {
+  return slab_copy(h, z0, nplanes, dst, capacity, false);
 }
 
-wf_status wf_slab_unpack(wf_handle *h, int z0, int nplanes, const float *src) {
-  return slab_copy(h, z0, nplanes, const_cast<float *>(src), true);
+wf_status wf_slab_unpack(wf_handle *h, int z0, int nplanes, const float *src, int64_t capacity) {
+  return slab_copy(h, z0, nplanes, const_cast<float *>(src), capacity, true);
 }
 
 wf_status wf_get_materials(wf_handle *h, uint8_t *ids) {

@@ -267,15 +267,15 @@ class DeviceFieldGrid:
             raise ValueError(f"bad plane count {nplanes} for nz = {self.dims.nz}")
         return n
 
-    def pack_planes(self, z0: int, nplanes: int, dst_ptr: int) -> None:
+    def pack_planes(self, z0: int, nplanes: int, dst_ptr: int, capacity: int) -> None:
         """Enqueues the copy of planes [z0, z0 + nplanes) of the current state
-        into the device buffer at dst_ptr (wf_slab_pack)."""
-        self._chk(_L.lib().wf_slab_pack(self._h, z0, nplanes, C.c_void_p(dst_ptr)))
+        into the device buffer of `capacity` floats at dst_ptr (wf_slab_pack)."""
+        self._chk(_L.lib().wf_slab_pack(self._h, z0, nplanes, C.c_void_p(dst_ptr), capacity))
 
-    def unpack_planes(self, z0: int, nplanes: int, src_ptr: int) -> None:
-        """Enqueues the copy of a packed buffer into planes [z0, z0 + nplanes)
-        of the current state (wf_slab_unpack)."""
-        self._chk(_L.lib().wf_slab_unpack(self._h, z0, nplanes, C.c_void_p(src_ptr)))
+    def unpack_planes(self, z0: int, nplanes: int, src_ptr: int, capacity: int) -> None:
+        """Enqueues the copy of a packed buffer of `capacity` floats into planes
+        [z0, z0 + nplanes) of the current state (wf_slab_unpack)."""
+        self._chk(_L.lib().wf_slab_unpack(self._h, z0, nplanes, C.c_void_p(src_ptr), capacity))
 
     def set_graph_steps(self, steps: int) -> None:
         """Steps per captured CUDA graph (even, default 32; wf_set_graph_steps)."""

@@ -169,11 +169,19 @@ class DeviceSlabState:
     def floats(self, nplanes: int) -> int:
         return self.grid.slab_floats(nplanes)
 
+    @staticmethod
+    def _device_buffer(t):
+        """(pointer, capacity in floats) of a contiguous float32 CUDA tensor."""
+        import torch
+        if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("slab buffers are contiguous float32 CUDA tensors")
+        return t.data_ptr(), t.numel()
+
     def pack(self, z0: int, nplanes: int, out) -> None:
-        self.grid.pack_planes(z0, nplanes, out.data_ptr())
+        self.grid.pack_planes(z0, nplanes, *self._device_buffer(out))
 
     def unpack(self, z0: int, nplanes: int, src) -> None:
-        self.grid.unpack_planes(z0, nplanes, src.data_ptr())
+        self.grid.unpack_planes(z0, nplanes, *self._device_buffer(src))
 
     def owned_fields(self) -> np.ndarray:
         s = self.spec.slab
