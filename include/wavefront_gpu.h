@@ -238,10 +238,13 @@ wf_status wf_device_fields(wf_handle *h, float **out6);
  * values saturate).  FP32 and bfloat16 storage report 0. */
 wf_status wf_storage_info(wf_handle *h, int *shift_e, int *shift_h, uint64_t *overflows);
 
-/* ---- z-slab decomposition (no reference counterpart) ------------------- */
+/* ---- z-slab decomposition ------------------------------------------------ */
 
-/* A grid split along z runs one handle per slab: the slab's own planes plus
- * a ghost block of neighbouring planes on each inner side.  These copy the
+/* The reference splits its grid into z slabs of whole blocks for threads
+ * that share one address space and read their neighbours' planes in place
+ * (src/engine.rs:8-13, 291-422).  Here a grid split along z runs one handle
+ * per slab: the slab's own planes plus a ghost block of neighbouring planes
+ * on each inner side, refreshed by copies.  These copy the
  * complete stepping state of the planes [z0, z0 + nplanes) (six field
  * components and the x and y CPML psi of those planes) between the current
  * state and a packed device buffer of wf_slab_floats(h, nplanes) floats
