@@ -11,7 +11,6 @@ identity CPML shell equals the run without CPML in every field.
 test_gpu_known_answers.py checks the same on the device.
 """
 import numpy as np
-import pytest
 
 from wavefront_b200 import configs
 
