@@ -67,6 +67,7 @@ def _check(sc, parts, **kw):
         d.step(STEPS - 3)
         assert d.exchanges == (STEPS - 1) // S.GHOST
         _eq(d.fields(), want, f"fields, {parts} slabs")
+        _eq(d.download_blocks(), whole.download_blocks(), f"FieldBlock snapshot, {parts} slabs")
         for i, p in enumerate(sc.probes):
             nf = len(p.frequencies_hz)
             gc, gs, gn = d.probe_sums(i, nf)

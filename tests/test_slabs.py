@@ -142,6 +142,9 @@ class OracleSlabState:
     def probe_sums(self, gi, nfreq):
         return self.sim.probe_sums(self.probe_index[gi], nfreq)
 
+    def owned_blocks(self):
+        return S.owned_block_range(self.sim.blocks(), self.spec)
+
     def close(self):
         self.sim.close()
 
@@ -158,9 +161,10 @@ def _rank_main(rank, world, port, out):
         r.step(5)
         r.step(STEPS - 5)  # the exchange period carries across calls
         f = r.gather_fields()
+        blk = r.gather_blocks()
         pr = r.gather_probe_sums(2)
         if rank == 0:
-            np.savez(out, fields=f, exchanges=r.exchanges,
+            np.savez(out, fields=f, blocks=blk, exchanges=r.exchanges,
                      **{f"p{k}_{i}": v[i] for k, v in pr.items() for i in range(2)},
                      **{f"n{k}": v[2] for k, v in pr.items()})
         r.close()
@@ -195,6 +199,8 @@ def test_gloo_ranks_equal_the_whole_grid(oracle, tmp_path, world):
     assert np.abs(ref).max() > 0
     assert int(got["exchanges"]) == 3
     np.testing.assert_array_equal(got["fields"].view(np.uint32), ref.view(np.uint32))
+    # the snapshot assembled from the slabs' owned block layers is the whole grid's
+    np.testing.assert_array_equal(got["blocks"].view(np.uint32), whole.blocks().view(np.uint32))
     for k, pb in enumerate(sc.probes):
         nf = len(pb.frequencies_hz)
         c, si, n = whole.probe_sums(k, nf)

@@ -190,8 +190,23 @@ class DeviceSlabState:
     def probe_sums(self, global_index: int, nfreq: int):
         return self.grid.probe_sums(self.probe_index[global_index], nfreq)
 
+    def owned_blocks(self) -> np.ndarray:
+        """The owned planes in the reference's FieldBlock order
+        (src/engine.rs:622-640): whole 8-plane block layers, so the slice of
+        the slab's own block stream that the whole grid's stream holds at
+        block layers [z0/8, z1/8)."""
+        return owned_block_range(self.grid.download_blocks(), self.spec)
+
     def close(self) -> None:
         self.grid.close()
+
+
+def owned_block_range(blocks: np.ndarray, spec: "SlabSpec") -> np.ndarray:
+    """The owned block layers of a slab's FieldBlock stream (6 x 512 floats
+    per block, blocks ordered (bz, by, bx))."""
+    d, s = spec.dims, spec.slab
+    per_layer = (d.nx // 8) * (d.ny // 8) * 6 * 512
+    return blocks[(s.z0 - s.lo) // 8 * per_layer:(s.z1 - s.lo) // 8 * per_layer]
 
 
 def _pml_z(sc) -> int:
@@ -298,6 +313,12 @@ class SlabDomain:
             if p in s.probe_index:
                 return s.probe_sums(p, nfreq)
         raise IndexError(f"no probe {p}")
+
+    def download_blocks(self) -> np.ndarray:
+        """The whole grid's snapshot in FieldBlock order: each slab's owned
+        block layers, in slab order (the bytes wave_trajectory.bin holds)."""
+        self.sync()
+        return np.concatenate([s.owned_blocks() for s in self.states])
 
     def close(self) -> None:
         self.sync()
@@ -418,6 +439,14 @@ class SlabRank:
         got = [None] * self.world if self.rank == dst else None
         self._dist.gather_object(part, got, dst=self._peer(dst), group=self.group)
         return np.concatenate(got, axis=1) if self.rank == dst else None
+
+    def gather_blocks(self, dst: int = 0) -> Optional[np.ndarray]:
+        """The whole grid's snapshot in FieldBlock order on rank `dst` (None
+        elsewhere)."""
+        part = self.state.owned_blocks()
+        got = [None] * self.world if self.rank == dst else None
+        self._dist.gather_object(part, got, dst=self._peer(dst), group=self.group)
+        return np.concatenate(got) if self.rank == dst else None
 
     def gather_probe_sums(self, nfreq: int, dst: int = 0) -> Optional[dict]:
         """{global probe index: (cos sums, sin sums, samples)} on rank `dst`."""
