@@ -234,3 +234,29 @@ def test_graph_steps_change_only_the_launch_grouping():
     assert np.abs(out[0]).max() > 0
     for f in out[1:]:
         assert np.array_equal(f.view(np.uint32), out[0].view(np.uint32))
+
+
+def test_slab_domain_checkpoint_resumes_bit_exactly(tmp_path):
+    sc = _scene()
+    ref = S.SlabDomain(sc, 3, steps=STEPS)
+    try:
+        ref.step(STEPS)
+        want, want_blocks = ref.fields(), ref.download_blocks()
+    finally:
+        ref.close()
+    for cut in (24, 29):  # right after an exchange period, and in the middle of one
+        a = S.SlabDomain(sc, 3, steps=STEPS)
+        try:
+            a.step(cut)
+            paths = a.checkpoint(str(tmp_path / f"ck{cut}"))
+        finally:
+            a.close()
+        assert len(paths) == 3
+        b = S.SlabDomain(sc, 3, steps=STEPS)
+        try:
+            b.restore(str(tmp_path / f"ck{cut}"))
+            b.step(STEPS - cut)
+            assert np.array_equal(b.fields().view(np.uint32), want.view(np.uint32))
+            assert np.array_equal(b.download_blocks().view(np.uint32), want_blocks.view(np.uint32))
+        finally:
+            b.close()

@@ -132,6 +132,24 @@ wf_status cuda_fail(wf_handle *h, cudaError_t e, const char *what) {
   return fail(h, s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Host-to-device copies and device memsets of the set-up calls, ordered on
+// the handle's stream and complete on return.  Plain cudaMemcpy from pageable
+// memory may return before its DMA lands and cudaMemset is asynchronous, both
+// on the legacy default stream, which kernels on the handles' non-blocking
+// streams are not ordered after.
+cudaError_t h2d_sync(void *dst, const void *src, size_t bytes, cudaStream_t s,
+                     cudaMemcpyKind kind = cudaMemcpyHostToDevice) {
+  if (bytes == 0) return cudaSuccess;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
+cudaError_t memset_sync(void *dst, int value, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(dst, value, bytes, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
 #define WF_CUDA(h, call)                                \
   do {                                                  \
     cudaError_t e_ = (call);                            \
@@ -257,7 +275,7 @@ wf_status build_maps(wf_handle *h) {
   cudaFree(h->d_items);
   h->d_items = nullptr;
   WF_CUDA(h, cudaMalloc(&h->d_items, sizeof(int) * std::max<size_t>(all.size(), 1)));
-  WF_CUDA(h, cudaMemcpy(h->d_items, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
+  WF_CUDA(h, h2d_sync(h->d_items, all.data(), sizeof(int) * all.size(), h->stream));
   h->maps_ok = true;
   return WF_OK;
 }
@@ -466,13 +484,13 @@ wf_status upload_src_probe_tables(wf_handle *h) {
     std::vector<SrcDev> v;
     for (auto &s : h->srcs) v.push_back(s.d);
     WF_CUDA(h, cudaMalloc(&h->d_src, sizeof(SrcDev) * v.size()));
-    WF_CUDA(h, cudaMemcpy(h->d_src, v.data(), sizeof(SrcDev) * v.size(), cudaMemcpyHostToDevice));
+    WF_CUDA(h, h2d_sync(h->d_src, v.data(), sizeof(SrcDev) * v.size(), h->stream));
   }
   if (!h->probes.empty()) {
     std::vector<ProbeDev> v;
     for (auto &p : h->probes) v.push_back(p.d);
     WF_CUDA(h, cudaMalloc(&h->d_probe, sizeof(ProbeDev) * v.size()));
-    WF_CUDA(h, cudaMemcpy(h->d_probe, v.data(), sizeof(ProbeDev) * v.size(), cudaMemcpyHostToDevice));
+    WF_CUDA(h, h2d_sync(h->d_probe, v.data(), sizeof(ProbeDev) * v.size(), h->stream));
   }
   return WF_OK;
 }
@@ -594,15 +612,12 @@ wf_status batch_build(wf_batch *b) {
     items.insert(items.end(), lists[k].begin(), lists[k].end());
   }
   WF_CUDA(nullptr, cudaMalloc(&b->d_scenes, sizeof(wf::BatchScene) * n));
-  WF_CUDA(nullptr, cudaMemcpy(b->d_scenes, scenes.data(), sizeof(wf::BatchScene) * n,
-                              cudaMemcpyHostToDevice));
+  WF_CUDA(nullptr, h2d_sync(b->d_scenes, scenes.data(), sizeof(wf::BatchScene) * n, b->stream));
   WF_CUDA(nullptr, cudaMalloc(&b->d_items, sizeof(int2) * std::max<size_t>(items.size(), 1)));
-  WF_CUDA(nullptr, cudaMemcpy(b->d_items, items.data(), sizeof(int2) * items.size(),
-                              cudaMemcpyHostToDevice));
+  WF_CUDA(nullptr, h2d_sync(b->d_items, items.data(), sizeof(int2) * items.size(), b->stream));
   for (int p = 0; p < 2; ++p) {
     WF_CUDA(nullptr, cudaMalloc(&b->d_tails[p], sizeof(TailArgs) * n));
-    WF_CUDA(nullptr, cudaMemcpy(b->d_tails[p], tails[p].data(), sizeof(TailArgs) * n,
-                                cudaMemcpyHostToDevice));
+    WF_CUDA(nullptr, h2d_sync(b->d_tails[p], tails[p].data(), sizeof(TailArgs) * n, b->stream));
   }
   b->n_items = static_cast<int>(items.size());
   WF_CUDA(nullptr, wf::fused_batch_prepare(b->cfg));
@@ -975,10 +990,10 @@ wf_status wf_set_pml(wf_handle *h, int axis, int T, const float *b, const float 
     prof[2 * A.W + s] = ik[c];
   }
   WF_CUDA(h, cudaMalloc(&A.prof, sizeof(float) * prof.size()));
-  WF_CUDA(h, cudaMemcpy(A.prof, prof.data(), sizeof(float) * prof.size(), cudaMemcpyHostToDevice));
+  WF_CUDA(h, h2d_sync(A.prof, prof.data(), sizeof(float) * prof.size(), h->stream));
   for (int k = 0; k < 2; ++k) {
     WF_CUDA(h, cudaMalloc(&A.psi[k], sizeof(float) * 4 * A.cells));
-    WF_CUDA(h, cudaMemset(A.psi[k], 0, sizeof(float) * 4 * A.cells));  // PmlAux::ZERO
+    WF_CUDA(h, memset_sync(A.psi[k], 0, sizeof(float) * 4 * A.cells, h->stream));  // PmlAux::ZERO
   }
   return WF_OK;
 }
@@ -996,7 +1011,7 @@ wf_status wf_add_source(wf_handle *h, int x, int y, int z, int comp, int mode,
   SrcRec r{};
   WF_CUDA(h, cudaMalloc(&r.vals, sizeof(float) * std::max(nvalues, 1)));
   if (nvalues > 0)
-    WF_CUDA(h, cudaMemcpy(r.vals, values, sizeof(float) * nvalues, cudaMemcpyHostToDevice));
+    WF_CUDA(h, h2d_sync(r.vals, values, sizeof(float) * nvalues, h->stream));
   r.d.comp = comp;
   r.d.mode = mode;
   r.d.x = x;
@@ -1024,19 +1039,19 @@ wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
   const size_t tab = static_cast<size_t>(nsteps) * nfreq;
   const size_t total = 2 * tab + 2 * static_cast<size_t>(nfreq) + 1;
   WF_CUDA(h, cudaMalloc(&r.base, sizeof(double) * total));
-  WF_CUDA(h, cudaMemset(r.base, 0, sizeof(double) * total));
+  WF_CUDA(h, memset_sync(r.base, 0, sizeof(double) * total, h->stream));
   r.cos_tab = r.base;
   r.sin_tab = r.base + tab;
   r.sc = r.base + 2 * tab;
   r.ss = r.sc + nfreq;
   if (tab) {
-    WF_CUDA(h, cudaMemcpy(r.cos_tab, cos_tab, sizeof(double) * tab, cudaMemcpyHostToDevice));
-    WF_CUDA(h, cudaMemcpy(r.sin_tab, sin_tab, sizeof(double) * tab, cudaMemcpyHostToDevice));
+    WF_CUDA(h, h2d_sync(r.cos_tab, cos_tab, sizeof(double) * tab, h->stream));
+    WF_CUDA(h, h2d_sync(r.sin_tab, sin_tab, sizeof(double) * tab, h->stream));
   }
   WF_CUDA(h, cudaMalloc(&r.n, sizeof(unsigned long long)));
-  WF_CUDA(h, cudaMemset(r.n, 0, sizeof(unsigned long long)));
+  WF_CUDA(h, memset_sync(r.n, 0, sizeof(unsigned long long), h->stream));
   WF_CUDA(h, cudaMalloc(&r.trace, sizeof(float) * std::max(nsteps, 1)));
-  WF_CUDA(h, cudaMemset(r.trace, 0, sizeof(float) * std::max(nsteps, 1)));
+  WF_CUDA(h, memset_sync(r.trace, 0, sizeof(float) * std::max(nsteps, 1), h->stream));
   r.d.comp = comp;
   r.d.x = x;
   r.d.y = y;
@@ -1201,7 +1216,7 @@ wf_status wf_set_fields(wf_handle *h, const float *in6) {
     WF_CUDA(h, cudaStreamSynchronize(h->stream));
     return WF_OK;
   }
-  WF_CUDA(h, cudaMemcpy(h->fld[h->cur], in6, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice));
+  WF_CUDA(h, h2d_sync(h->fld[h->cur], in6, sizeof(float) * 6 * h->N, h->stream));
   return WF_OK;
 }
 
@@ -1450,11 +1465,11 @@ wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) 
   if (st != WF_OK) return st;
   for (auto &A : h->ax)
     for (int k = 0; k < 2; ++k)
-      if (A.psi[k]) WF_CUDA(h, cudaMemset(A.psi[k], 0, sizeof(float) * 4 * A.cells));
-  WF_CUDA(h, cudaMemset(h->d_err, 0, sizeof(int)));
+      if (A.psi[k]) WF_CUDA(h, memset_sync(A.psi[k], 0, sizeof(float) * 4 * A.cells, h->stream));
+  WF_CUDA(h, memset_sync(h->d_err, 0, sizeof(int), h->stream));
   if (store16(h)) {  // the trial steps ran the 16-bit tail: rewind its counters
-    WF_CUDA(h, cudaMemset(h->d_step, 0, sizeof(long long)));
-    WF_CUDA(h, cudaMemset(h->d_ovf, 0, sizeof(unsigned long long)));
+    WF_CUDA(h, memset_sync(h->d_step, 0, sizeof(long long), h->stream));
+    WF_CUDA(h, memset_sync(h->d_ovf, 0, sizeof(unsigned long long), h->stream));
   }
   if (best) {
     best->tile_rows = bc.ty;
@@ -1487,14 +1502,14 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
   const void *src[3] = {w1, w2, w3};
   for (int l = 0; l < 3; ++l) {
     if (!h->cl_w[l]) WF_CUDA(h, cudaMalloc(&h->cl_w[l], 2 * nw[l]));
-    WF_CUDA(h, cudaMemcpy(h->cl_w[l], src[l], 2 * nw[l], cudaMemcpyDefault));
+    WF_CUDA(h, h2d_sync(h->cl_w[l], src[l], 2 * nw[l], h->stream, cudaMemcpyDefault));
   }
   if (!h->cl_buf) {
     const long long P = static_cast<long long>(wf::kBandDepth) * h->nx * h->nx;
     WF_CUDA(h, cudaMalloc(&h->cl_buf, sizeof(float) * (6 * P * (wf::kBandIn + 2 * kClHidden + 6) + 16)));
     const int faces[6] = {0, 1, 2, 3, 4, 5};
     WF_CUDA(h, cudaMalloc(&h->cl_face, sizeof(faces)));
-    WF_CUDA(h, cudaMemcpy(h->cl_face, faces, sizeof(faces), cudaMemcpyHostToDevice));
+    WF_CUDA(h, h2d_sync(h->cl_face, faces, sizeof(faces), h->stream));
   }
   h->cl_ge = gain_e;
   h->cl_gh = gain_h;
@@ -1944,17 +1959,17 @@ wf_status wf_checkpoint_load(wf_handle *h, const char *path) {
       const size_t n = std::min(kCkptChunk, p.bytes - off);
       if (fread(buf.p, 1, n, f.f) != n) return fail(h, WF_ERR_IO, "checkpoint truncated");
       sum.add(buf.p, n);
-      WF_CUDA(h, cudaMemcpy(static_cast<unsigned char *>(p.dev) + off, buf.p, n, cudaMemcpyHostToDevice));
+      WF_CUDA(h, h2d_sync(static_cast<unsigned char *>(p.dev) + off, buf.p, n, h->stream));
     }
   }
   if (sum.v != c.checksum) return fail(h, WF_ERR_IO, "checkpoint checksum mismatch");
   h->steps_done = c.steps_done;
   const long long step = c.steps_done;
-  WF_CUDA(h, cudaMemcpy(h->d_step, &step, sizeof(step), cudaMemcpyHostToDevice));
+  WF_CUDA(h, h2d_sync(h->d_step, &step, sizeof(step), h->stream));
   if (store16(h)) {
     const unsigned long long ovf = c.ovf;
-    WF_CUDA(h, cudaMemcpy(h->d_ovf, &ovf, sizeof(ovf), cudaMemcpyHostToDevice));
-    WF_CUDA(h, cudaMemset(h->slab_max, 0, sizeof(unsigned) * 2 * h->nslab));
+    WF_CUDA(h, h2d_sync(h->d_ovf, &ovf, sizeof(ovf), h->stream));
+    WF_CUDA(h, memset_sync(h->slab_max, 0, sizeof(unsigned) * 2 * h->nslab, h->stream));
     h->shifts_dirty = false;
   }
   return WF_OK;

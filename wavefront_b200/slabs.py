@@ -320,6 +320,28 @@ class SlabDomain:
         self.sync()
         return np.concatenate([s.owned_blocks() for s in self.states])
 
+    def checkpoint(self, prefix: str) -> list:
+        """Saves every slab's complete state (ghost blocks included) to
+        `prefix`.slab<i> (wf_checkpoint_save); returns the paths."""
+        self.sync()
+        paths = [f"{prefix}.slab{i}" for i in range(len(self.states))]
+        for st, path in zip(self.states, paths):
+            st.grid.checkpoint(path)
+        return paths
+
+    def restore(self, prefix: str) -> None:
+        """Loads the slabs saved by checkpoint(prefix) into this domain, which
+        must be set up like the one that saved them.  The exchange phase
+        follows from the step count: an exchange is due before every step
+        whose index is a positive multiple of GHOST."""
+        self.sync()
+        for i, st in enumerate(self.states):
+            st.grid.restore(f"{prefix}.slab{i}")
+        done = self.states[0].grid.steps_done
+        if any(st.grid.steps_done != done for st in self.states):
+            raise ValueError("the slab checkpoints are from different steps")
+        self._since = (done - 1) % GHOST + 1 if done > 0 else 0
+
     def close(self) -> None:
         self.sync()
         for s in self.states:
