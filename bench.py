@@ -592,8 +592,8 @@ def run_ours(args, rank, world, local_rank):
 
 def run_slabs(args, local_rank):
     """The workload split into `--slabs` z slabs on one GPU (SlabDomain: one
-    handle per slab, 8-plane ghost blocks refreshed every 8 steps by the
-    pack/unpack kernels, all on one stream).  value counts the whole grid's
+    handle per slab on a stream of its own, 8-plane ghost blocks refreshed
+    every 8 steps by the pack/unpack kernels).  value counts the whole grid's
     cells once; the ghost planes are the decomposition's extra work."""
     import torch
     from wavefront_b200 import slabs as S

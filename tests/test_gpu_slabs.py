@@ -1,7 +1,8 @@
 """GPU: the z-slab decomposition in one process against the whole grid.
 
-A grid split into 2-4 z slabs (SlabDomain: one handle per slab on one device
-and one stream, ghost blocks moved every 8 steps by the pack/unpack kernels)
+A grid split into 2-4 z slabs (SlabDomain: one handle per slab on one device,
+each on its own stream, ghost blocks moved every 8 steps by the pack/unpack
+kernels)
 must give the whole grid's fields and probe sums, with +0 and -0 treated as
 equal (the slabs holding the z CPML run its interior-valued profile on their
 other side, where the correction can flip the sign of a zero).  The scenes
