@@ -135,15 +135,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(sc, seconds=15.0, seconds_one_core=6.0):
+def cpu_baseline(desc, seconds=15.0, seconds_one_core=6.0):
     """The oracle (C restatement of the reference, AVX2 rows, one worker
     thread per host core splitting each phase into contiguous block ranges
     like the reference's rayon Z-slabs) on a bounded sample: as many full
     steps of the workload as fit in about `seconds`; then the same on one
-    core for about `seconds_one_core`."""
+    core for about `seconds_one_core`.  The oracle builds the workload from
+    its description with its own voxelizer and tables."""
     from oracle import oracle as O
     nt = os.cpu_count() or 1
-    sim = O.sim_from_scenario(sc, steps=128)
+    sim = O.sim_from_description(desc, steps=128)
 
     def timed(threads, budget):
         t0 = time.perf_counter()
@@ -159,31 +160,42 @@ def cpu_baseline(sc, seconds=15.0, seconds_one_core=6.0):
     n, el = timed(nt, seconds)
     n1, el1 = timed(1, seconds_one_core)
     sim.close()
-    cells = sc.dims.voxel_count()
+    nx, ny, nz = desc["dims"]
+    cells = nx * ny * nz
     return {"value": round(cells * n / el / 1e6, 2), "unit": METRIC, "cores": nt,
             "kind": "port", "sample": f"{n} full {GRID}^3 steps after 1 warm-up step, {el:.1f} s",
             "one_core": {"value": round(cells * n1 / el1 / 1e6, 2), "unit": METRIC,
                          "sample": f"the next {n1} steps on 1 thread, {el1:.1f} s"}}
 
 
-def scenario(args, steps, device_voxelize=None):
-    """The workload; random spheres above 256^3 are voxelized on the device
-    (the host voxelizer's 32 full-grid passes take minutes at 1024^3)."""
+def description(args, steps):
+    """The workload as plain data (scene text, grid, dt/dx, CPML request,
+    sources, probes): building it loads no library, so the reference arm
+    can hand it to the oracle alone."""
     from wavefront_b200 import configs
     if args.workload == "random_spheres":
-        dv = GRID > 256 if device_voxelize is None else device_voxelize
-        return configs.random_spheres(n=GRID, steps=steps, device_voxelize=dv)
+        return configs.random_spheres_desc(n=GRID, steps=steps)
     if args.workload == "demo_sphere":
-        return configs.demo_sphere_cube(n=GRID, steps=steps)
-    return configs.two_spheres(n=GRID, steps=steps)
+        return configs.demo_sphere_cube_desc(n=GRID, steps=steps)
+    return configs.two_spheres_desc(n=GRID, steps=steps)
 
 
-def scene_config(sc, precision=None) -> dict:
+def scenario(args, steps, device_voxelize=None):
+    """The workload for the CUDA path; random spheres above 256^3 are
+    voxelized on the device (the host voxelizer's 32 full-grid passes take
+    minutes at 1024^3)."""
+    from wavefront_b200 import configs
+    dv = args.workload == "random_spheres" and (GRID > 256 if device_voxelize is None
+                                                else device_voxelize)
+    return configs.from_desc(description(args, steps), device_voxelize=dv)
+
+
+def scene_config(desc, precision=None) -> dict:
     """The workload keys both arms report (the reference arm stores FP32)."""
     p = precision or PRECISION
     return {"workload": WORKLOAD, "grid": [GRID] * 3,
-            "cpml_cells": sc.pml.thickness_voxels[0] if sc.pml is not None else 0,
-            "probes": len(sc.probes), "storage": p,
+            "cpml_cells": desc["pml"]["cells"] if desc["pml"] is not None else 0,
+            "probes": len(desc["probes"]), "storage": p,
             "l2": f"inputs larger than L2 ({N_CELLS * 6 * ELEM[p] / 1e9:.1f} GB of fields "
                   "per state buffer)"}
 
@@ -191,10 +203,12 @@ def scene_config(sc, precision=None) -> dict:
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    sc = scenario(args, args.warmup + args.steps, device_voxelize=False)
+    # the oracle builds the workload from its plain description with its own
+    # voxelizer and tables: this process never loads the CUDA library
+    desc = description(args, args.warmup + args.steps)
     from oracle import oracle as O
     nt = os.cpu_count() or 1
-    sim = O.sim_from_scenario(sc, steps=args.warmup + args.steps)
+    sim = O.sim_from_description(desc, steps=args.warmup + args.steps)
     budget = float(os.environ.get("WF_REF_SECONDS", "120"))
     for _ in range(args.warmup):
         sim.step(1, nt)
@@ -212,7 +226,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": METRIC,
         "n_gpus": world, "steps": n, "warmup": args.warmup, "ms_per_step": round(el / n * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": scene_config(sc, "f32"),
+        "data": "synthetic", "config": scene_config(desc, "f32"),
         "cpu_baseline": {"value": round(v, 2), "unit": METRIC, "cores": nt, "kind": "port",
                          "sample": f"{n} of {args.steps} requested {GRID}^3 steps in {el:.1f} s "
                                    "(time-bounded); the Rust reference cannot be built here, so "
@@ -454,6 +468,7 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     total = args.warmup + args.steps
+    desc = description(args, total)
     sc = scenario(args, total)
 
     def load(g):
@@ -571,7 +586,7 @@ def run_ours(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {**scene_config(sc), "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
+            "config": {**scene_config(desc), "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
                        "tiling": {"tile_rows": tiling[0], "z_chunk": tiling[1],
                                   "stages": tiling[2]},
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
@@ -584,7 +599,7 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu and sc.grid is not None:
-            line["cpu_baseline"] = cpu_baseline(sc)
+            line["cpu_baseline"] = cpu_baseline(desc)
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -599,6 +614,7 @@ def run_slabs(args, local_rank):
     from wavefront_b200 import slabs as S
     torch.cuda.set_device(local_rank)
     total = args.warmup + args.steps
+    desc = description(args, total)
     sc = scenario(args, total)
     d = S.SlabDomain(sc, args.slabs, steps=total, device=local_rank)
     if args.tiling:
@@ -627,7 +643,7 @@ def run_slabs(args, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {**scene_config(sc), "slabs": args.slabs, "ghost_planes": S.GHOST,
+        "config": {**scene_config(desc), "slabs": args.slabs, "ghost_planes": S.GHOST,
                    "exchange_every_steps": S.GHOST, "planes_stepped_per_step": planes,
                    "parallelism": f"z slabs x{args.slabs} on 1 GPU"},
         "e2e": {"value": None, "unit": METRIC, "skipped": "--slabs measures the decomposition"},
@@ -653,6 +669,7 @@ def run_slab_ranks(args, rank, world, local_rank):
     dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=300))
     try:
         total = args.warmup + args.steps
+        desc = description(args, total)
         sc = scenario(args, total)
         r = S.SlabRank(sc, steps=total)
         if args.tiling:
@@ -685,7 +702,7 @@ def run_slab_ranks(args, rank, world, local_rank):
                 "ranks": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {**scene_config(sc), "slabs": world, "ghost_planes": S.GHOST,
+                "config": {**scene_config(desc), "slabs": world, "ghost_planes": S.GHOST,
                            "exchange_every_steps": S.GHOST,
                            "rank0_planes_stepped_per_step": planes,
                            "parallelism": f"z slabs x{world}, {args.backend} exchange"},

@@ -400,11 +400,17 @@ wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best
  * Allocates nothing: the next-state buffer is a static device array of at
  * most 262144 cells (6 MiB, held by every GPU that loads the library until
  * the process exits); larger grids are rejected with WF_ERR_ARG.  The first
- * call on a device looks up that array's device address (cudaGetSymbolAddress)
- * and should come before any stream capture.  Every call shares the array,
- * so calls that overlap on the GPU (other streams, other threads) race.
- * Results are bit-identical to wf_step on a handle with the same inputs.
- * Errors are described by wf_noalloc_last_error(). */
+ * call on a device (and the first after a new context is made current on it)
+ * looks up that array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  fields6 and ids must be device or managed
+ * memory of the current device: a host pointer or another device's memory is
+ * refused with WF_ERR_ARG before anything is launched.  Each call uploads the
+ * coefficient table from a host array that lives only for the call, so a call
+ * on a stream that is capturing a graph is refused with WF_ERR_UNSUPPORTED.
+ * Every call shares the array, so calls that overlap on the GPU (other
+ * streams, other threads) race.  Results are bit-identical to wf_step on a
+ * handle with the same inputs.  Errors are described by
+ * wf_noalloc_last_error(). */
 wf_status wf_step_fields_noalloc(float *fields6, const uint8_t *ids,
                                  const int32_t (*table_q16)[4], int nx, int ny,
                                  int nz, const int32_t boundary[3], int arith,

@@ -334,6 +334,62 @@ def store16(v: float, kind: str, shift: int) -> float:
     return float(lib().or_store16(v, STORAGE_KINDS[kind], shift, C.byref(ov)))
 
 
+def tables_from_description(d):
+    """Material ids and the Q16.16 table of a workload description (the plain
+    dict of wavefront_b200.configs.*_desc), computed by the oracle alone:
+    scene text through the oracle's voxelizer (src/scene.rs:149-230), the
+    demo sphere through its rasterizer (src/main.rs:403-425), else vacuum."""
+    nx, ny, nz = d["dims"]
+    dt, dx = d["dt"], d["dx"]
+    table = vacuum_table(dt, dx)
+    sc = d["scene"]
+    if sc is not None and "text" in sc:
+        ids, table, _ = scene_voxelize(sc["text"], nx, ny, nz, dt, dx, table)
+    elif sc is not None and "demo_sphere_eps" in sc:
+        ids = demo_sphere(nx, ny, nz)
+        table[1] = material_coeffs(sc["demo_sphere_eps"], 1.0, 0.0, dt, dx)
+    else:
+        ids = np.zeros(nx * ny * nz, np.uint8)
+    return ids, table
+
+
+def pml_thickness_from_description(d):
+    """Graded depth per axis: the reference's whole-block rounding
+    (src/layout.rs:525-533) or, in the exact mode, the request capped at
+    half the axis."""
+    n = d["dims"]
+    p = d["pml"]
+    if p is None:
+        return (0, 0, 0)
+    if p["exact"]:
+        return tuple(min(p["cells"], v // 2) for v in n)
+    t = effective_pml_thickness_blocks(n[0], n[1], n[2], p["cells"]) * 8
+    return (t, t, t)
+
+
+def sim_from_description(d, steps=None, dtype="f32"):
+    """An oracle Sim for a workload description (wavefront_b200.configs.*_desc)
+    built with the oracle's own C code only: ids and table, CPML profiles,
+    source values and probe twiddles.  Nothing here loads the CUDA library."""
+    steps = d["steps"] if steps is None else steps
+    nx, ny, nz = d["dims"]
+    dt, dx = d["dt"], d["dx"]
+    ids, table = tables_from_description(d)
+    sim = Sim(nx, ny, nz, ids, table, (0, 0, 0), dtype)
+    t = pml_thickness_from_description(d)
+    if d["pml"] is not None:
+        sim.set_pml([pml_profile(n, dt, dx, tv) for n, tv in zip((nx, ny, nz), t)],
+                    [(tv + 7) // 8 for tv in t])
+    for s in d["sources"]:
+        sim.add_source(s["x"], s["y"], s["z"], s["comp"],
+                       source_values(s["kind"], s["p0"], s["p1"], s["amp"], dt, steps), s["mode"])
+    for p in d["probes"]:
+        c, si = probe_tables(p["freqs"], dt, steps)
+        sim.add_probe(p["x"], p["y"], p["z"], p["comp"], c, si, steps,
+                      probe_first_step(p["start"], dt))
+    return sim
+
+
 def sim_from_scenario(sc, dtype="f32", periodic=(0, 0, 0), steps=None, storage="f32",
                       arith="exact"):
     """Builds an oracle Sim for a wavefront_b200.configs.Scenario, computing every

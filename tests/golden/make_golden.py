@@ -8,14 +8,17 @@ The reference's example scene scenes/two_spheres.scene is copied too, as a
 scene-format fixture.  They are data, not code, and they pin the oracle (oracle/wf_oracle.c) to the
 reference's arithmetic: the oracle's restated studies must reproduce them.
 
-Run from the repository root with the reference checked out at REF_ROOT
-(default /root/reference).
+Usage: python tests/golden/make_golden.py REF_ROOT
+(or REF_ROOT in the environment), where REF_ROOT is a checkout of the
+reference; there is no default location.
 """
 import os
 import shutil
 import sys
 
-REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+REF_ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT")
+if not REF_ROOT:
+    sys.exit("usage: make_golden.py REF_ROOT (a checkout of the reference)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 for sub, name in (("validation", "convergence_data.csv"),

@@ -91,3 +91,31 @@ def test_ctypes_signatures_match_the_header():
         assert len(fn.argtypes) == arity[name], (name, len(fn.argtypes), arity[name])
         checked += 1
     assert checked >= 40
+
+
+def test_noalloc_argument_errors_before_any_cuda_call():
+    """wf_step_fields_noalloc checks its arguments before touching CUDA: null
+    pointers, dimensions that are not multiples of 8, grids above its static
+    limit, unknown modes and negative step counts are WF_ERR_ARG with a
+    message, on a machine with or without a GPU."""
+    import numpy as np
+    lib = L.lib()
+    q = np.zeros((256, 4), np.int32)
+    b = (C.c_int32 * 3)(0, 0, 0)
+    one = C.c_void_p(16)  # never dereferenced: every case fails before any use
+
+    def call(fields, ids, nx, ny, nz, boundary=b, arith=0, n=1):
+        return lib.wf_step_fields_noalloc(fields, ids, L.ptr(q, L.i32p), nx, ny, nz, boundary,
+                                          arith, n, None)
+
+    assert call(None, one, 8, 8, 8) == L.WF_ERR_ARG
+    assert b"null argument" in lib.wf_noalloc_last_error()
+    assert call(one, None, 8, 8, 8) == L.WF_ERR_ARG
+    assert call(one, one, 12, 8, 8) == L.WF_ERR_ARG
+    assert b"multiples of BLOCK_DIM" in lib.wf_noalloc_last_error()
+    assert call(one, one, 72, 64, 64) == L.WF_ERR_ARG
+    assert b"exceeds the allocation-free limit of 262144 cells" in lib.wf_noalloc_last_error()
+    assert call(one, one, 8, 8, 8, arith=7) == L.WF_ERR_ARG
+    assert call(one, one, 8, 8, 8, n=-1) == L.WF_ERR_ARG
+    assert call(one, one, 8, 8, 8, boundary=(C.c_int32 * 3)(0, 5, 0)) == L.WF_ERR_ARG
+    assert b"unknown boundary kind" in lib.wf_noalloc_last_error()

@@ -68,3 +68,41 @@ def test_reference_arm_under_torchrun_prints_once():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["steps"] == 2 and d["warmup"] == 3
     assert d["e2e"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+
+
+def test_reference_arm_maps_only_the_oracle():
+    """bench.py --impl reference builds the workload with the oracle's own
+    voxelizer and tables: after a run in a fresh process, the CUDA library was
+    never loaded there, and the oracle's shared object was."""
+    code = (
+        "import sys, json; sys.argv=['bench.py','--impl','reference','--grid','64','--steps','2',"
+        "'--warmup','3']; import bench; bench.main();"
+        "import wavefront_b200._lib as L;"
+        "maps=open('/proc/self/maps').read();"
+        "print(json.dumps({'lib': L._lib is None, 'gpu_so': 'libwavefront_gpu.so' in maps,"
+        "'oracle_so': 'libwforacle.so' in maps}))")
+    env = dict(os.environ, WF_REF_SECONDS="5")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert lines[0]["impl"] == "reference"
+    assert lines[-1] == {"lib": True, "gpu_so": False, "oracle_so": True}
+
+
+@pytest.mark.parametrize("which", ["two_spheres", "demo_sphere", "random_spheres"])
+def test_oracle_description_tables_equal_the_products(which):
+    """The oracle's tables built from a workload description (ids, Q16.16
+    table, graded depth per axis) equal those of the Scenario the CUDA path
+    runs, built from the same description by the library's host code."""
+    import numpy as np
+    from oracle import oracle as O
+    from wavefront_b200 import configs
+    desc = {"two_spheres": lambda: configs.two_spheres_desc(n=64, steps=4),
+            "demo_sphere": lambda: configs.demo_sphere_cube_desc(n=64, steps=4),
+            "random_spheres": lambda: configs.random_spheres_desc(n=64, steps=4)}[which]()
+    sc = configs.from_desc(desc)
+    ids, table = O.tables_from_description(desc)
+    assert np.array_equal(ids, sc.grid.ids)
+    assert np.array_equal(table, sc.table.q16)
+    assert O.pml_thickness_from_description(desc) == tuple(sc.pml.thickness_voxels)

@@ -51,22 +51,32 @@ class Scenario:
     scene_text: Optional[str] = None
 
 
-def plain_cube_64(steps: int = 500, pml_cells: int = 10, exact_pml: bool = False,
-                  n: int = 64) -> Scenario:
-    dims = GridDims(n, n, n)
+def _src(x, y, z, kind, freq, comp=2, amp=1.0, mode=0) -> dict:
+    w = default_waveform(kind, freq)
+    return {"x": x, "y": y, "z": z, "comp": comp, "amp": amp, "kind": w.kind, "p0": w.p0,
+            "p1": w.p1, "mode": mode}
+
+
+def _prb(x, y, z, freq, comp=2, start=0.0) -> dict:
+    return {"x": x, "y": y, "z": z, "comp": comp, "freqs": [freq], "start": start}
+
+
+def plain_cube_64_desc(steps: int = 500, pml_cells: int = 10, exact_pml: bool = False,
+                       n: int = 64) -> dict:
+    """Description of plain_cube_64 (plain data: computing it loads no library)."""
     dx = 1.0e-3
     dt = courant_dt(dx)
     f0 = float(np.float32(C0 / (20.0 * dx)))
-    grid = MaterialGrid(dims)
-    table = MaterialTable.vacuum_filled(dt, dx)
-    cfg = PmlConfig(thickness=pml_cells)
-    pml = (PmlContext.build_exact(dims, cfg, dt, dx) if exact_pml
-           else PmlContext.build(dims, cfg, dt, dx)) if pml_cells else None
     c = n // 2
-    src = Source(c, c, c, FieldComponent.Ez, 1.0, default_waveform("ricker", f0))
-    prb = Probe(c + 16, c, c, PC.Ez, [f0], 0.0)
-    return Scenario("plain_cube_64", dims, dx, dt, grid, table, pml, [src], [prb], steps,
-                    {"f0": f0})
+    return {"name": "plain_cube_64", "dims": (n, n, n), "dx": dx, "dt": dt, "scene": None,
+            "pml": {"cells": pml_cells, "exact": exact_pml} if pml_cells else None,
+            "sources": [_src(c, c, c, "ricker", f0)], "probes": [_prb(c + 16, c, c, f0)],
+            "steps": steps, "meta": {"f0": f0}}
+
+
+def plain_cube_64(steps: int = 500, pml_cells: int = 10, exact_pml: bool = False,
+                  n: int = 64) -> Scenario:
+    return from_desc(plain_cube_64_desc(steps, pml_cells, exact_pml, n))
 
 
 def two_spheres_text(n: int) -> str:
@@ -75,20 +85,22 @@ def two_spheres_text(n: int) -> str:
             f"sphere 2.25 1.0 0.0 {352 * s:g} {256 * s:g} {256 * s:g} {60 * s:g}\n")
 
 
-def two_spheres(n: int = 512, steps: int = 1000, pml_cells: int = 16) -> Scenario:
-    dims = GridDims(n, n, n)
+def two_spheres_desc(n: int = 512, steps: int = 1000, pml_cells: int = 16) -> dict:
+    """Description of two_spheres (plain data: computing it loads no library)."""
     dx = 1.0e-3
     dt = courant_dt(dx)
     f = float(np.float32(C0 / (20.0 * dx)))
-    grid = MaterialGrid(dims)
-    table = MaterialTable.vacuum_filled(dt, dx)
-    Scene.parse(two_spheres_text(n)).voxelize(grid, table, dt, dx)
-    pml = PmlContext.build(dims, PmlConfig(thickness=pml_cells), dt, dx) if pml_cells else None
-    src = Source(n // 2, n // 2, n // 8, FieldComponent.Ez, 1.0, default_waveform("gaussian", f))
     zp = (7 * n) // 8
-    probes = [Probe(n // 16 + (n // 8) * k, n // 2, zp, PC.Ez, [f], 0.0) for k in range(8)]
-    return Scenario(f"two_spheres_{n}", dims, dx, dt, grid, table, pml, [src], probes, steps,
-                    {"f": f})
+    return {"name": f"two_spheres_{n}", "dims": (n, n, n), "dx": dx, "dt": dt,
+            "scene": {"text": two_spheres_text(n)},
+            "pml": {"cells": pml_cells, "exact": False} if pml_cells else None,
+            "sources": [_src(n // 2, n // 2, n // 8, "gaussian", f)],
+            "probes": [_prb(n // 16 + (n // 8) * k, n // 2, zp, f) for k in range(8)],
+            "steps": steps, "meta": {"f": f}}
+
+
+def two_spheres(n: int = 512, steps: int = 1000, pml_cells: int = 16) -> Scenario:
+    return from_desc(two_spheres_desc(n, steps, pml_cells))
 
 
 def random_spheres_text(n: int, count: int = 32, seed: int = 1234) -> str:
@@ -106,6 +118,22 @@ def random_spheres_text(n: int, count: int = 32, seed: int = 1234) -> str:
     return "\n".join(lines) + "\n"
 
 
+def random_spheres_desc(n: int = 1024, steps: int = 2000, pml_cells: int = 16,
+                        seed: int = 1234) -> dict:
+    """Description of random_spheres (plain data: computing it loads no library)."""
+    dx = 1.0e-3
+    dt = courant_dt(dx)
+    f = float(np.float32(C0 / (15.0 * dx)))
+    c = n // 2
+    zp = (7 * n) // 8
+    return {"name": f"random_spheres_{n}", "dims": (n, n, n), "dx": dx, "dt": dt,
+            "scene": {"text": random_spheres_text(n, seed=seed)},
+            "pml": {"cells": pml_cells, "exact": False} if pml_cells else None,
+            "sources": [_src(c, c, c, "sinusoid", f)],
+            "probes": [_prb(n // 16 + (n // 8) * k, c, zp, f) for k in range(8)],
+            "steps": steps, "meta": {"f": f, "seed": seed}}
+
+
 def random_spheres(n: int = 1024, steps: int = 2000, pml_cells: int = 16,
                    seed: int = 1234, device_voxelize: bool = False) -> Scenario:
     """Mixed-precision workload: 32 seeded random dielectric spheres, 16-cell
@@ -114,23 +142,54 @@ def random_spheres(n: int = 1024, steps: int = 2000, pml_cells: int = 16,
     scene at n = 128 is small enough for the FP64 oracle.  device_voxelize
     leaves the ids to the device voxelizer (device_grid), which at 1024^3
     takes milliseconds instead of the host's minutes."""
-    dims = GridDims(n, n, n)
-    dx = 1.0e-3
-    dt = courant_dt(dx)
-    f = float(np.float32(C0 / (15.0 * dx)))
+    return from_desc(random_spheres_desc(n, steps, pml_cells, seed),
+                     device_voxelize=device_voxelize)
+
+
+def demo_sphere_cube_desc(n: int = 256, steps: int = 150, pml_cells: int = 8) -> dict:
+    """Description of demo_sphere_cube (plain data: computing it loads no library)."""
+    dx, dt = 1.0e-3, 1.5e-12
+    f = float(np.float32(1.0) / (np.float32(20.0) * np.float32(dt)))
+    return {"name": f"demo_sphere_{n}", "dims": (n, n, n), "dx": dx, "dt": dt,
+            "scene": {"demo_sphere_eps": 4.0},
+            "pml": {"cells": pml_cells, "exact": False} if pml_cells else None,
+            "sources": [_src(n // 2, n // 2, n // 2, "ricker", f)], "probes": [],
+            "steps": steps, "meta": {"f": f}}
+
+
+def demo_sphere_cube(n: int = 256, steps: int = 150, pml_cells: int = 8) -> Scenario:
+    return from_desc(demo_sphere_cube_desc(n, steps, pml_cells))
+
+
+def from_desc(d: dict, device_voxelize: bool = False) -> Scenario:
+    """The Scenario a description stands for, with the library's host code:
+    the scene voxelized (or left to the device voxelizer), the Q16.16 table,
+    the CPML context (rounded to whole blocks like the reference, or exact),
+    the sources and probes."""
+    dims = GridDims(*d["dims"])
+    dx, dt = d["dx"], d["dt"]
     table = MaterialTable.vacuum_filled(dt, dx)
-    text = random_spheres_text(n, seed=seed)
-    grid = None
-    if not device_voxelize:
-        grid = MaterialGrid(dims)
-        Scene.parse(text).voxelize(grid, table, dt, dx)
-    pml = PmlContext.build(dims, PmlConfig(thickness=pml_cells), dt, dx) if pml_cells else None
-    c = n // 2
-    src = Source(c, c, c, FieldComponent.Ez, 1.0, default_waveform("sinusoid", f))
-    zp = (7 * n) // 8
-    probes = [Probe(n // 16 + (n // 8) * k, c, zp, PC.Ez, [f], 0.0) for k in range(8)]
-    return Scenario(f"random_spheres_{n}", dims, dx, dt, grid, table, pml, [src], probes, steps,
-                    {"f": f, "seed": seed}, scene_text=text if device_voxelize else None)
+    grid, text = MaterialGrid(dims), None
+    sc_ = d["scene"]
+    if sc_ is not None and "text" in sc_:
+        if device_voxelize:
+            grid, text = None, sc_["text"]
+        else:
+            Scene.parse(sc_["text"]).voxelize(grid, table, dt, dx)
+    elif sc_ is not None and "demo_sphere_eps" in sc_:
+        demo_sphere(grid)
+        table.set_material(1, sc_["demo_sphere_eps"], 1.0, 0.0, dt, dx)
+    pml = None
+    if d["pml"] is not None:
+        cfg = PmlConfig(thickness=d["pml"]["cells"])
+        pml = (PmlContext.build_exact(dims, cfg, dt, dx) if d["pml"]["exact"]
+               else PmlContext.build(dims, cfg, dt, dx))
+    srcs = [Source(s["x"], s["y"], s["z"], FieldComponent(s["comp"]), s["amp"],
+                   Waveform(s["kind"], s["p0"], s["p1"]), s["mode"]) for s in d["sources"]]
+    prbs = [Probe(p["x"], p["y"], p["z"], PC(p["comp"]), list(p["freqs"]), p["start"])
+            for p in d["probes"]]
+    return Scenario(d["name"], dims, dx, dt, grid, table, pml, srcs, prbs, d["steps"],
+                    dict(d["meta"]), scene_text=text)
 
 
 def batched_sweep(n_scenes: int = 256, steps: int = 800, seed: int = 4321,
@@ -200,19 +259,6 @@ def load_batch(b, scenes: List[Scenario], steps: Optional[int] = None):
             c, si = p_.tables(sc.dt, n)
             g.add_probe_tables(p_.x, p_.y, p_.z, p_.component, c, si, p_.first_step(sc.dt))
     return b
-
-
-def demo_sphere_cube(n: int = 256, steps: int = 150, pml_cells: int = 8) -> Scenario:
-    dims = GridDims(n, n, n)
-    dx, dt = 1.0e-3, 1.5e-12
-    grid = MaterialGrid(dims)
-    demo_sphere(grid)
-    table = MaterialTable.vacuum_filled(dt, dx)
-    table.set_material(1, 4.0, 1.0, 0.0, dt, dx)
-    pml = PmlContext.build(dims, PmlConfig(thickness=pml_cells), dt, dx) if pml_cells else None
-    f = float(np.float32(1.0) / (np.float32(20.0) * np.float32(dt)))
-    src = Source(n // 2, n // 2, n // 2, FieldComponent.Ez, 1.0, default_waveform("ricker", f))
-    return Scenario(f"demo_sphere_{n}", dims, dx, dt, grid, table, pml, [src], [], steps, {"f": f})
 
 
 def device_grid(sc: Scenario, **kw):

@@ -27,9 +27,12 @@ __device__ __align__(256) float g_next_state[6 * kMaxCells];
 __device__ __align__(256) float4 g_coef[256];
 
 // Host-side stand-ins above are not device addresses; their device
-// addresses are looked up once per device, with that device current.
+// addresses are looked up with the device current, once per device and
+// context: a context created anew on the device (after cudaDeviceReset, or
+// another context made current) loads the module again at other addresses,
+// so the lookup is repeated whenever the current context changes.
 struct DeviceScratch {
-  bool ready = false;
+  void *ctx = nullptr;  // the CUcontext the addresses belong to
   float *next_state = nullptr;
   float4 *coef = nullptr;
 };
@@ -43,23 +46,70 @@ wf_status fail(wf_status s, const std::string &msg) {
   return s;
 }
 
-wf_status scratch_for_current_device(DeviceScratch **out) {
+// cuCtxGetCurrent through the runtime's driver entry point (the library
+// links no libcuda).
+using CtxGetCurrentFn = int (*)(void **);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      return reinterpret_cast<CtxGetCurrentFn>(p);
+    return static_cast<CtxGetCurrentFn>(nullptr);
+  }();
+  return fn;
+}
+
+wf_status scratch_for_current_device(int *dev_out, DeviceScratch **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(WF_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return fail(WF_ERR_UNSUPPORTED, "device ordinal above 63");
+  // the context the kernels will run in: the current one, or, when none is
+  // current yet, the device's primary context (cudaSetDevice initialises
+  // and binds it; it allocates nothing)
+  CtxGetCurrentFn get = ctx_get_current();
+  void *ctx = nullptr;
+  if (!get || get(&ctx) != 0) return fail(WF_ERR_CUDA, "cuCtxGetCurrent failed");
+  if (!ctx) {
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return fail(WF_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    if (get(&ctx) != 0 || !ctx) return fail(WF_ERR_CUDA, "no CUDA context on the current device");
+  }
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   DeviceScratch &s = g_scratch[dev];
-  if (!s.ready) {
+  if (s.ctx != ctx) {
+    s.ctx = nullptr;
     e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.next_state), g_next_state);
     if (e != cudaSuccess)
       return fail(WF_ERR_CUDA, std::string("cudaGetSymbolAddress(next state): ") + cudaGetErrorString(e));
     e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.coef), g_coef);
     if (e != cudaSuccess)
       return fail(WF_ERR_CUDA, std::string("cudaGetSymbolAddress(coefficients): ") + cudaGetErrorString(e));
-    s.ready = true;
+    s.ctx = ctx;
   }
+  *dev_out = dev;
   *out = &s;
+  return WF_OK;
+}
+
+// The caller's buffers must be device (or managed) memory that the current
+// device can address: a host pointer handed to the kernels would fault the
+// GPU (or, where the GPU can reach host memory, silently use it).
+wf_status check_device_buffer(const void *p, int dev, const char *what) {
+  cudaPointerAttributes a{};
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear the (non-sticky) error the query recorded
+    return fail(WF_ERR_ARG, std::string(what) + ": not a CUDA allocation (" + cudaGetErrorString(e) + ")");
+  }
+  if (a.type == cudaMemoryTypeManaged) return WF_OK;
+  if (a.type != cudaMemoryTypeDevice)
+    return fail(WF_ERR_ARG, std::string(what) + ": host memory; a device pointer is required");
+  if (a.device != dev)
+    return fail(WF_ERR_ARG, std::string(what) + ": memory of device " + std::to_string(a.device) +
+                                ", but device " + std::to_string(dev) + " is current");
   return WF_OK;
 }
 
@@ -86,10 +136,20 @@ wf_status wf_step_fields_noalloc(float *fields6, const uint8_t *ids,
   for (int i = 0; i < 3; ++i)
     if (boundary[i] != WF_BOUNDARY_ZERO && boundary[i] != WF_BOUNDARY_PERIODIC)
       return fail(WF_ERR_ARG, "unknown boundary kind");
-  DeviceScratch *sc = nullptr;
-  wf_status st = scratch_for_current_device(&sc);
-  if (st != WF_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The coefficient upload below reads a host array that lives only for
+  // this call; a captured graph would replay it from a dead stack frame.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return fail(WF_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(WF_ERR_UNSUPPORTED, "the stream is capturing a graph; call outside stream capture");
+  int dev = -1;
+  DeviceScratch *sc = nullptr;
+  wf_status st = scratch_for_current_device(&dev, &sc);
+  if (st != WF_OK) return st;
+  if ((st = check_device_buffer(fields6, dev, "fields6")) != WF_OK) return st;
+  if ((st = check_device_buffer(ids, dev, "ids")) != WF_OK) return st;
 
   float4 coef[256];
   for (int m = 0; m < 256; ++m)
@@ -98,7 +158,7 @@ wf_status wf_step_fields_noalloc(float *fields6, const uint8_t *ids,
   // The table is rewritten on every call (the array keeps the previous
   // call's contents otherwise).  The next-state array needs no clearing:
   // each step writes every cell of it before anything reads it.
-  cudaError_t e = cudaMemcpyAsync(sc->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, s);
+  e = cudaMemcpyAsync(sc->coef, coef, sizeof(coef), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return fail(WF_ERR_CUDA, std::string("coefficient upload: ") + cudaGetErrorString(e));
 
   wf::GridArgs g{};
