@@ -20,8 +20,11 @@ the handle's stream), `e2e` (through the C ABI from host buffers: upload of
 the scene, K steps, download of probe sums and one snapshot), `roofline`
 (fused kernel: algorithmic bytes per launch / event-timed launch duration),
 `cpu_baseline` (the CPU oracle restating the reference, timed on this host),
-and `clocks` sampled by nvidia-smi during the timed region.  With N > 1 each
-rank runs its own replica of the workload (the path needs no collective).
+and `clocks` sampled by nvidia-smi during the timed region.  With N > 1
+ranks (torchrun) the grid is split into one z slab per rank with 8-plane
+ghost blocks exchanged every 8 steps over NCCL (strong scaling; the value
+counts the whole grid's cells once); --replicas runs an independent copy of
+the workload per rank instead (weak scaling, no collective).
 The reference arm times the reference's CPU algorithm (the oracle port; the
 Rust reference cannot be built here) with all host threads.
 """
@@ -653,50 +656,81 @@ def run_slabs(args, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def run_slab_ranks(args, rank, world, local_rank):
+def run_slab_ranks(args, rank, world, local_rank, make_state=None):
     """The workload split into one z slab per rank (SlabRank): each rank
     steps its slab and exchanges 8-plane ghost blocks with its neighbours
     every 8 steps (NCCL by default; --backend gloo stages them through pinned
     host buffers).  Strong scaling: the whole grid is fixed, value counts its
-    cells once over the slowest rank's time."""
+    cells once over the slowest rank's time.  make_state replaces the device
+    slab (a CPU test drives this leg with oracle slabs over gloo; times are
+    then host clocks)."""
     import datetime
 
     import torch
     import torch.distributed as dist
     from wavefront_b200 import slabs as S
-    dev = local_rank % torch.cuda.device_count()
-    torch.cuda.set_device(dev)
+    gpu = make_state is None
+    dev = 0
+    if gpu:
+        dev = local_rank % torch.cuda.device_count()
+        torch.cuda.set_device(dev)
     dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=300))
+    red = "cuda" if gpu and args.backend == "nccl" else "cpu"
     try:
         total = args.warmup + args.steps
         desc = description(args, total)
         sc = scenario(args, total)
-        r = S.SlabRank(sc, steps=total)
-        if args.tiling:
+
+        def drain(r):
+            if r.stream is not None:
+                r.stream.synchronize()
+
+        r = S.SlabRank(sc, steps=total, make_state=make_state)
+        if args.tiling and gpu:
             r.state.grid.set_tiling(*[int(v) for v in args.tiling.split(",")])
         r.step(args.warmup)
-        r.stream.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        k_before, x_before = r.state.grid.kernel_launches, r.exchanges
+        drain(r)
+        k_before = r.state.grid.kernel_launches if gpu else 0
+        x_before = r.exchanges
         dist.barrier()
-        torch.cuda.synchronize()
-        with ClockSampler(dev) as clk:
-            e0.record(r.stream)
-            r.step(args.steps)
-            e1.record(r.stream)
-            r.stream.synchronize()
+        if gpu:
             torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev) as clk:
+            if gpu:
+                e0.record(r.stream)
+            t0 = time.perf_counter()
+            r.step(args.steps)
+            drain(r)
+            wall_ms = (time.perf_counter() - t0) * 1e3
+            if gpu:
+                e1.record(r.stream)
+                r.stream.synchronize()
+                torch.cuda.synchronize()
         dist.barrier()
-        ms = max_over_ranks(dist, e0.elapsed_time(e1),
-                            device="cuda" if args.backend == "nccl" else "cpu")
+        ms = max_over_ranks(dist, e0.elapsed_time(e1) if gpu else wall_ms, device=red)
         # this rank's step kernels plus its packs and unpacks (one each per neighbour)
         nbrs = (rank > 0) + (rank < world - 1)
-        launches = r.state.grid.kernel_launches - k_before + 2 * nbrs * (r.exchanges - x_before)
+        launches = ((r.state.grid.kernel_launches - k_before) if gpu else 0) + \
+            2 * nbrs * (r.exchanges - x_before)
         planes = r.slab.nz
         r.close()
         value = whole_job_value(1, N_CELLS, args.steps, ms / 1e3)
+
+        # end to end from host buffers: every rank builds its slab (allocation,
+        # ids, tables), steps, and the probe sums are gathered on rank 0
+        dist.barrier()
+        t0 = time.perf_counter()
+        r = S.SlabRank(sc, steps=total, make_state=make_state)
+        r.step(args.steps)
+        drain(r)
+        sums = r.gather_probe_sums(1)
+        e2e_s = max_over_ranks(dist, time.perf_counter() - t0, device=red)
+        r.close()
+        e2e = whole_job_value(1, N_CELLS, args.steps, e2e_s)
         if rank == 0:
-            gpus = min(world, torch.cuda.device_count())  # ranks may share a GPU under gloo
+            gpus = min(world, torch.cuda.device_count()) if gpu else 0  # ranks may share a GPU
+            h2d = N_CELLS + 256 * 16 + total * (4 + 8 * 16)
             line = {
                 "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": gpus,
                 "ranks": world, "steps": args.steps, "warmup": args.warmup,
@@ -706,8 +740,12 @@ def run_slab_ranks(args, rank, world, local_rank):
                            "exchange_every_steps": S.GHOST,
                            "rank0_planes_stepped_per_step": planes,
                            "parallelism": f"z slabs x{world}, {args.backend} exchange"},
-                "e2e": {"value": None, "unit": METRIC,
-                        "skipped": "--slabs measures the decomposition"},
+                "e2e": {"value": round(e2e, 1), "unit": METRIC,
+                        "h2d_bytes_per_step": int(h2d / args.steps),
+                        "d2h_bytes_per_step": int(len(sums or {}) * 24 / args.steps),
+                        "includes": "every rank's slab set-up (handle allocation, ids, CPML and "
+                                    "source/probe tables), K steps with ghost-block exchanges, "
+                                    "probe sums gathered on rank 0"},
                 "gpu_launches": int(launches),
                 "clocks": clk.summary(),
             }
@@ -738,6 +776,9 @@ def main():
     ap.add_argument("--slabs", type=int, default=0,
                     help="two_spheres/random_spheres/demo_sphere on one GPU split into this many "
                          "z slabs with ghost-block exchange (FP32)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="under torchrun: an independent replica of the workload per rank "
+                         "(weak scaling) instead of one z slab per rank")
     ap.add_argument("--backend", default="nccl", choices=["nccl", "gloo"],
                     help="--slabs under torchrun: how ghost blocks travel between ranks")
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"],
@@ -770,11 +811,13 @@ def main():
         run_batched(args, rank, world, local_rank)
     elif args.workload == "closure":
         run_closure(args, rank, world, local_rank)
-    elif args.slabs:
+    elif args.slabs or (world > 1 and not args.replicas and PRECISION == "f32"):
+        # under torchrun the grid is split into one z slab per rank (strong
+        # scaling); --replicas runs an independent copy per rank instead
         if PRECISION != "f32":
             raise SystemExit("--slabs needs FP32 storage")
         if world > 1:
-            if args.slabs != world:
+            if args.slabs and args.slabs != world:
                 raise SystemExit("under torchrun --slabs must equal the number of ranks")
             run_slab_ranks(args, rank, world, local_rank)
         else:

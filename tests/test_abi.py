@@ -119,3 +119,15 @@ def test_noalloc_argument_errors_before_any_cuda_call():
     assert call(one, one, 8, 8, 8, n=-1) == L.WF_ERR_ARG
     assert call(one, one, 8, 8, 8, boundary=(C.c_int32 * 3)(0, 5, 0)) == L.WF_ERR_ARG
     assert b"unknown boundary kind" in lib.wf_noalloc_last_error()
+
+
+def test_rust_sys_crate_declares_the_header():
+    """The Rust -sys crate (source only: no Rust toolchain here) declares
+    every function the header declares, with the header's parameter count."""
+    src = open(os.path.join(ROOT, "wavefront_b200", "bindings", "rust", "wavefront-gpu-sys", "src",
+                            "lib.rs")).read()
+    rust = {}
+    for m in re.finditer(r"pub fn (wf_[a-z0-9_]+)\(([^)]*)\)", src):
+        params = m.group(2).strip()
+        rust[m.group(1)] = 0 if not params else params.count(":")
+    assert rust == _header_arity()

@@ -5,6 +5,7 @@ job's time is the slowest rank's (max over ranks), and the whole-job value
 counts every rank's cells. The reference arm under torchrun runs on rank 0
 alone and prints one line; the other ranks exit 0 without work.
 """
+import argparse
 import json
 import datetime
 import os
@@ -106,3 +107,44 @@ def test_oracle_description_tables_equal_the_products(which):
     assert np.array_equal(ids, sc.grid.ids)
     assert np.array_equal(table, sc.table.q16)
     assert O.pml_thickness_from_description(desc) == tuple(sc.pml.thickness_voxels)
+
+
+def _slab_bench_main(rank, world, port, out_dir):
+    """One rank of bench.py's slab leg (the path `--gpus N` takes under
+    torchrun), with the oracle stepping each slab and gloo moving the ghost
+    blocks; rank 0's JSON line goes to a file."""
+    import contextlib
+    import io
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from test_slabs import OracleSlabState
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK="0")
+    bench.GRID = 64
+    bench.N_CELLS = 64 ** 3
+    args = argparse.Namespace(workload="two_spheres", steps=12, warmup=3, tiling="",
+                              backend="gloo")
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        bench.run_slab_ranks(args, rank, world, 0, make_state=OracleSlabState)
+    with open(os.path.join(out_dir, f"slab{rank}.txt"), "w") as f:
+        f.write(buf.getvalue())
+
+
+def test_bench_slab_leg_two_gloo_ranks(tmp_path):
+    """bench.py's z-slab leg (`--gpus N` under torchrun) with world_size 2:
+    both ranks step their slab, exchange ghost blocks, agree on the slowest
+    rank's time, and rank 0 alone prints one strong-scaling line whose value
+    counts the whole grid's cells once, with an end-to-end figure."""
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_slab_bench_main, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    lines = [l for l in (tmp_path / "slab0.txt").read_text().splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    assert not (tmp_path / "slab1.txt").read_text().strip()
+    d = json.loads(lines[0])
+    assert d["scaling"] == "strong" and d["ranks"] == 2 and d["config"]["slabs"] == 2
+    assert d["steps"] == 12 and d["value"] > 0
+    assert d["value"] == pytest.approx(64 ** 3 * 12 / (d["ms_per_step"] * 12 / 1e3) / 1e6, rel=1e-3)
+    assert d["e2e"]["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] > 0
+    assert d["config"]["rank0_planes_stepped_per_step"] == 32 + 8
