@@ -191,6 +191,17 @@ wf_status wf_set_fields(wf_handle *h, const float *in6);
  * src/engine.rs:622-640): blocks (bz*nby+by)*nbx+bx, each ex..hz x 512. */
 wf_status wf_download_blocks(wf_handle *h, void *out);
 wf_status wf_upload_blocks(wf_handle *h, const void *in);
+/* The same FieldBlock bytes, downloaded while stepping goes on (FP32
+ * storage): the state is reordered on the handle's stream into a staging
+ * buffer of the handle's, and copied to `out` on a copy stream of its own;
+ * the call returns at once.  `out` must stay valid, and should be pinned
+ * host memory for the copy to overlap, until wf_sync returns (wf_sync waits
+ * for the copy).  The reference's writer overlaps its snapshot writes with
+ * stepping the same way (src/engine.rs:617-640, 784-802).  The staging
+ * buffer (24 bytes a voxel) is allocated at the first call, or beforehand by
+ * wf_reserve_download; WF_ERR_UNSUPPORTED for 16-bit storage. */
+wf_status wf_download_blocks_async(wf_handle *h, void *out);
+wf_status wf_reserve_download(wf_handle *h);
 
 /* ---- trajectory snapshots (src/engine.rs:617-640, 688-802) --------------- */
 
@@ -299,6 +310,18 @@ wf_status wf_get_tiling(const wf_handle *h, wf_tiling *out);
 wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t);
 /* Times each candidate tiling for `steps` steps and keeps the fastest. */
 wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms);
+/* Fused-kernel work layout of the x-CPML slabs (no counterpart in the
+ * reference, whose rayon slabs split along z only, src/engine.rs:291-422).
+ * With column tiles on (the default), the two x slabs run as tiles 16 cells
+ * wide and 32 rows tall in which every lane holds graded cells, and the wide
+ * 128-cell tiles cover x in [16, nx-16) with no x-psi work; this applies when
+ * the x CPML is at most 16 cells deep and nx >= 48.  Off: the wide tiles
+ * cover the whole x range and their edge lanes run the x-psi recursion.
+ * Results are bit-identical either way. */
+wf_status wf_set_column_tiles(wf_handle *h, int enable);
+/* 1 when the handle's fused step uses column tiles, 0 otherwise, -1 on a
+ * null handle. */
+int wf_column_tiles_active(const wf_handle *h);
 
 /* ---- learned boundary closure (no reference counterpart) ---------------- */
 
@@ -354,6 +377,15 @@ wf_status wf_nn_gelu_backward(const float *dout, const float *pre, float *dpre, 
 wf_status wf_nn_mse(const float *y, const float *t, float *dy, float *loss, int64_t m, void *stream);
 wf_status wf_nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, int64_t n,
                      float lr, float b1, float b2, float eps, int t, void *stream);
+/* Which kernels run conv3d_forward and conv3d_backward_data (process-wide):
+ * 1 (default) the tensor cores -- tcgen05 implicit GEMMs, 128 voxels x 16
+ * channels per tile, FP32 activations split into two bfloat16 parts so the
+ * operands keep 16 significant bits, FP32 accumulation in tensor memory --
+ * or 0 the FP32 CUDA-core kernels.  The two agree to about 1e-6 relative. */
+wf_status wf_nn_set_tensor_cores(int enable);
+/* Tensor-core convolution tiles whose bounded completion wait ran out
+ * (their outputs were not written); 0 in a healthy run. */
+int64_t wf_nn_tensor_core_timeouts(void);
 
 /* ---- batched stepping (no reference counterpart) ------------------------ */
 

@@ -11,6 +11,8 @@
    of the 16-cell grading) against the same thin layer without it, with the
    plain CPML judging both through the reflection test.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -45,6 +47,68 @@ def test_training_kernels_match_numpy():
     for k in range(3):
         g, go = net.dw[k].cpu().numpy(), dws_o[k]
         assert np.abs(g - go).max() <= 1e-5 * np.abs(go).max(), k
+
+
+@pytest.mark.parametrize("shape", [(2, 10, 16, 8, 6, 7), (3, 16, 16, 8, 37, 65), (6, 16, 6, 8, 9, 33),
+                                   (1, 3, 5, 5, 4, 61)])
+def test_tensor_core_convs_match_the_oracle(shape):
+    """The tcgen05 implicit-GEMM convolutions (forward with GELU and the
+    pre-activation, and the gradient with respect to the input) against the
+    float64 restatement with the same bfloat16 weights, within 1e-5 of the
+    largest magnitude; tile edges in every direction (30-column, 4-row and
+    4-plane tiles), channel counts below 16 and a depth below a tile."""
+    n, ci, co, D, H, W = shape
+    rng = np.random.default_rng(sum(shape))
+    face = (np.arange(n) * 5 % 6).astype(np.int32)
+    x = rng.standard_normal((n, ci, D, H, W)).astype(np.float32)
+    dz = rng.standard_normal((n, co, D, H, W)).astype(np.float32)
+    w = CO.bf16_round((rng.standard_normal((6, co, ci, 27)) * 0.2).astype(np.float32))
+    dev = torch.device("cuda", 0)
+    wb = torch.from_numpy(w.astype(np.float32)).to(dev).to(torch.bfloat16)
+    fx, tf, tdz = (torch.from_numpy(v).to(dev) for v in (x, face, dz))
+    z = torch.empty(n, co, D, H, W, device=dev)
+    a = torch.empty_like(z)
+    din = torch.empty(n, ci, D, H, W, device=dev)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.lib().wf_nn_set_tensor_cores(1) == L.WF_OK
+    L.check(L.lib().wf_nn_conv3d_forward(CL._p(fx), CL._p(wb), CL._p(tf), CL._p(z), CL._p(a),
+                                         n, ci, co, D, H, W, 1, st))
+    L.check(L.lib().wf_nn_conv3d_backward_data(CL._p(tdz), CL._p(wb), CL._p(tf), CL._p(din),
+                                               n, ci, co, D, H, W, st))
+    torch.cuda.synchronize()
+    assert L.lib().wf_nn_tensor_core_timeouts() == 0
+    zo = CO.conv_fwd(x.astype(np.float64), w.astype(np.float64), face)
+    ao = CO.gelu(zo)
+    do = CO.conv_bwd_data(dz.astype(np.float64), w.astype(np.float64), face, ci)
+    for got, want, what in ((z, zo, "pre-activation"), (a, ao, "GELU output"), (din, do, "input gradient")):
+        g = got.cpu().numpy()
+        err = np.abs(g - want).max() / np.abs(want).max()
+        assert err <= 1e-5, (what, err)
+
+
+def test_tensor_core_and_cuda_core_convs_agree():
+    """The two kernel sets behind wf_nn_set_tensor_cores agree to 1e-6 of the
+    largest magnitude on a closure-sized band (6 faces, 10 -> 16 channels)."""
+    rng = np.random.default_rng(3)
+    n, ci, co, D, H, W = 6, 10, 16, 8, 48, 48
+    dev = torch.device("cuda", 0)
+    x = torch.from_numpy(rng.standard_normal((n, ci, D, H, W)).astype(np.float32)).to(dev)
+    wb = (torch.from_numpy(rng.standard_normal((6, co, ci, 27)).astype(np.float32)) * 0.2).to(dev).to(torch.bfloat16)
+    face = torch.arange(6, dtype=torch.int32, device=dev)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    outs = []
+    try:
+        for on in (1, 0):
+            L.lib().wf_nn_set_tensor_cores(on)
+            out = torch.empty(n, co, D, H, W, device=dev)
+            L.check(L.lib().wf_nn_conv3d_forward(CL._p(x), CL._p(wb), CL._p(face), None, CL._p(out),
+                                                 n, ci, co, D, H, W, 1, st))
+            outs.append(out)
+    finally:
+        L.lib().wf_nn_set_tensor_cores(1)
+    torch.cuda.synchronize()
+    err = (outs[0] - outs[1]).abs().max().item() / outs[1].abs().max().item()
+    assert err <= 1e-6, err
 
 
 def test_closure_in_step_equals_explicit_pipeline():

@@ -180,3 +180,42 @@ def test_checkpoint_refuses_other_configurations_and_damage(tmp_path):
     finally:
         for x in (g, other, no_pml):
             x.close()
+
+
+def test_async_download_overlaps_stepping_and_equals_the_oracle():
+    """wf_download_blocks_async: the FieldBlock bytes of the state at the
+    call, copied while later steps run (two downloads in flight order
+    themselves on the staging buffer), equal the oracle's blocks at those
+    steps; 16-bit storage is refused."""
+    import torch
+    sc = configs.two_spheres(n=64, steps=40)
+    sim = O.sim_from_scenario(sc)
+    g = configs.device_grid(sc, kernel="fused")
+    try:
+        for s in sc.sources:
+            g.add_source_values(s.x, s.y, s.z, s.component, s.values(sc.dt, sc.steps))
+        bufs = [torch.empty(sc.dims.voxel_count() * 6, dtype=torch.float32).pin_memory()
+                for _ in range(2)]
+        g.step(3)
+        g.download_blocks_async(bufs[0].numpy())
+        g.step(9)
+        g.download_blocks_async(bufs[1].numpy())
+        g.step(20)
+        g.sync()
+        sim.step(3, NT)
+        want3 = sim.blocks()
+        sim.step(9, NT)
+        want12 = sim.blocks()
+        _eq(bufs[0].numpy(), want3, "download after 3 steps")
+        _eq(bufs[1].numpy(), want12, "download after 12 steps")
+        sim.step(20, NT)
+        _eq(g.fields(), sim.fields(), "fields after the downloads")
+    finally:
+        g.close()
+        sim.close()
+    h = wf.DeviceFieldGrid(wf.GridDims(16, 16, 16), precision="f16")
+    try:
+        with pytest.raises(wf.WfError):
+            h.reserve_download()
+    finally:
+        h.close()

@@ -63,12 +63,24 @@ def cube64(oracle):
     return sc, sim
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split"])
-def test_plain_cube_64_bit_exact(cube64, kernel):
-    """64^3 vacuum, CPML 10 -> 16 cells, Ricker at the centre, 500 steps."""
+@pytest.mark.parametrize("kernel,columns", [("fused", True), ("fused", False), ("split", None)])
+def test_plain_cube_64_bit_exact(cube64, kernel, columns):
+    """64^3 vacuum, CPML 10 -> 16 cells, Ricker at the centre, 500 steps; the
+    fused step with the x-CPML slabs as 16-wide column tiles (the default
+    here) and inside the wide tiles."""
     sc, sim = cube64
-    g = _run_device(sc, kernel=kernel)
+    g = configs.device_grid(sc, kernel=kernel)
     try:
+        if columns is not None:
+            g.set_column_tiles(columns)
+            assert g.column_tiles == columns
+        for s in sc.sources:
+            g.add_source_values(s.x, s.y, s.z, s.component, s.values(sc.dt, sc.steps))
+        for p in sc.probes:
+            c, si = p.tables(sc.dt, sc.steps)
+            g.add_probe_tables(p.x, p.y, p.z, p.component, c, si)
+        g.step(sc.steps)
+        g.sync()
         _compare(g, sim, sc)
         assert g.steps_done == 500
     finally:
@@ -204,8 +216,9 @@ def test_extreme_grid_shapes(oracle, shape):
 
 def test_ragged_grid_materials_h_probes_and_late_start(oracle):
     """nx not a multiple of the 128-cell tile, ny not a multiple of the tile
-    rows, a thin z axis, a lossy scene, several sources and H-component
-    probes with a recording start time."""
+    rows (nor of the 32-row column tiles), a thin z axis, a lossy scene,
+    several sources and H-component probes with a recording start time;
+    fused with and without x-CPML column tiles."""
     dims = wf.GridDims(136, 40, 24)
     dx = 1e-3
     dt = configs.courant_dt(dx)
@@ -223,12 +236,16 @@ def test_ragged_grid_materials_h_probes_and_late_start(oracle):
     sc = configs.Scenario("ragged", dims, dx, dt, grid, table, pml, srcs, prbs, 200)
     sim = oracle.sim_from_scenario(sc)
     sim.step(sc.steps, NT)
-    for kernel, tiling in (("fused", (8, 64, 3)), ("fused", (16, 10, 3)),
-                           ("fused", (4, 10, 4)), ("fused", (8, 24, 4)), ("split", None)):
+    for kernel, tiling, cols in (("fused", (8, 64, 3), True), ("fused", (16, 10, 3), True),
+                                 ("fused", (4, 10, 4), True), ("fused", (8, 24, 4), True),
+                                 ("fused", (4, 10, 3), False), ("split", None, None)):
         g = configs.device_grid(sc, kernel=kernel)
         try:
             if tiling:
                 g.set_tiling(*tiling)
+            if cols is not None:
+                g.set_column_tiles(cols)
+                assert g.column_tiles == cols  # 8-cell x CPML, nx 136: columns apply
             for s in srcs:
                 g.add_source_values(s.x, s.y, s.z, s.component, s.values(dt, sc.steps))
             for p in prbs:

@@ -9,7 +9,10 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libwavefront_gpu.so")
+# WF_BOUNDS_CHECK=1 loads the bounds-checked variant (device index checks
+# that latch an error flag reported by wf_sync as WF_ERR_DEVICE_FLAG)
+LIB_PATH = os.path.join(HERE, "lib", "libwavefront_gpu_checked.so"
+                        if os.environ.get("WF_BOUNDS_CHECK") == "1" else "libwavefront_gpu.so")
 
 WF_OK, WF_ERR_ARG, WF_ERR_CUDA, WF_ERR_OOM, WF_ERR_TIMEOUT, WF_ERR_DEVICE_FLAG, \
     WF_ERR_STATE, WF_ERR_UNSUPPORTED, WF_ERR_IO = range(9)
@@ -25,14 +28,17 @@ EXPORTS = [
     "wf_set_closure", "wf_set_closure_guard", "wf_band_gather", "wf_band_scatter_add",
     "wf_restrict_state",
     "wf_nn_conv3d_forward", "wf_nn_conv3d_backward_data", "wf_nn_conv3d_backward_weight",
-    "wf_nn_gelu_backward", "wf_nn_mse", "wf_nn_adam",
+    "wf_nn_gelu_backward", "wf_nn_mse", "wf_nn_adam", "wf_nn_set_tensor_cores",
+    "wf_nn_tensor_core_timeouts",
     "wf_probe_sums", "wf_probe_trace", "wf_get_fields", "wf_set_fields",
-    "wf_download_blocks", "wf_upload_blocks", "wf_get_psi", "wf_device_fields",
+    "wf_download_blocks", "wf_upload_blocks", "wf_download_blocks_async", "wf_reserve_download",
+    "wf_get_psi", "wf_device_fields",
     "wf_snapshot_open", "wf_snapshot_capture", "wf_snapshot_close", "wf_set_test_stall",
     "wf_set_graph_steps",
     "wf_checkpoint_save", "wf_checkpoint_load",
     "wf_set_scene_window", "wf_slab_floats", "wf_slab_pack", "wf_slab_unpack",
-    "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune", "wf_q16_from_f32", "wf_q16_to_f32",
+    "wf_get_stream", "wf_set_timing", "wf_get_timing", "wf_get_tiling", "wf_set_tiling", "wf_autotune",
+    "wf_set_column_tiles", "wf_column_tiles_active", "wf_q16_from_f32", "wf_q16_to_f32",
     "wf_material_coeffs", "wf_effective_pml_thickness_blocks", "wf_pml_profile",
     "wf_waveform_eval", "wf_source_values", "wf_probe_first_step", "wf_probe_tables",
     "wf_spectrum", "wf_scene_voxelize", "wf_demo_sphere",
@@ -165,6 +171,10 @@ def lib() -> C.CDLL:
         L.wf_nn_mse.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
         L.wf_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float,
                                  C.c_float, C.c_int, vp]
+        L.wf_nn_set_tensor_cores.argtypes = [C.c_int]
+        L.wf_nn_set_tensor_cores.restype = S
+        L.wf_nn_tensor_core_timeouts.argtypes = []
+        L.wf_nn_tensor_core_timeouts.restype = C.c_int64
         for name in ("wf_set_closure", "wf_set_closure_guard", "wf_band_gather", "wf_band_scatter_add", "wf_restrict_state",
                      "wf_nn_conv3d_forward", "wf_nn_conv3d_backward_data",
                      "wf_nn_conv3d_backward_weight", "wf_nn_gelu_backward", "wf_nn_mse",
@@ -182,6 +192,10 @@ def lib() -> C.CDLL:
         L.wf_download_blocks.restype = S
         L.wf_upload_blocks.argtypes = [_h, C.c_void_p]
         L.wf_upload_blocks.restype = S
+        L.wf_download_blocks_async.argtypes = [_h, C.c_void_p]
+        L.wf_download_blocks_async.restype = S
+        L.wf_reserve_download.argtypes = [_h]
+        L.wf_reserve_download.restype = S
         L.wf_get_psi.argtypes = [_h, C.c_int, _f32p]
         L.wf_get_psi.restype = S
         L.wf_device_fields.argtypes = [_h, C.POINTER(C.c_void_p)]
@@ -198,6 +212,10 @@ def lib() -> C.CDLL:
         L.wf_set_tiling.restype = S
         L.wf_autotune.argtypes = [_h, C.c_int, C.POINTER(Tiling), _f32p]
         L.wf_autotune.restype = S
+        L.wf_set_column_tiles.argtypes = [_h, C.c_int]
+        L.wf_set_column_tiles.restype = S
+        L.wf_column_tiles_active.argtypes = [_h]
+        L.wf_column_tiles_active.restype = C.c_int
         L.wf_q16_from_f32.argtypes = [C.c_float]
         L.wf_q16_from_f32.restype = C.c_int32
         L.wf_q16_to_f32.argtypes = [C.c_int32]

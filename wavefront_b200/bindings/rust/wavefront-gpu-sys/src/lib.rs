@@ -100,6 +100,8 @@ extern "C" {
     pub fn wf_set_fields(h: *mut wf_handle, in6: *const f32) -> wf_status;
     pub fn wf_download_blocks(h: *mut wf_handle, out: *mut c_void) -> wf_status;
     pub fn wf_upload_blocks(h: *mut wf_handle, in_: *const c_void) -> wf_status;
+    pub fn wf_download_blocks_async(h: *mut wf_handle, out: *mut c_void) -> wf_status;
+    pub fn wf_reserve_download(h: *mut wf_handle) -> wf_status;
     pub fn wf_snapshot_open(h: *mut wf_handle, path: *const c_char, out: *mut *mut wf_snapshot_writer) -> wf_status;
     pub fn wf_snapshot_capture(w: *mut wf_snapshot_writer) -> wf_status;
     pub fn wf_snapshot_close(w: *mut wf_snapshot_writer, bytes_written: *mut u64) -> wf_status;

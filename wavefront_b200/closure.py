@@ -222,13 +222,24 @@ def truncated_profiles(n: int, dt: float, dx: float):
     return out
 
 
-def set_thin_cpml(grid: DeviceFieldGrid, dt: float, dx: float):
+def graded_profiles(n: int, dt: float, dx: float):
+    """The plain thin CPML: a THIN-cell layer graded over its own THIN cells
+    (PmlContext::build's grading, src/layout.rs:471-513, per cell)."""
+    ctx = PmlContext.build_exact(GridDims(n, n, n), PmlConfig(thickness=THIN), dt, dx)
+    return [tuple(np.ascontiguousarray(v, np.float32) for v in (p.b, p.a, p.inv_kappa))
+            for p in ctx.profiles]
+
+
+def set_thin_cpml(grid: DeviceFieldGrid, dt: float, dx: float, profile: str = "truncated"):
+    """The thin layer on every face: "truncated" (the innermost THIN cells of
+    the THICK grading) or "graded" (a plain THIN-cell CPML)."""
     n = grid.dims.nx
-    for ax, (b, a, ik) in enumerate(truncated_profiles(n, dt, dx)):
+    profs = truncated_profiles(n, dt, dx) if profile == "truncated" else graded_profiles(n, dt, dx)
+    for ax, (b, a, ik) in enumerate(profs):
         grid.set_pml_axis(ax, THIN, b, a, ik)
 
 
-def _grids(run: Run, dx: float, dt: float, steps: int, device: int):
+def _grids(run: Run, dx: float, dt: float, steps: int, device: int, profile: str = "truncated"):
     tdims, sdims = GridDims(TEACHER_N, TEACHER_N, TEACHER_N), GridDims(STUDENT_N, STUDENT_N, STUDENT_N)
     tgrid = MaterialGrid(tdims)
     table = MaterialTable.vacuum_filled(dt, dx)
@@ -247,14 +258,14 @@ def _grids(run: Run, dx: float, dt: float, steps: int, device: int):
     for _ in range(2):
         st = DeviceFieldGrid(sdims, kernel="fused", device=device)
         st.set_materials(sgrid, table)
-        set_thin_cpml(st, dt, dx)
+        set_thin_cpml(st, dt, dx, profile)
         students.append(st)
     return teacher, students
 
 
 def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, crop: int = 16,
              seed: int = 1, device: int = 0, net: Optional["ClosureNet"] = None, max_lead: int = 12,
-             guard: bool = False):
+             guard: bool = False, profile: str = "truncated"):
     """Teacher-forced one-step samples: returns (X [M][10][8][c][c],
     R [M][6][8][c][c], face [M] int32, 1.0) on the device.  H-side values
     are times ETA0, and every sample is divided by the RMS of the E channels
@@ -266,7 +277,8 @@ def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, cr
     (the last of them without the closure, whose input is the sample): the
     target is the teacher's state at the same time, so the network also
     learns to pull a drifting student back (a DAgger-style round).  guard
-    runs those closure steps with the energy guard on."""
+    runs those closure steps with the energy guard on.  profile is the
+    student's thin layer (set_thin_cpml)."""
     torch = _torch()
     dev = torch.device("cuda", device)
     rng = np.random.default_rng(seed)
@@ -278,7 +290,7 @@ def generate(n_runs: int, steps: int = 160, first: int = 30, every: int = 10, cr
     xs, rs, fs = [], [], []
     for _ in range(n_runs):
         run = random_run(rng, dx)
-        teacher, (s1, s2) = _grids(run, dx, dt, steps + 1, device)
+        teacher, (s1, s2) = _grids(run, dx, dt, steps + 1, device, profile)
         try:
             done = 0
             for k in range(first, steps, every):

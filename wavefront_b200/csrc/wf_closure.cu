@@ -412,9 +412,17 @@ inline unsigned blocks_for(long long n, int t) { return static_cast<unsigned>((n
 
 }  // namespace
 
+// Which kernels run the forward and input-gradient convolutions: the
+// tensor-core implicit GEMMs (wf_conv_tc.cu, the default) or the CUDA-core
+// kernels above.
+static int g_nn_tensor_cores = 1;
+void nn_set_tensor_cores(int on) { g_nn_tensor_cores = on != 0; }
+int nn_tensor_cores() { return g_nn_tensor_cores; }
+
 int nn_conv_fwd(const float *in, const void *w_bf16, const int *face, float *z, float *a, int n,
                 int ci, int co, int D, int H, int W, int act, void *stream) {
   if (ci > kMaxC || co > kMaxC || ci < 1 || co < 1 || n < 1) return cudaErrorInvalidValue;
+  if (g_nn_tensor_cores) return nn_conv_fwd_tc(in, w_bf16, face, z, a, n, ci, co, D, H, W, act, stream);
   const long long P = static_cast<long long>(D) * H * W;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const __nv_bfloat16 *wb = static_cast<const __nv_bfloat16 *>(w_bf16);
@@ -437,6 +445,7 @@ int nn_conv_fwd(const float *in, const void *w_bf16, const int *face, float *z, 
 int nn_conv_bwd_data(const float *dz, const void *w_bf16, const int *face, float *din, int n,
                      int ci, int co, int D, int H, int W, void *stream) {
   if (ci > kMaxC || co > kMaxC || ci < 1 || co < 1 || n < 1) return cudaErrorInvalidValue;
+  if (g_nn_tensor_cores) return nn_conv_bwd_data_tc(dz, w_bf16, face, din, n, ci, co, D, H, W, stream);
   const long long P = static_cast<long long>(D) * H * W;
   dim3 grid(blocks_for(P, 128), n);
   k_conv_bwd_data<<<grid, 128, sizeof(float) * co * ci * kTaps, static_cast<cudaStream_t>(stream)>>>(

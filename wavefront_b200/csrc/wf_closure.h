@@ -32,6 +32,16 @@ int nn_conv_bwd_data(const float *dz, const void *w_bf16, const int *face, float
 int nn_conv_bwd_weight(const float *in, const float *dz, const int *face, float *dw, int n, int ci,
                        int co, int D, int H, int W, int nface, void *stream);
 int nn_gelu_bwd(const float *da, const float *z, float *dz, long long m, void *stream);
+// The same forward and input-gradient convolutions on the tensor cores
+// (tcgen05 implicit GEMMs, wf_conv_tc.cu); nn_conv_fwd / nn_conv_bwd_data
+// dispatch to them unless nn_set_tensor_cores(0).
+int nn_conv_fwd_tc(const float *in, const void *w_bf16, const int *face, float *z, float *a, int n,
+                   int ci, int co, int D, int H, int W, int act, void *stream);
+int nn_conv_bwd_data_tc(const float *dz, const void *w_bf16, const int *face, float *din, int n,
+                        int ci, int co, int D, int H, int W, void *stream);
+void nn_set_tensor_cores(int on);
+int nn_tensor_cores();
+unsigned long long nn_tc_timeouts();
 int nn_mse(const float *y, const float *t, float *dy, float *loss, long long m, void *stream);
 int nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, long long n, float lr,
             float b1, float b2, float eps, int t, void *stream);

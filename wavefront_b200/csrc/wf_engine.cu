@@ -110,7 +110,22 @@ struct wf_handle {
   // stream onto these streams and joined back before the step tail
   cudaStream_t side[wf::kFusedClassCount - 1] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[wf::kFusedClassCount - 1] = {};
+  // x-CPML column tiles (wf_set_column_tiles): whether they are in use, the
+  // caller's preference, their maps, work lists and streams
+  bool cols = false;
+  bool col_pref = true;
+  wf::FusedMaps col_maps[2];
+  int col_off[wf::kColClassCount] = {}, col_n[wf::kColClassCount] = {};
+  cudaStream_t side_col[wf::kColClassCount] = {};
+  cudaEvent_t join_col[wf::kColClassCount] = {};
   bool maps_ok = false;
+  // asynchronous FieldBlock download (wf_download_blocks_async): a staging
+  // buffer the state is reordered into on the handle's stream, copied to the
+  // host on a stream of its own while stepping goes on
+  float *d_stage = nullptr;
+  cudaStream_t copy = nullptr;
+  cudaEvent_t staged = nullptr, copied = nullptr;
+  bool copy_pending = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graph_steps = 0;
   bool timing = false;
@@ -205,6 +220,17 @@ bool use_fused(const wf_handle *h) {
 
 bool has_pml(const wf_handle *h) { return h->ax[0].T > 0 || h->ax[1].T > 0 || h->ax[2].T > 0; }
 FusedArgs fused_args(const wf_handle *h);
+FusedArgs col_args(const wf_handle *h);
+
+// The x-CPML slabs run as 16-wide column tiles when each is at most 16
+// cells deep and the grid leaves a wide region of at least 16 cells.
+bool cols_apply(const wf_handle *h) {
+  const int T = h->ax[0].T;
+  return h->col_pref && T > 0 && T <= wf::kColWidth && h->nx >= 3 * wf::kColWidth;
+}
+
+// Column-class index (0..3) of CPML class 1, 3, 5, 7.
+constexpr int col_slot(int ax) { return ax >> 1; }
 
 // One tiled TMA descriptor (no swizzle, no interleave, zero out-of-bounds fill).
 bool encode(CUtensorMap *m, CUtensorMapDataType t, int rank, void *base, const cuuint64_t *dims,
@@ -233,10 +259,11 @@ FusedConfig default_cfg(const wf_handle *h) {
 // TMA descriptors per state buffer: fields as a 4D tensor {nx, ny, nz, 6},
 // ids as {nx, ny, nz} with a 16-byte-multiple row pitch, and each CPML
 // axis's psi slab as a 4D tensor {.., .., .., 4 terms}.
-wf_status build_maps(wf_handle *h) {
+wf_status build_maps(wf_handle *h, bool allow_cols = true) {
   h->maps_ok = false;
   if (!encode_fn()) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   if (!h->cfg_user_set) h->cfg = default_cfg(h);
+  h->cols = allow_cols && cols_apply(h);
   unsigned eb[4], hb[4], mb[3];
   wf::fused_boxes(h->cfg.ty, h->precision, eb, hb, mb);
   const cuuint64_t es = elem_bytes(h);
@@ -260,6 +287,21 @@ wf_status build_maps(wf_handle *h) {
       return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(fields/ids) failed");
   }
   WF_CUDA(h, wf::fused_prepare(h->cfg, h->precision));
+  if (h->cols) {
+    wf::fused_col_boxes(h->precision, eb, hb, mb);
+    const cuuint32_t cebox[4] = {eb[0], eb[1], eb[2], eb[3]};
+    const cuuint32_t chbox[4] = {hb[0], hb[1], hb[2], hb[3]};
+    const cuuint32_t cmbox[3] = {mb[0], mb[1], mb[2]};
+    for (int b = 0; b < 2; ++b) {
+      wf::FusedMaps &m = h->col_maps[b];
+      std::memset(&m, 0, sizeof(m));
+      if (!encode(&m.e, ft, 4, h->fld[b], fdim, fstr, cebox) ||
+          !encode(&m.h, ft, 4, h->fld[b], fdim, fstr, chbox) ||
+          !encode(&m.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->mat, mdim, mstr, cmbox))
+        return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(column tiles) failed");
+    }
+    WF_CUDA(h, wf::fused_col_prepare(h->precision));
+  }
   // Work lists, one per kernel class (interior first): each class runs the
   // kernel instantiation that carries only the CPML code it needs.
   const FusedArgs a = fused_args(h);
@@ -271,6 +313,18 @@ wf_status build_maps(wf_handle *h) {
     h->class_off[k] = static_cast<int>(all.size());
     h->class_n[k] = static_cast<int>(lists[k].size());
     all.insert(all.end(), lists[k].begin(), lists[k].end());
+  }
+  // column items (low and high x edge, 32-row tiles), one list per class
+  std::vector<int> clists[wf::kColClassCount];
+  if (h->cols) {
+    const FusedArgs c = col_args(h);
+    const int nc = c.tiles_x * c.tiles_y * ((h->nz + c.zchunk - 1) / c.zchunk);
+    for (int i = 0; i < nc; ++i) clists[col_slot(wf::fused_col_item_class(c, i))].push_back(i);
+  }
+  for (int k = 0; k < wf::kColClassCount; ++k) {
+    h->col_off[k] = static_cast<int>(all.size());
+    h->col_n[k] = static_cast<int>(clists[k].size());
+    all.insert(all.end(), clists[k].begin(), clists[k].end());
   }
   cudaFree(h->d_items);
   h->d_items = nullptr;
@@ -375,18 +429,30 @@ TailArgs tail_args(const wf_handle *h) {
   t.kh = h->kh;
   t.ke = h->ke;
   t.ovf = h->d_ovf;
+  t.err = h->d_err;
   return t;
 }
 
 FusedArgs fused_args(const wf_handle *h) {
   FusedArgs a{};
   a.g = grid_args(h);
-  a.tiles_x = (h->nx + wf::kTileX - 1) / wf::kTileX;
+  a.x_lo = h->cols ? wf::kColWidth : 0;
+  a.x_hi = h->cols ? h->nx - wf::kColWidth : h->nx;
+  a.tiles_x = (a.x_hi - a.x_lo + wf::kTileX - 1) / wf::kTileX;
   a.tiles_y = (h->ny + h->cfg.ty - 1) / h->cfg.ty;
   a.zchunk = h->cfg.zchunk;
   a.has_pml = has_pml(h) ? 1 : 0;
   a.prof_in_smem = (h->ax[0].W <= 64 && h->ax[1].W <= 64 && h->ax[2].W <= 64) ? 1 : 0;
   a.test_extra_tx = h->test_extra_tx;
+  return a;
+}
+
+// Arguments of a column-tile launch: two tiles across (the low and the high
+// x edge), 32-row tiles, the wide tiles' z chunk.
+FusedArgs col_args(const wf_handle *h) {
+  FusedArgs a = fused_args(h);
+  a.tiles_x = 2;
+  a.tiles_y = (h->ny + wf::kColTileRows - 1) / wf::kColTileRows;
   return a;
 }
 
@@ -422,6 +488,18 @@ wf_status enqueue_one(wf_handle *h) {
     static constexpr int kOrder[wf::kFusedClassCount] = {7, 5, 3, 6, 1, 4, 2, 0};
     WF_CUDA(h, cudaEventRecord(h->fork_ev, h->stream));
     e = cudaSuccess;
+    // the x-CPML column tiles first (every lane runs the psi recursion)
+    const FusedArgs ca = col_args(h);
+    for (int ax = 7; ax >= 1 && h->cols && e == cudaSuccess; ax -= 2) {
+      const int k = col_slot(ax);
+      if (h->col_n[k] == 0) continue;
+      cudaStream_t s = h->side_col[k];
+      WF_CUDA(h, cudaStreamWaitEvent(s, h->fork_ev, 0));
+      e = wf::launch_fused_col(h->col_maps[h->cur], ca, h->d_items + h->col_off[k], h->col_n[k],
+                               ax, fma, s);
+      if (e == cudaSuccess) h->kernel_launches += 1;
+      if (e == cudaSuccess) WF_CUDA(h, cudaEventRecord(h->join_col[k], s));
+    }
     for (int i = 0; i < wf::kFusedClassCount && e == cudaSuccess; ++i) {
       const int k = kOrder[i];
       if (h->class_n[k] == 0) continue;
@@ -435,6 +513,8 @@ wf_status enqueue_one(wf_handle *h) {
     // the main stream waits for every side class only after all are launched
     for (int k = 1; k < wf::kFusedClassCount && e == cudaSuccess; ++k)
       if (h->class_n[k] > 0) WF_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_ev[k - 1], 0));
+    for (int k = 0; k < wf::kColClassCount && h->cols && e == cudaSuccess; ++k)
+      if (h->col_n[k] > 0) WF_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_col[k], 0));
   } else {
     e = wf::launch_split(g, fma, h->stream);
     if (e == cudaSuccess) h->kernel_launches += 2;  // H pass, E pass
@@ -585,7 +665,7 @@ wf_status batch_build(wf_batch *b) {
         return fail(nullptr, WF_ERR_UNSUPPORTED, "batched grids need CPML slabs of at most 64 cells");
     h->cfg = b->cfg;
     h->cfg_user_set = true;
-    wf_status st = build_maps(h);
+    wf_status st = build_maps(h, false);  // the batched kernel tiles the whole x range
     if (st != WF_OK) return st;
     const int cur = h->cur;
     for (int p = 0; p < 2; ++p) {
@@ -751,6 +831,11 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
         (e = cudaEventCreateWithFlags(&h->join_ev[k], cudaEventDisableTiming)) != cudaSuccess)
       return cleanup_fail(cuda_fail(nullptr, e, "side stream setup"));
   }
+  for (int k = 0; k < wf::kColClassCount; ++k) {
+    if ((e = cudaStreamCreateWithFlags(&h->side_col[k], cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->join_col[k], cudaEventDisableTiming)) != cudaSuccess)
+      return cleanup_fail(cuda_fail(nullptr, e, "side stream setup"));
+  }
   if ((e = cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup_fail(cuda_fail(nullptr, e, "cudaEventCreate"));
   for (int b = 0; b < 2; ++b) {
@@ -801,7 +886,21 @@ wf_status wf_destroy(wf_handle *h) {
     }
     if (h->join_ev[k]) cudaEventDestroy(h->join_ev[k]);
   }
+  for (int k = 0; k < wf::kColClassCount; ++k) {
+    if (h->side_col[k]) {
+      cudaStreamSynchronize(h->side_col[k]);
+      cudaStreamDestroy(h->side_col[k]);
+    }
+    if (h->join_col[k]) cudaEventDestroy(h->join_col[k]);
+  }
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+  if (h->copy) {
+    cudaStreamSynchronize(h->copy);
+    cudaStreamDestroy(h->copy);
+  }
+  if (h->staged) cudaEventDestroy(h->staged);
+  if (h->copied) cudaEventDestroy(h->copied);
+  cudaFree(h->d_stage);
   for (auto &f : h->fld) cudaFree(f);
   for (auto &s : h->shift) cudaFree(s);
   for (auto &w : h->cl_w) cudaFree(w);
@@ -1131,7 +1230,43 @@ wf_status wf_sync(wf_handle *h) {
   if (!h) return fail(h, WF_ERR_ARG, "null handle");
   DeviceGuard guard(h->dev);
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->copy_pending) {
+    WF_CUDA(h, cudaEventSynchronize(h->copied));
+    h->copy_pending = false;
+  }
   return check_device_error(h);
+}
+
+wf_status wf_reserve_download(wf_handle *h) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  if (store16(h))
+    return fail(h, WF_ERR_UNSUPPORTED, "asynchronous downloads need FP32 storage (use wf_download_blocks)");
+  DeviceGuard guard(h->dev);
+  if (!h->d_stage) {
+    WF_CUDA(h, cudaMalloc(&h->d_stage, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking));
+    WF_CUDA(h, cudaEventCreateWithFlags(&h->staged, cudaEventDisableTiming));
+    WF_CUDA(h, cudaEventCreateWithFlags(&h->copied, cudaEventDisableTiming));
+  }
+  return WF_OK;
+}
+
+wf_status wf_download_blocks_async(wf_handle *h, void *out) {
+  if (!h || !out) return fail(h, WF_ERR_ARG, "null argument");
+  wf_status st = wf_reserve_download(h);
+  if (st != WF_OK) return st;
+  DeviceGuard guard(h->dev);
+  // the staging buffer may still feed the previous download
+  if (h->copy_pending) WF_CUDA(h, cudaStreamWaitEvent(h->stream, h->copied, 0));
+  WF_CUDA(h, wf::launch_soa_to_blocks(h->fld[h->cur], h->d_stage, h->nx, h->ny, h->nz, h->stream));
+  WF_CUDA(h, cudaEventRecord(h->staged, h->stream));
+  WF_CUDA(h, cudaStreamWaitEvent(h->copy, h->staged, 0));
+  WF_CUDA(h, cudaMemcpyAsync(out, h->d_stage, sizeof(float) * 6 * h->N, cudaMemcpyDeviceToHost,
+                             h->copy));
+  WF_CUDA(h, cudaEventRecord(h->copied, h->copy));
+  h->copy_pending = true;
+  h->kernel_launches += 1;  // the reorder
+  return WF_OK;
 }
 
 int64_t wf_steps_done(const wf_handle *h) { return h ? h->steps_done : -1; }
@@ -1402,6 +1537,23 @@ wf_status wf_set_tiling(wf_handle *h, const wf_tiling *t) {
   return WF_OK;
 }
 
+wf_status wf_set_column_tiles(wf_handle *h, int enable) {
+  if (!h) return fail(h, WF_ERR_ARG, "null handle");
+  DeviceGuard guard(h->dev);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  drop_graphs(h);
+  h->col_pref = enable != 0;
+  ++h->version;
+  h->maps_ok = false;
+  return WF_OK;
+}
+
+int wf_column_tiles_active(const wf_handle *h) {
+  if (!h) return -1;
+  if (!use_fused(h)) return 0;
+  return (h->maps_ok ? h->cols : cols_apply(h)) ? 1 : 0;
+}
+
 wf_status wf_autotune(wf_handle *h, int steps, wf_tiling *best, float *best_ms) {
   if (!h || steps <= 0) return fail(h, WF_ERR_ARG, "bad autotune arguments");
   if (!use_fused(h)) return fail(h, WF_ERR_UNSUPPORTED, "autotuning applies to the fused kernel");
@@ -1583,6 +1735,13 @@ wf_status wf_nn_conv3d_backward_weight(const float *in, const float *dpre, const
                                                                    d, hh, ww, nface, stream)));
   return WF_OK;
 }
+
+wf_status wf_nn_set_tensor_cores(int enable) {
+  wf::nn_set_tensor_cores(enable);
+  return WF_OK;
+}
+
+int64_t wf_nn_tensor_core_timeouts(void) { return static_cast<int64_t>(wf::nn_tc_timeouts()); }
 
 wf_status wf_nn_gelu_backward(const float *dout, const float *pre, float *dpre, int64_t m,
                               void *stream) {

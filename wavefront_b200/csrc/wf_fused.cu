@@ -16,15 +16,17 @@ void fused_boxes(int ty, int prec, unsigned e_box[4], unsigned h_box[4], unsigne
   m_box[0] = kTileX + 16; m_box[1] = ty + 1; m_box[2] = 1;
 }
 
-int fused_item_class(const FusedArgs &a, int ty, int item) {
+static int item_class(const FusedArgs &a, int ty, int item, bool col) {
   if (!a.has_pml) return 0;
   const int txi = item % a.tiles_x;
   const int tyi = (item / a.tiles_x) % a.tiles_y;
   const int zc = item / (a.tiles_x * a.tiles_y);
-  const int x0 = txi * kTileX, y0 = tyi * ty;
+  const int x0 = col ? (txi == 0 ? 0 : a.g.nx - kColWidth) : a.x_lo + txi * kTileX;
+  const int y0 = tyi * ty;
   const int k0 = zc * a.zchunk, k1 = std::min(k0 + a.zchunk, a.g.nz);
   const PmlAxis &X = a.g.pml[0], &Y = a.g.pml[1], &Z = a.g.pml[2];
-  const int xh = std::min(x0 + kTileX, a.g.nx) - 1, yh = std::min(y0 + ty, a.g.ny) - 1;
+  const int xh = col ? x0 + kColWidth - 1 : std::min(x0 + kTileX, a.x_hi) - 1;
+  const int yh = std::min(y0 + ty, a.g.ny) - 1;
   // an axis's CPML code is needed if the CTA's cells, its -x/-y halo or its
   // warm-up plane (k0-1) meet that axis's graded slab
   int mask = 0;
@@ -32,6 +34,37 @@ int fused_item_class(const FusedArgs &a, int ty, int item) {
   if (Y.T > 0 && (y0 - 1 < Y.T || yh >= a.g.ny - Y.T)) mask |= 2;
   if (Z.T > 0 && (k0 - 1 < Z.T || k1 - 1 >= a.g.nz - Z.T)) mask |= 4;
   return mask;
+}
+
+int fused_item_class(const FusedArgs &a, int ty, int item) { return item_class(a, ty, item, false); }
+
+int fused_col_item_class(const FusedArgs &a, int item) {
+  return item_class(a, kColTileRows, item, true) | 1;
+}
+
+void fused_col_boxes(int prec, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]) {
+  const unsigned pad = prec == kPrecF32 ? 4u : 8u;  // 16 bytes of x
+  e_box[0] = kColWidth + 2 * pad; e_box[1] = kColTileRows + 2; e_box[2] = 1; e_box[3] = 3;
+  h_box[0] = kColWidth + pad; h_box[1] = kColTileRows + 1; h_box[2] = 1; h_box[3] = 3;
+  m_box[0] = kColWidth + 32; m_box[1] = kColTileRows + 1; m_box[2] = 1;  // see Layout::MW
+}
+
+static_assert(kColWidth == 4 * kColLanes && kColTileRows == kColRows, "column tile shape");
+
+cudaError_t fused_col_prepare(int prec) {
+  if (prec != kPrecF32) return fused16_col_prepare(prec);
+  cudaError_t e = col_prepare_t<false, float>();
+  return e != cudaSuccess ? e : col_prepare_t<true, float>();
+}
+
+cudaError_t launch_fused_col(const FusedMaps &m, const FusedArgs &a, const int *items,
+                             int n_items, int ax, bool fma, cudaStream_t s) {
+  if (a.g.prec != kPrecF32) {
+    if (fma) return cudaErrorInvalidValue;  // 16-bit storage runs the exact arithmetic
+    return fused16_col_launch(m, a, items, n_items, ax, s);
+  }
+  return fma ? col_launch_t<true, float>(m, a, items, n_items, ax, s)
+             : col_launch_t<false, float>(m, a, items, n_items, ax, s);
 }
 
 bool fused_supported(const FusedConfig &c, int prec) {

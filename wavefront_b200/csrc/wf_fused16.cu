@@ -46,4 +46,14 @@ cudaError_t fused16_launch(const FusedConfig &c, const FusedMaps &m, const Fused
   return cudaErrorInvalidValue;
 }
 
+cudaError_t fused16_col_prepare(int prec) {
+  return prec == kPrecF16 ? col_prepare_t<false, __half>() : col_prepare_t<false, __nv_bfloat16>();
+}
+
+cudaError_t fused16_col_launch(const FusedMaps &m, const FusedArgs &a, const int *items,
+                               int n_items, int ax, cudaStream_t s) {
+  return a.g.prec == kPrecF16 ? col_launch_t<false, __half>(m, a, items, n_items, ax, s)
+                              : col_launch_t<false, __nv_bfloat16>(m, a, items, n_items, ax, s);
+}
+
 }  // namespace wf

@@ -58,13 +58,21 @@ namespace {
 constexpr int kProfSmem = 3 * 3 * 64;  // floats: 3 axes x {b, a, 1/kappa} x 64 positions
 
 // Box x extents start PAD elements left of the tile (PAD = 16 bytes, the TMA
-// x alignment): E x0-PAD..x0+128+PAD-1, H x0-PAD..x0+127.
-template <int TY, int S, typename ST>
+// x alignment): E x0-PAD..x0+TW+PAD-1, H x0-PAD..x0+TW-1.  A tile is TW = 4*LX
+// cells wide (LX lanes per row, 4 cells each) and TY rows tall: the wide
+// tiles have LX = 32 (one row per warp), the x-CPML column tiles LX = 4
+// (eight rows per warp).
+template <int TY, int S, typename ST, int LX = 32>
 struct Layout {
   static constexpr int PAD = Store<ST>::PAD;
-  static constexpr int EW = kTileX + 2 * PAD, EH = TY + 2;  // E box rows y0-1..y0+TY
-  static constexpr int HW = kTileX + PAD, HH = TY + 1;      // H box rows y0-1..y0+TY-1
-  static constexpr int MW = kTileX + 16, MH = TY + 1;       // ids:   x0-16..x0+127
+  static constexpr int TW = 4 * LX;
+  static constexpr int RW = 32 / LX;  // rows per tile warp
+  static constexpr int EW = TW + 2 * PAD, EH = TY + 2;  // E box rows y0-1..y0+TY
+  static constexpr int HW = TW + PAD, HH = TY + 1;      // H box rows y0-1..y0+TY-1
+  // ids: the box starts at (x0-16) rounded down to 16 (u8 TMA x alignment):
+  // x0-16 for the wide tiles (x0 a multiple of 16), x0-16 or x0-24 for a
+  // column tile at nx-16 (nx a multiple of 8)
+  static constexpr int MW = LX == 32 ? TW + 16 : TW + 32, MH = TY + 1;
   static constexpr int E_BYTES = 3 * EH * EW * static_cast<int>(sizeof(ST));
   static constexpr int H_BYTES = 3 * HH * HW * static_cast<int>(sizeof(ST));
   static constexpr int M_BYTES = MH * MW;
@@ -74,13 +82,15 @@ struct Layout {
   static constexpr int STAGE = M_OFF + al(M_BYTES);
   static constexpr int STAGE_OFF = 4096;  // after the 256-entry float4 coefficient table
   static constexpr int PROWS = TY + 1;    // plane rows: 0 = y0-1, 1..TY = tile rows
-  static constexpr int PLANE_FLOATS = 2 * PROWS * kTileX + 64;  // hz, hx rows; x-halo hz, hy
+  static constexpr int HALO = TY + 1 <= 32 ? 32 : 64;  // x-halo column entries (rows 1..TY)
+  static constexpr int PLANE_FLOATS = 2 * PROWS * TW + 2 * HALO;  // hz, hx rows; x-halo hz, hy
   static constexpr int PLANE_OFF = STAGE_OFF + S * STAGE;
   static constexpr int PROF_OFF = PLANE_OFF + 2 * PLANE_FLOATS * 4;  // CPML profiles
   static constexpr int BAR_OFF = PROF_OFF + kProfSmem * 4;
   static constexpr int BYTES = BAR_OFF + S * 8 + 128;  // +128: base alignment slack
-  static constexpr int THREADS = 32 * (TY + 1);
-  static_assert(TY + 1 <= 32, "x-halo column is handled by one warp");
+  static constexpr int THREADS = 32 * (TY / RW + 1);  // tile warps + the halo warp
+  static_assert(TY % RW == 0, "whole tile warps");
+  static_assert(TY <= 32, "x-halo column is handled by one warp");
 };
 
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -161,8 +171,15 @@ struct HaloPsi {
   float x0, x1, y0, y1, z0, z1;
 };
 
-__device__ __forceinline__ Psi2 load_psi2(const PmlAxis &P, int comp0, long long idx) {
+__device__ __forceinline__ Psi2 load_psi2(const PmlAxis &P, int comp0, long long idx, int *err) {
+  if (!idx_ok(err, idx + 3, P.cells)) return Psi2{};
   return Psi2{ldg4(P.psi_cur + comp0 * P.cells + idx), ldg4(P.psi_cur + (comp0 + 1) * P.cells + idx)};
+}
+
+// float4 store of psi components comp0 at idx (checked in bounds-checked builds)
+__device__ __forceinline__ void store_psi4(const PmlAxis &P, int comp, long long idx, float4 v,
+                                           int *err) {
+  if (idx_ok(err, idx + 3, P.cells)) stg4(P.psi_nxt + comp * P.cells + idx, v);
 }
 
 // Computing units <-> field units of psi: 16-bit storage (U) computes in
@@ -220,6 +237,7 @@ __device__ __forceinline__ void corr_x_cell(const GridArgs &g, const Prof &pf, i
   const int s = slab_pos(x, g.nx, P.T, P.W);
   if (s < 0) return;
   const long long idx = (static_cast<long long>(p) * g.ny + y) * P.pitch + s;
+  if (!idx_ok(g.err, idx, P.cells)) return;
   float p0 = __ldg(P.psi_cur + comp0 * P.cells + idx), p1 = __ldg(P.psi_cur + (comp0 + 1) * P.cells + idx);
   const float b = pf.b(0, s), a = pf.a(0, s), ik = pf.ik(0, s);
   d0 = corr_u<FMA, U>(d0, b, a, ik, p0, u);
@@ -231,11 +249,14 @@ __device__ __forceinline__ void corr_x_cell(const GridArgs &g, const Prof &pf, i
 }
 
 // AX: the CPML axes this body handles (bit 1 x, 2 y, 4 z; 0 = interior).
-template <int TY, int S, bool FMA, int AX, typename ST>
+// The tile's cells are x in [x0, x_end), y in [y0, y0+TY), z in [k0, k1).
+template <int TY, int S, bool FMA, int AX, typename ST, int LX = 32>
 __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtensorMap *tmH,
                                            const CUtensorMap *tmM, const FusedArgs &a,
-                                           unsigned char *smem, int x0, int y0, int k0, int k1) {
-  using L = Layout<TY, S, ST>;
+                                           unsigned char *smem, int x0, int y0, int k0, int k1,
+                                           int x_end) {
+  using L = Layout<TY, S, ST, LX>;
+  constexpr int TW = L::TW;
   using SD = Store<ST>;
   constexpr int PAD = L::PAD;
   constexpr bool PML = AX != 0;
@@ -249,6 +270,7 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
 
   const int nx = g.nx, ny = g.ny;
   const long long N = g.N;
+  const int moff = x0 - ((x0 - 16) & ~15);  // column of x0 in the ids box (16 or 24)
   const int kfirst = k0 > 0 ? k0 - 1 : 0;  // k0-1: warm-up plane for H(k0-1)
   const int np = k1 - kfirst + 1;          // planes staged; plane k1 brings only E
 
@@ -265,7 +287,7 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     tma_load_4d(smem_u32(st), tmE, x0 - PAD, y0 - 1, p, 0, bar);
     if (!e_only) {
       tma_load_4d(smem_u32(st + L::H_OFF), tmH, x0 - PAD, y0 - 1, p, 3, bar);
-      tma_load_3d(smem_u32(st + L::M_OFF), tmM, x0 - 16, y0 - 1, p, bar);
+      tma_load_3d(smem_u32(st + L::M_OFF), tmM, x0 - moff, y0 - 1, p, bar);
     }
   };
 
@@ -278,14 +300,18 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   bool ok = mbar_wait(smem_u32(&s_bar[0]), 0);
   int done = ok ? 1 : 0;  // stages [0, done) seen complete, in order
 
-  const bool tile_warp = warp < TY;
-  const int r = tile_warp ? warp + 1 : 0;  // smem row: 0 is the -y halo row y0-1
+  // tile warps hold L::RW rows of LX lanes each; the halo warp computes the
+  // -y halo row (every lane, col = lane % LX: lanes of the same col compute
+  // the same cells) and the -x halo column (lanes 0..TY-1)
+  const bool tile_warp = warp < TY / L::RW;
+  const int col = lane % LX;
+  const int r = tile_warp ? warp * L::RW + lane / LX + 1 : 0;  // smem row: 0 is y0-1
   const int y = y0 - 1 + r;
-  const int xg = x0 + 4 * lane;
+  const int xg = x0 + 4 * col;
   const bool row_in = (y >= 0) && (y < ny);
-  const bool x_in = xg < nx;  // nx % 8 == 0: a lane's 4 cells are all in or all out
+  const bool x_in = xg < x_end;  // x_end % 4 == 0: a lane's 4 cells are all in or all out
   const bool cell_ok = row_in && x_in;
-  const int cE = PAD + 4 * lane;
+  const int cE = PAD + 4 * col;
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;  // H(p-1), own cells
   // E(p+1) of the own row as decoded for plane p's z differences: plane p+1's
   // own ex, ey when the warp worked on plane p and p+1 is in the same slab
@@ -321,9 +347,9 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
   Psi2 qx_n{}, qy_n{}, qz_n{};
   auto prefetch = [&](int pp) {
     lp_n = lane_pml<AX>(g, lc, xg, y, pp);
-    if (AXY && lp_n.y) qy_n = load_psi2(g.pml[1], 0, lp_n.iy);
-    if (AXZ && lp_n.z) qz_n = load_psi2(g.pml[2], 0, lp_n.iz);
-    if (AXX && lp_n.xmode == 1) qx_n = load_psi2(g.pml[0], 0, lp_n.ix);
+    if (AXY && lp_n.y) qy_n = load_psi2(g.pml[1], 0, lp_n.iy, g.err);
+    if (AXZ && lp_n.z) qz_n = load_psi2(g.pml[2], 0, lp_n.iz, g.err);
+    if (AXX && lp_n.xmode == 1) qx_n = load_psi2(g.pml[0], 0, lp_n.ix, g.err);
   };
   // ... and so is the H-term psi of the -x halo cell (x0-1, y0+lane) that
   // lanes 0..TY-1 of the halo warp update.
@@ -336,8 +362,10 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       hh_n.sx = slab_pos(xh, nx, P.T, P.W);
       if (hh_n.sx >= 0) {
         const long long i = (static_cast<long long>(pp) * ny + yh) * P.pitch + hh_n.sx;
-        hh_n.x0 = __ldg(P.psi_cur + i);
-        hh_n.x1 = __ldg(P.psi_cur + P.cells + i);
+        if (idx_ok(g.err, i, P.cells)) {
+          hh_n.x0 = __ldg(P.psi_cur + i);
+          hh_n.x1 = __ldg(P.psi_cur + P.cells + i);
+        }
       }
     }
     if (AXY) {
@@ -345,8 +373,10 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       hh_n.sy = slab_pos(yh, ny, P.T, P.W);
       if (hh_n.sy >= 0) {
         const long long i = (static_cast<long long>(pp) * P.W + hh_n.sy) * nx + xh;
-        hh_n.y0 = __ldg(P.psi_cur + i);
-        hh_n.y1 = __ldg(P.psi_cur + P.cells + i);
+        if (idx_ok(g.err, i, P.cells)) {
+          hh_n.y0 = __ldg(P.psi_cur + i);
+          hh_n.y1 = __ldg(P.psi_cur + P.cells + i);
+        }
       }
     }
     if (AXZ) {
@@ -354,8 +384,10 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       hh_n.sz = slab_pos(pp, g.nz, P.T, P.W);
       if (hh_n.sz >= 0) {
         const long long i = (static_cast<long long>(hh_n.sz) * ny + yh) * nx + xh;
-        hh_n.z0 = __ldg(P.psi_cur + i);
-        hh_n.z1 = __ldg(P.psi_cur + P.cells + i);
+        if (idx_ok(g.err, i, P.cells)) {
+          hh_n.z0 = __ldg(P.psi_cur + i);
+          hh_n.z1 = __ldg(P.psi_cur + P.cells + i);
+        }
       }
     }
   };
@@ -402,8 +434,8 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     const ST *Hc = reinterpret_cast<const ST *>(stc + L::H_OFF);
     const uint8_t *Mc = stc + L::M_OFF;
     float *pl = s_plane + (p & 1) * L::PLANE_FLOATS;
-    float *pl_hz = pl, *pl_hx = pl + L::PROWS * kTileX;
-    float *pl_hzh = pl + 2 * L::PROWS * kTileX, *pl_hyh = pl_hzh + 32;
+    float *pl_hz = pl, *pl_hx = pl + L::PROWS * TW;
+    float *pl_hzh = pl + 2 * L::PROWS * TW, *pl_hyh = pl_hzh + L::HALO;
 
     // ---------------- H phase (update_h_field[_pml], src/fdtd.rs:194-345) ----
     float ha[4], hb[4], hc[4];  // new hx, hy, hz of this lane's 4 cells
@@ -446,11 +478,11 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
       ey_nx = ey_pz;
       float ez_n = __shfl_down_sync(0xffffffffu, ez4.x, 1);
       float ey_n = __shfl_down_sync(0xffffffffu, ey4.x, 1);
-      if (lane == 31) {
-        ez_n = SD::template ld1<SD::k16>(Ec + (2 * L::EH + r) * L::EW + PAD + kTileX, fC);
-        ey_n = SD::template ld1<SD::k16>(Ec + (1 * L::EH + r) * L::EW + PAD + kTileX, fC);
+      if (col == LX - 1) {
+        ez_n = SD::template ld1<SD::k16>(Ec + (2 * L::EH + r) * L::EW + PAD + TW, fC);
+        ey_n = SD::template ld1<SD::k16>(Ec + (1 * L::EH + r) * L::EW + PAD + TW, fC);
       }
-      m4 = *reinterpret_cast<const uchar4 *>(Mc + r * L::MW + 16 + 4 * lane);
+      m4 = *reinterpret_cast<const uchar4 *>(Mc + r * L::MW + moff + 4 * col);
 
       float d_ez_dy[4], d_ex_dy[4], d_ey_dz[4], d_ex_dz[4], d_ez_dx[4], d_ey_dx[4];
 #pragma unroll
@@ -467,9 +499,8 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         if (AXX && lp.xmode == 1) {
           corr4_x<FMA, SD::k16>(d_ez_dx, d_ey_dx, qx, pf, lp.sx, un);
           if (wpsi) {
-            const PmlAxis &P = g.pml[0];
-            stg4(P.psi_nxt + lp.ix, qx.p0);
-            stg4(P.psi_nxt + P.cells + lp.ix, qx.p1);
+            store_psi4(g.pml[0], 0, lp.ix, qx.p0, g.err);
+            store_psi4(g.pml[0], 1, lp.ix, qx.p1, g.err);
           }
         } else if (AXX && lp.xmode == 2) {
 #pragma unroll
@@ -480,24 +511,22 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
           corr4_uniform<FMA, SD::k16>(d_ez_dy, d_ex_dy, qy, pf.b(1, lp.sy), pf.a(1, lp.sy),
                                       pf.ik(1, lp.sy), un);
           if (wpsi) {
-            const PmlAxis &P = g.pml[1];
-            stg4(P.psi_nxt + lp.iy, qy.p0);
-            stg4(P.psi_nxt + P.cells + lp.iy, qy.p1);
+            store_psi4(g.pml[1], 0, lp.iy, qy.p0, g.err);
+            store_psi4(g.pml[1], 1, lp.iy, qy.p1, g.err);
           }
         }
         if (AXZ && lp.z) {
           corr4_uniform<FMA, SD::k16>(d_ey_dz, d_ex_dz, qz, pf.b(2, lp.sz), pf.a(2, lp.sz),
                                       pf.ik(2, lp.sz), un);
           if (wpsi) {
-            const PmlAxis &P = g.pml[2];
-            stg4(P.psi_nxt + lp.iz, qz.p0);
-            stg4(P.psi_nxt + P.cells + lp.iz, qz.p1);
+            store_psi4(g.pml[2], 0, lp.iz, qz.p0, g.err);
+            store_psi4(g.pml[2], 1, lp.iz, qz.p1, g.err);
           }
         }
         if (wpsi) {  // the E terms' psi: in flight across the barrier
-          if (AXX && lp.xmode == 1) ex_ = load_psi2(g.pml[0], 2, lp.ix);
-          if (AXY && lp.y) ey_ = load_psi2(g.pml[1], 2, lp.iy);
-          if (AXZ && lp.z) ez_ = load_psi2(g.pml[2], 2, lp.iz);
+          if (AXX && lp.xmode == 1) ex_ = load_psi2(g.pml[0], 2, lp.ix, g.err);
+          if (AXY && lp.y) ey_ = load_psi2(g.pml[1], 2, lp.iy, g.err);
+          if (AXZ && lp.z) ez_ = load_psi2(g.pml[2], 2, lp.iz, g.err);
         }
       }
 #pragma unroll
@@ -527,10 +556,11 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         }
       }
       if (!warm) {
-        stg4(pl_hz + r * kTileX + 4 * lane, make_float4(hc[0], hc[1], hc[2], hc[3]));
-        stg4(pl_hx + r * kTileX + 4 * lane, make_float4(ha[0], ha[1], ha[2], ha[3]));
-        if (hstore) {
-          ST *Hn = nxt + 3 * N + (static_cast<long long>(p) * ny + y) * nx + xg;
+        stg4(pl_hz + r * TW + 4 * col, make_float4(hc[0], hc[1], hc[2], hc[3]));
+        stg4(pl_hx + r * TW + 4 * col, make_float4(ha[0], ha[1], ha[2], ha[3]));
+        const long long hcell = (static_cast<long long>(p) * ny + y) * nx + xg;
+        if (hstore && idx_ok(g.err, hcell + 3, N)) {
+          ST *Hn = nxt + 3 * N + hcell;
           SD::st4(Hn, wa);
           SD::st4(Hn + N, wb);
           SD::st4(Hn + 2 * N, wc);
@@ -574,7 +604,7 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
             d_ey_dz1 = corr_u<FMA, U>(d_ey_dz1, b, a_, ik, hh.z0, un);
             d_ex_dz1 = corr_u<FMA, U>(d_ex_dz1, b, a_, ik, hh.z1, un);
           }
-          const float4 cf = s_coef[Mc[rh * L::MW + 15]];
+          const float4 cf = s_coef[Mc[rh * L::MW + moff - 1]];
           auto Hv = [&](int c) {
             return SD::template ld1<SD::k16>(Hc + (c * L::HH + rh) * L::HW + PAD - 1, fC);
           };
@@ -600,11 +630,11 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
     // ---------------- E phase (update_e_field[_pml], src/fdtd.rs:369-509) ----
     if (tile_warp) {
       if (!warm) {
-        const float4 hz_my = lds4(pl_hz + (r - 1) * kTileX + 4 * lane);
-        const float4 hx_my = lds4(pl_hx + (r - 1) * kTileX + 4 * lane);
+        const float4 hz_my = lds4(pl_hz + (r - 1) * TW + 4 * col);
+        const float4 hx_my = lds4(pl_hx + (r - 1) * TW + 4 * col);
         float hz_w = __shfl_up_sync(0xffffffffu, hc[3], 1);
         float hy_w = __shfl_up_sync(0xffffffffu, hb[3], 1);
-        if (lane == 0) {
+        if (col == 0) {
           hz_w = pl_hzh[r];
           hy_w = pl_hyh[r];
         }
@@ -620,31 +650,29 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
         }
         if (PML && cell_ok) {
           if (AXX && lp.xmode == 1) {
-            const PmlAxis &P = g.pml[0];
             corr4_x<FMA, SD::k16>(d_hz_dx, d_hy_dx, ex_, pf, lp.sx, un);
-            stg4(P.psi_nxt + 2 * P.cells + lp.ix, ex_.p0);
-            stg4(P.psi_nxt + 3 * P.cells + lp.ix, ex_.p1);
+            store_psi4(g.pml[0], 2, lp.ix, ex_.p0, g.err);
+            store_psi4(g.pml[0], 3, lp.ix, ex_.p1, g.err);
           } else if (AXX && lp.xmode == 2) {
 #pragma unroll
             for (int q = 0; q < 4; ++q)
               corr_x_cell<FMA, SD::k16>(g, pf, 2, xg + q, y, p, d_hz_dx[q], d_hy_dx[q], true, un);
           }
           if (AXY && lp.y) {
-            const PmlAxis &P = g.pml[1];
             corr4_uniform<FMA, SD::k16>(d_hz_dy, d_hx_dy, ey_, pf.b(1, lp.sy), pf.a(1, lp.sy),
                                         pf.ik(1, lp.sy), un);
-            stg4(P.psi_nxt + 2 * P.cells + lp.iy, ey_.p0);
-            stg4(P.psi_nxt + 3 * P.cells + lp.iy, ey_.p1);
+            store_psi4(g.pml[1], 2, lp.iy, ey_.p0, g.err);
+            store_psi4(g.pml[1], 3, lp.iy, ey_.p1, g.err);
           }
           if (AXZ && lp.z) {
-            const PmlAxis &P = g.pml[2];
             corr4_uniform<FMA, SD::k16>(d_hy_dz, d_hx_dz, ez_, pf.b(2, lp.sz), pf.a(2, lp.sz),
                                         pf.ik(2, lp.sz), un);
-            stg4(P.psi_nxt + 2 * P.cells + lp.iz, ez_.p0);
-            stg4(P.psi_nxt + 3 * P.cells + lp.iz, ez_.p1);
+            store_psi4(g.pml[2], 2, lp.iz, ez_.p0, g.err);
+            store_psi4(g.pml[2], 3, lp.iz, ez_.p1, g.err);
           }
         }
-        if (cell_ok) {
+        const long long ecell = (static_cast<long long>(p) * ny + y) * nx + xg;
+        if (cell_ok && idx_ok(g.err, ecell + 3, N)) {
           float eo[3][4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
@@ -654,7 +682,7 @@ __device__ __forceinline__ void fused_body(const CUtensorMap *tmE, const CUtenso
             eo[1][q] = e_new<FMA>(cf.x, comp(ey4, q), cf.y, sub(d_hx_dz[q], d_hz_dx[q]));
             eo[2][q] = e_new<FMA>(cf.x, comp(ez4, q), cf.y, sub(d_hy_dx[q], d_hx_dy[q]));
           }
-          ST *Ep = nxt + (static_cast<long long>(p) * ny + y) * nx + xg;
+          ST *Ep = nxt + ecell;
           const typename SD::Word w0 = SD::enc4(eo[0]), w1 = SD::enc4(eo[1]), w2 = SD::enc4(eo[2]);
           SD::st4(Ep, w0);
           SD::st4(Ep + N, w1);
@@ -697,12 +725,20 @@ template <int AX>
 constexpr int kMultiAxis = (AX & (AX - 1)) != 0;
 template <int AX, typename ST>
 constexpr int kCtasPerSm4 = kMultiAxis<AX> ? 2 : (sizeof(ST) == 2 && AX == 0 ? 4 : 3);
+// five-warp CTAs (four tile warps + the halo warp) follow the rule above
+template <int TY, int LX, int AX, typename ST>
+constexpr int kCtasPerSm = Layout<TY, 3, ST, LX>::THREADS <= 160 ? kCtasPerSm4<AX, ST> : 1;
 
-template <int TY, int S, bool FMA, int AX, typename ST>
-__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, ST> : 1)
+// Column tiles of the x-CPML slabs: 16 cells (4 lanes) wide, 32 rows tall,
+// so that every lane of the CTA holds graded cells and the wide tiles hold
+// none (their x range is [x_lo, x_hi) = [16, nx-16)).
+constexpr int kColLanes = 4, kColRows = 32, kColStages = 3;
+
+template <int TY, int S, bool FMA, int AX, typename ST, int LX = 32>
+__global__ void __launch_bounds__(Layout<TY, S, ST, LX>::THREADS, kCtasPerSm<TY, LX, AX, ST>)
     k_fused(const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmH,
             const __grid_constant__ CUtensorMap tmM, const FusedArgs a, const int *items) {
-  using L = Layout<TY, S, ST>;
+  using L = Layout<TY, S, ST, LX>;
   extern __shared__ unsigned char smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
@@ -711,7 +747,11 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, ST> :
   item /= a.tiles_x;
   const int tyi = item % a.tiles_y;
   const int zc = item / a.tiles_y;
-  const int x0 = txi * kTileX, y0 = tyi * TY;
+  // wide tiles step through [x_lo, x_hi); a column tile is the low (txi 0)
+  // or the high (txi 1) x edge of the grid
+  const int x0 = LX == 32 ? a.x_lo + txi * kTileX : (txi == 0 ? 0 : a.g.nx - L::TW);
+  const int x_end = LX == 32 ? min(x0 + kTileX, a.x_hi) : x0 + L::TW;
+  const int y0 = tyi * TY;
   const int k0 = zc * a.zchunk;
   const int k1 = min(k0 + a.zchunk, a.g.nz);
 
@@ -732,7 +772,7 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, ST> :
     mbar_fence_init();
   }
   __syncthreads();
-  fused_body<TY, S, FMA, AX, ST>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1);
+  fused_body<TY, S, FMA, AX, ST, LX>(&tmE, &tmH, &tmM, a, smem, x0, y0, k0, k1, x_end);
 }
 
 // Batched step: one persistent launch per CPML class AX.  A CTA takes
@@ -796,7 +836,8 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, float
     first = false;
     __syncthreads();
     fused_body<TY, S, false, AX, float>(&sc->maps[parity][0], &sc->maps[parity][1],
-                                        &sc->maps[parity][2], a, smem, x0, y0, k0, k1);
+                                        &sc->maps[parity][2], a, smem, x0, y0, k0, k1,
+                                        min(x0 + kTileX, a.g.nx));
   }
 }
 
@@ -869,6 +910,43 @@ cudaError_t prepare_t() {
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+// x-CPML column tiles: classes with the x bit only (1, 3, 5, 7)
+#define WF_COL_CLASSES(X) X(1) X(3) X(5) X(7)
+
+template <bool FMA, typename ST>
+cudaError_t col_prepare_t() {
+  using L = Layout<kColRows, kColStages, ST, kColLanes>;
+  const void *fns[] = {
+#define X(A) (const void *)k_fused<kColRows, kColStages, FMA, A, ST, kColLanes>,
+      WF_COL_CLASSES(X)
+#undef X
+  };
+  for (const void *f : fns) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <bool FMA, typename ST>
+cudaError_t col_launch_t(const FusedMaps &m, const FusedArgs &a, const int *items, int n_items,
+                         int ax, cudaStream_t s) {
+  using L = Layout<kColRows, kColStages, ST, kColLanes>;
+  if (n_items <= 0) return cudaSuccess;
+  switch (ax) {
+#define X(A)                                                                                \
+  case A:                                                                                  \
+    k_fused<kColRows, kColStages, FMA, A, ST, kColLanes>                                   \
+        <<<n_items, L::THREADS, L::BYTES, s>>>(m.e, m.h, m.m, a, items);                    \
+    break;
+    WF_COL_CLASSES(X)
+#undef X
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 template <int TY, int S, bool FMA, typename ST>

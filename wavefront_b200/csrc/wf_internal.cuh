@@ -77,6 +77,23 @@ struct GridArgs {
   int nslab;
 };
 
+// Bounds-checked builds (compiled with -DWF_BOUNDS_CHECK, the library's
+// debugging variant): each checked global access first tests its index
+// against the extent of its buffer; a bad index latches kErrBounds in the
+// grid's error word (reported by wf_sync) and the access is skipped, a load
+// reading zero.  In the normal build the checks compile to nothing.
+#ifdef WF_BOUNDS_CHECK
+constexpr bool kBoundsCheck = true;
+#else
+constexpr bool kBoundsCheck = false;
+#endif
+__device__ __forceinline__ bool idx_ok(int *err, long long i, long long n) {
+  if (!kBoundsCheck) return true;
+  if (i >= 0 && i < n) return true;
+  if (err) atomicOr(err, kErrBounds);
+  return false;
+}
+
 __device__ __forceinline__ int slab_pos(int c, int n, int T, int W) {
   if (T <= 0) return -1;
   if (c < T) return c;

@@ -26,11 +26,16 @@ struct TailArgs {
   int nslab, periodic_z;
   float kh, ke;  // 8 * max |Db|, 8 * max |Cb| over the material table
   unsigned long long *ovf;
+  int *err;  // device error word (bounds-checked builds latch kErrBounds)
 };
 
 struct FusedArgs {
   GridArgs g;
   int tiles_x, tiles_y, zchunk;
+  // wide tiles cover x in [x_lo, x_hi): the whole grid, or [16, nx-16) when
+  // the x-CPML slabs run as column tiles (tiles_x = 2 in a column launch:
+  // the low and the high edge)
+  int x_lo, x_hi;
   int has_pml;
   int prof_in_smem;  // every CPML axis has at most 64 slab positions
   int test_extra_tx;  // testing aid: bytes stage 0 expects beyond its copies (0 normally)
@@ -72,6 +77,16 @@ cudaError_t fused_prepare(const FusedConfig &c, int prec);
 // the CPML slabs it meets (1 x, 2 y, 4 z; 0 interior).
 int fused_item_class(const FusedArgs &a, int ty, int item);
 constexpr int kFusedClassCount = 8;
+// x-CPML column tiles (16 cells wide, 32 rows; every lane holds graded
+// cells): boxes, class of an item (always has the x bit: 1, 3, 5 or 7),
+// kernel preparation and launch (any storage; FMA only for FP32).
+constexpr int kColWidth = 16, kColTileRows = 32;
+constexpr int kColClassCount = 4;  // classes 1, 3, 5, 7
+void fused_col_boxes(int prec, unsigned e_box[4], unsigned h_box[4], unsigned m_box[3]);
+int fused_col_item_class(const FusedArgs &a, int item);
+cudaError_t fused_col_prepare(int prec);
+cudaError_t launch_fused_col(const FusedMaps &m, const FusedArgs &a, const int *items,
+                             int n_items, int ax, bool fma, cudaStream_t s);
 // Launches the kernel of class `ax` over a device list of n_items items.
 cudaError_t launch_fused(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                          const int *items, int n_items, int ax, bool fma, cudaStream_t s);
@@ -94,6 +109,9 @@ int fused16_smem_bytes(const FusedConfig &c, int prec);
 cudaError_t fused16_prepare(const FusedConfig &c, int prec);
 cudaError_t fused16_launch(const FusedConfig &c, const FusedMaps &m, const FusedArgs &a,
                            const int *items, int n_items, int ax, cudaStream_t s);
+cudaError_t fused16_col_prepare(int prec);
+cudaError_t fused16_col_launch(const FusedMaps &m, const FusedArgs &a, const int *items,
+                               int n_items, int ax, cudaStream_t s);
 
 // 16-bit storage helpers (wf_split.cu).
 // Encodes FP32 values `in` (6*N) as the 16-bit state `out`: per slab and

@@ -38,6 +38,12 @@ __device__ __forceinline__ bool pml_slot(const PmlAxis &P, int axis, int x, int 
   return true;
 }
 
+// value i of a component array of n cells, zero when a bounds-checked build
+// finds i outside it
+__device__ __forceinline__ float ld_chk(const float *p, long long i, long long n, int *err) {
+  return idx_ok(err, i, n) ? p[i] : 0.0f;
+}
+
 // update_h_field[_pml] for one cell (src/fdtd.rs:194-345)
 template <bool FMA>
 __global__ void k_split_h(GridArgs g) {
@@ -50,16 +56,21 @@ __global__ void k_split_h(GridArgs g) {
   const long long ixp = x + 1 < g.nx ? i + 1 : (g.periodic[0] ? i - (g.nx - 1) : -1);
   const long long iyp = y + 1 < g.ny ? i + sy : (g.periodic[1] ? i - (g.ny - 1) * sy : -1);
   const long long izp = z + 1 < g.nz ? i + sz : (g.periodic[2] ? i - (g.nz - 1) * sz : -1);
+  int *err = g.err;
   const float ex = E[i], ey = E[N + i], ez = E[2 * N + i];
-  const float ez_py = iyp >= 0 ? E[2 * N + iyp] : 0.0f, ex_py = iyp >= 0 ? E[iyp] : 0.0f;
-  const float ey_pz = izp >= 0 ? E[N + izp] : 0.0f, ex_pz = izp >= 0 ? E[izp] : 0.0f;
-  const float ez_px = ixp >= 0 ? E[2 * N + ixp] : 0.0f, ey_px = ixp >= 0 ? E[N + ixp] : 0.0f;
+  const float ez_py = iyp >= 0 ? ld_chk(E + 2 * N, iyp, N, err) : 0.0f;
+  const float ex_py = iyp >= 0 ? ld_chk(E, iyp, N, err) : 0.0f;
+  const float ey_pz = izp >= 0 ? ld_chk(E + N, izp, N, err) : 0.0f;
+  const float ex_pz = izp >= 0 ? ld_chk(E, izp, N, err) : 0.0f;
+  const float ez_px = ixp >= 0 ? ld_chk(E + 2 * N, ixp, N, err) : 0.0f;
+  const float ey_px = ixp >= 0 ? ld_chk(E + N, ixp, N, err) : 0.0f;
   float d_ez_dy = sub(ez_py, ez), d_ex_dy = sub(ex_py, ex);
   float d_ey_dz = sub(ey_pz, ey), d_ex_dz = sub(ex_pz, ex);
   float d_ez_dx = sub(ez_px, ez), d_ey_dx = sub(ey_px, ey);
   long long idx;
   float b, a, ik;
-  if (pml_slot(g.pml[0], 0, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik)) {
+  if (pml_slot(g.pml[0], 0, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik) &&
+      idx_ok(err, idx, g.pml[0].cells)) {
     const PmlAxis &P = g.pml[0];
     float p0 = P.psi_cur[idx], p1 = P.psi_cur[P.cells + idx];
     d_ez_dx = pml_corr<FMA>(d_ez_dx, b, a, ik, p0);
@@ -67,7 +78,8 @@ __global__ void k_split_h(GridArgs g) {
     P.psi_nxt[idx] = p0;
     P.psi_nxt[P.cells + idx] = p1;
   }
-  if (pml_slot(g.pml[1], 1, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik)) {
+  if (pml_slot(g.pml[1], 1, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik) &&
+      idx_ok(err, idx, g.pml[1].cells)) {
     const PmlAxis &P = g.pml[1];
     float p0 = P.psi_cur[idx], p1 = P.psi_cur[P.cells + idx];
     d_ez_dy = pml_corr<FMA>(d_ez_dy, b, a, ik, p0);
@@ -75,7 +87,8 @@ __global__ void k_split_h(GridArgs g) {
     P.psi_nxt[idx] = p0;
     P.psi_nxt[P.cells + idx] = p1;
   }
-  if (pml_slot(g.pml[2], 2, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik)) {
+  if (pml_slot(g.pml[2], 2, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik) &&
+      idx_ok(err, idx, g.pml[2].cells)) {
     const PmlAxis &P = g.pml[2];
     float p0 = P.psi_cur[idx], p1 = P.psi_cur[P.cells + idx];
     d_ey_dz = pml_corr<FMA>(d_ey_dz, b, a, ik, p0);
@@ -87,7 +100,7 @@ __global__ void k_split_h(GridArgs g) {
   const float curl_hy = sub(d_ex_dz, d_ez_dx);
   const float curl_hz = sub(d_ey_dx, d_ex_dy);
   const float4 cf = g.coef[g.mat[(static_cast<long long>(z) * g.ny + y) * g.mat_pitch + x]];
-  const float *H = g.cur + 3 * N;
+  const float *H = g.cur + 3 * N;  // (i < N: all indices below are in range)
   float *Hn = g.nxt + 3 * N;
   Hn[i] = h_new<FMA>(cf.z, H[i], cf.w, curl_hx);
   Hn[N + i] = h_new<FMA>(cf.z, H[N + i], cf.w, curl_hy);
@@ -106,16 +119,21 @@ __global__ void k_split_e(GridArgs g) {
   const long long ixm = x > 0 ? i - 1 : (g.periodic[0] ? i + (g.nx - 1) : -1);
   const long long iym = y > 0 ? i - sy : (g.periodic[1] ? i + (g.ny - 1) * sy : -1);
   const long long izm = z > 0 ? i - sz : (g.periodic[2] ? i + (g.nz - 1) * sz : -1);
+  int *err = g.err;
   const float hx = H[i], hy = H[N + i], hz = H[2 * N + i];
-  const float hz_my = iym >= 0 ? H[2 * N + iym] : 0.0f, hx_my = iym >= 0 ? H[iym] : 0.0f;
-  const float hy_mz = izm >= 0 ? H[N + izm] : 0.0f, hx_mz = izm >= 0 ? H[izm] : 0.0f;
-  const float hz_mx = ixm >= 0 ? H[2 * N + ixm] : 0.0f, hy_mx = ixm >= 0 ? H[N + ixm] : 0.0f;
+  const float hz_my = iym >= 0 ? ld_chk(H + 2 * N, iym, N, err) : 0.0f;
+  const float hx_my = iym >= 0 ? ld_chk(H, iym, N, err) : 0.0f;
+  const float hy_mz = izm >= 0 ? ld_chk(H + N, izm, N, err) : 0.0f;
+  const float hx_mz = izm >= 0 ? ld_chk(H, izm, N, err) : 0.0f;
+  const float hz_mx = ixm >= 0 ? ld_chk(H + 2 * N, ixm, N, err) : 0.0f;
+  const float hy_mx = ixm >= 0 ? ld_chk(H + N, ixm, N, err) : 0.0f;
   float d_hz_dy = sub(hz, hz_my), d_hx_dy = sub(hx, hx_my);
   float d_hy_dz = sub(hy, hy_mz), d_hx_dz = sub(hx, hx_mz);
   float d_hz_dx = sub(hz, hz_mx), d_hy_dx = sub(hy, hy_mx);
   long long idx;
   float b, a, ik;
-  if (pml_slot(g.pml[0], 0, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik)) {
+  if (pml_slot(g.pml[0], 0, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik) &&
+      idx_ok(err, idx, g.pml[0].cells)) {
     const PmlAxis &P = g.pml[0];
     float p2 = P.psi_cur[2 * P.cells + idx], p3 = P.psi_cur[3 * P.cells + idx];
     d_hz_dx = pml_corr<FMA>(d_hz_dx, b, a, ik, p2);
@@ -123,7 +141,8 @@ __global__ void k_split_e(GridArgs g) {
     P.psi_nxt[2 * P.cells + idx] = p2;
     P.psi_nxt[3 * P.cells + idx] = p3;
   }
-  if (pml_slot(g.pml[1], 1, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik)) {
+  if (pml_slot(g.pml[1], 1, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik) &&
+      idx_ok(err, idx, g.pml[1].cells)) {
     const PmlAxis &P = g.pml[1];
     float p2 = P.psi_cur[2 * P.cells + idx], p3 = P.psi_cur[3 * P.cells + idx];
     d_hz_dy = pml_corr<FMA>(d_hz_dy, b, a, ik, p2);
@@ -131,7 +150,8 @@ __global__ void k_split_e(GridArgs g) {
     P.psi_nxt[2 * P.cells + idx] = p2;
     P.psi_nxt[3 * P.cells + idx] = p3;
   }
-  if (pml_slot(g.pml[2], 2, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik)) {
+  if (pml_slot(g.pml[2], 2, x, y, z, g.nx, g.ny, g.nz, idx, b, a, ik) &&
+      idx_ok(err, idx, g.pml[2].cells)) {
     const PmlAxis &P = g.pml[2];
     float p2 = P.psi_cur[2 * P.cells + idx], p3 = P.psi_cur[3 * P.cells + idx];
     d_hy_dz = pml_corr<FMA>(d_hy_dz, b, a, ik, p2);
@@ -251,8 +271,8 @@ __device__ void tail_body(const TailArgs &t, float *s_src) {
     const SrcDev q = t.src[s];
     const float v = st < q.nvals ? q.vals[st] : 0.0f;
     if (q.mode == 0) {
-      if (threadIdx.x == 0) {
-        const long long i = q.comp * N + (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x;
+      const long long i = q.comp * N + (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x;
+      if (threadIdx.x == 0 && idx_ok(t.err, i, 6 * N)) {
         if (f16) {
           const int b = q.z / kSlabPlanes, sh = t.shift_f[2 * b];
           const float d = enc16(t.f, i, t.prec, sh, __fadd_rn(dec16(t.f, i, t.prec, sh), v));
@@ -266,6 +286,7 @@ __device__ void tail_body(const TailArgs &t, float *s_src) {
       for (long long c = threadIdx.x; c < m; c += blockDim.x) {
         const long long yy = c % t.ny, zz = c / t.ny;
         const long long i = q.comp * N + (zz * t.ny + yy) * t.nx + q.x;
+        if (!idx_ok(t.err, i, 6 * N)) continue;
         if (f16) {
           const int b = static_cast<int>(zz) / kSlabPlanes;
           const float d = enc16(t.f, i, t.prec, t.shift_f[2 * b], v);
@@ -280,6 +301,7 @@ __device__ void tail_body(const TailArgs &t, float *s_src) {
   for (int p = threadIdx.x; p < t.nprobe; p += blockDim.x) {
     const ProbeDev q = t.probe[p];
     const long long i = q.comp * N + (static_cast<long long>(q.z) * t.ny + q.y) * t.nx + q.x;
+    if (!idx_ok(t.err, i, 6 * N)) continue;
     const float raw =
         f16 ? dec16(t.f, i, t.prec, t.shift_f[2 * (q.z / kSlabPlanes) + (q.comp >= 3)]) : t.f[i];
     if (q.record && st < q.nsteps) q.trace[st] = raw;

@@ -215,6 +215,15 @@ class DeviceFieldGrid:
         self._chk(_L.lib().wf_autotune(self._h, steps, C.byref(t), C.byref(ms)))
         return (t.tile_rows, t.z_chunk, t.stages), ms.value
 
+    def set_column_tiles(self, enable: bool) -> None:
+        """x-CPML slabs as 16-wide column tiles (default) or inside the wide
+        tiles; bit-identical results either way."""
+        self._chk(_L.lib().wf_set_column_tiles(self._h, int(bool(enable))))
+
+    @property
+    def column_tiles(self) -> bool:
+        return _L.lib().wf_column_tiles_active(self._h) == 1
+
     # -- read-back ------------------------------------------------------------
     def fields(self) -> np.ndarray:
         d = self.dims
@@ -230,6 +239,21 @@ class DeviceFieldGrid:
         out = np.empty(self.dims.voxel_count() * 6, np.float32)
         self._chk(_L.lib().wf_download_blocks(self._h, out.ctypes.data_as(C.c_void_p)))
         return out
+
+    def download_blocks_async(self, out) -> None:
+        """Starts a FieldBlock download into `out` (a writable buffer of
+        6*cells float32, ideally pinned, e.g. a pinned torch tensor's
+        numpy view) that overlaps with the following steps; complete once
+        sync() returns."""
+        a = np.asarray(out)
+        if a.dtype != np.float32 or a.size != self.dims.voxel_count() * 6 or not a.flags.c_contiguous:
+            raise ValueError("download buffer: contiguous float32, 6 values per voxel")
+        self._keep_download = out
+        self._chk(_L.lib().wf_download_blocks_async(self._h, a.ctypes.data_as(C.c_void_p)))
+
+    def reserve_download(self) -> None:
+        """Allocates the staging buffer of download_blocks_async now."""
+        self._chk(_L.lib().wf_reserve_download(self._h))
 
     def upload_blocks(self, blocks):
         a = np.ascontiguousarray(blocks, np.float32)
