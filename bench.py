@@ -491,6 +491,8 @@ def run_ours(args, rank, world, local_rank):
             g.set_pml(sc.pml)
         if args.tiling:
             g.set_tiling(*[int(v) for v in args.tiling.split(",")])
+        if args.columns == "off":
+            g.set_column_tiles(False)
         for s in sc.sources:
             g.add_source_values(s.x, s.y, s.z, s.component, s.values(sc.dt, total))
         for p in sc.probes:
@@ -504,6 +506,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- device-resident throughput (value) + fused-kernel roofline -------
     g = build()
     tiling = list(g.tiling())
+    column_tiles = g.column_tiles
     g.step(args.warmup)
     g.sync()
     g.set_timing(True)
@@ -616,6 +619,7 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {**scene_config(desc), "kernel": "fused TMA z-march", "arith": "exact (no FMA)",
+                       "x_cpml_column_tiles": column_tiles,
                        "tiling": {"tile_rows": tiling[0], "z_chunk": tiling[1],
                                   "stages": tiling[2]},
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
@@ -802,6 +806,8 @@ def main():
     ap.add_argument("--slabs", type=int, default=0,
                     help="two_spheres/random_spheres/demo_sphere on one GPU split into this many "
                          "z slabs with ghost-block exchange (FP32)")
+    ap.add_argument("--columns", default="on", choices=["on", "off"],
+                    help="x-CPML slabs as 16-wide column tiles (on) or inside the wide tiles")
     ap.add_argument("--replicas", action="store_true",
                     help="under torchrun: an independent replica of the workload per rank "
                          "(weak scaling) instead of one z slab per rank")
