@@ -52,7 +52,24 @@ def test_batch_matches_oracle_through_graph_replays(oracle):
         b.close()
 
 
-@pytest.mark.parametrize("tiling", [(8, 16, 4), (4, 1000, 3), (16, 8, 3)])
+def test_narrow_batch_is_one_launch_per_step_and_matches_oracle(oracle):
+    """The narrow tiling (tile_rows 32: every grid in 16-wide, 32-row tiles,
+    all items in one persistent launch of the all-axes body): one step
+    kernel plus the tail per step, bit for bit against the oracle, on grids
+    whose x extent is not a multiple of the 16-cell tile (40, 56, 120)."""
+    scenes = configs.batched_sweep(7, steps=70, seed=13, sizes=(32, 40, 56, 120))
+    b = configs.device_batch(scenes)
+    try:
+        b.set_tiling(32, 16, 3)
+        b.step(70)
+        b.sync()
+        assert b.kernel_launches == 2 * 70, b.kernel_launches
+        _check_against_oracle(oracle, b, scenes, 70)
+    finally:
+        b.close()
+
+
+@pytest.mark.parametrize("tiling", [(8, 16, 4), (4, 1000, 3), (16, 8, 3), (32, 1000, 3), (32, 7, 3)])
 def test_batch_tilings_match_oracle(oracle, tiling):
     scenes = configs.batched_sweep(5, steps=40, seed=11, sizes=(32, 48, 64))
     b = configs.device_batch(scenes)

@@ -617,6 +617,8 @@ struct wf_batch {
   int class_off[wf::kFusedClassCount] = {}, class_n[wf::kFusedClassCount] = {};
   int class_ctas[wf::kFusedClassCount] = {};
   int step_kernels = 0;    // non-empty classes: step-kernel launches per step
+  bool narrow = false;     // one launch over 16 x 32 tiles (tile_rows == kColTileRows)
+  int narrow_ctas = 0;
   int *d_counter = nullptr;  // one work counter per class
   // the class launches of a step run concurrently: forked from `stream` onto
   // these and joined back before the tail
@@ -647,6 +649,62 @@ void batch_drop(wf_batch *b) {
   b->built = false;
 }
 
+// A grid's TMA maps and fused arguments for the narrow batched step:
+// 16-wide, 32-row tiles over the whole grid (the boxes of the column tiles).
+wf_status narrow_batch_maps(wf_handle *h, int zchunk, wf::BatchScene *sc) {
+  if (!encode_fn()) return fail(h, WF_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  unsigned eb[4], hb[4], mb[3];
+  wf::fused_col_boxes(wf::kPrecF32, eb, hb, mb);
+  const cuuint64_t es = sizeof(float);
+  const cuuint64_t fdim[4] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz, 6};
+  const cuuint64_t fstr[3] = {(cuuint64_t)h->nx * es, (cuuint64_t)h->nx * h->ny * es,
+                              (cuuint64_t)h->N * es};
+  const cuuint64_t mdim[3] = {(cuuint64_t)h->nx, (cuuint64_t)h->ny, (cuuint64_t)h->nz};
+  const cuuint64_t mstr[2] = {(cuuint64_t)h->mat_pitch, (cuuint64_t)h->mat_pitch * h->ny};
+  const cuuint32_t ebox[4] = {eb[0], eb[1], eb[2], eb[3]};
+  const cuuint32_t hbox[4] = {hb[0], hb[1], hb[2], hb[3]};
+  const cuuint32_t mbox[3] = {mb[0], mb[1], mb[2]};
+  const int cur = h->cur;
+  const FusedConfig saved = h->cfg;
+  h->cfg = FusedConfig{wf::kColTileRows, zchunk, 3};
+  h->cols = false;
+  for (int p = 0; p < 2; ++p) {
+    CUtensorMap *m = sc->maps[p];
+    std::memset(m, 0, sizeof(CUtensorMap) * 3);
+    if (!encode(&m[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[p], fdim, fstr, ebox) ||
+        !encode(&m[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->fld[p], fdim, fstr, hbox) ||
+        !encode(&m[2], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->mat, mdim, mstr, mbox)) {
+      h->cfg = saved;
+      return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(narrow batch) failed");
+    }
+    h->cur = p;
+    FusedArgs a = fused_args(h);
+    a.tiles_x = (h->nx + wf::kColWidth - 1) / wf::kColWidth;
+    a.tiles_y = (h->ny + wf::kColTileRows - 1) / wf::kColTileRows;
+    sc->args[p] = a;
+  }
+  h->cur = cur;
+  h->cfg = saved;
+  h->maps_ok = false;  // a single-grid step rebuilds its own maps and lists
+  return WF_OK;
+}
+
+// CPML class of narrow batched item k (the axes whose slabs its cells, its
+// -x/-y halo or its warm-up plane meet): orders the items, costliest first.
+int narrow_item_class(const FusedArgs &a, int k) {
+  const int txi = k % a.tiles_x, tyi = (k / a.tiles_x) % a.tiles_y, zc = k / (a.tiles_x * a.tiles_y);
+  const int x0 = txi * wf::kColWidth, y0 = tyi * wf::kColTileRows;
+  const int xh = std::min(x0 + wf::kColWidth, a.g.nx) - 1;
+  const int yh = std::min(y0 + wf::kColTileRows, a.g.ny) - 1;
+  const int k0 = zc * a.zchunk, k1 = std::min(k0 + a.zchunk, a.g.nz);
+  const wf::PmlAxis &X = a.g.pml[0], &Y = a.g.pml[1], &Z = a.g.pml[2];
+  int mask = 0;
+  if (X.T > 0 && (x0 - 1 < X.T || xh >= a.g.nx - X.T)) mask |= 1;
+  if (Y.T > 0 && (y0 - 1 < Y.T || yh >= a.g.ny - Y.T)) mask |= 2;
+  if (Z.T > 0 && (k0 - 1 < Z.T || k1 - 1 >= a.g.nz - Z.T)) mask |= 4;
+  return mask;
+}
+
 // (Re)builds the batch's device tables when any grid's tables changed.
 wf_status batch_build(wf_batch *b) {
   bool fresh = b->built && b->versions.size() == b->h.size();
@@ -658,22 +716,30 @@ wf_status batch_build(wf_batch *b) {
   std::vector<int2> lists[wf::kFusedClassCount];
   std::vector<TailArgs> tails[2];
   b->have_tail = false;
+  b->narrow = wf::fused_batch_narrow(b->cfg);
   for (size_t i = 0; i < n; ++i) {
     wf_handle *h = b->h[i];
     for (const AxisState &A : h->ax)
       if (A.T > 0 && A.W > 64)
         return fail(nullptr, WF_ERR_UNSUPPORTED, "batched grids need CPML slabs of at most 64 cells");
-    h->cfg = b->cfg;
-    h->cfg_user_set = true;
-    wf_status st = build_maps(h, false);  // the batched kernel tiles the whole x range
+    wf_status st;
+    if (b->narrow) {
+      st = narrow_batch_maps(h, b->cfg.zchunk, &scenes[i]);
+    } else {
+      h->cfg = b->cfg;
+      h->cfg_user_set = true;
+      st = build_maps(h, false);  // the batched kernel tiles the whole x range
+    }
     if (st != WF_OK) return st;
     const int cur = h->cur;
     for (int p = 0; p < 2; ++p) {
       h->cur = p;
-      scenes[i].args[p] = fused_args(h);
-      scenes[i].maps[p][0] = h->maps[p].e;
-      scenes[i].maps[p][1] = h->maps[p].h;
-      scenes[i].maps[p][2] = h->maps[p].m;
+      if (!b->narrow) {
+        scenes[i].args[p] = fused_args(h);
+        scenes[i].maps[p][0] = h->maps[p].e;
+        scenes[i].maps[p][1] = h->maps[p].h;
+        scenes[i].maps[p][2] = h->maps[p].m;
+      }
       tails[p].push_back(tail_args(h));
     }
     h->cur = cur;
@@ -681,11 +747,17 @@ wf_status batch_build(wf_batch *b) {
     const FusedArgs &a = scenes[i].args[0];
     const int nit = a.tiles_x * a.tiles_y * ((h->nz + a.zchunk - 1) / a.zchunk);
     for (int k = 0; k < nit; ++k)
-      lists[wf::fused_item_class(a, b->cfg.ty, k)].push_back(make_int2(static_cast<int>(i), k));
+      lists[b->narrow ? narrow_item_class(a, k) : wf::fused_item_class(a, b->cfg.ty, k)].push_back(
+          make_int2(static_cast<int>(i), k));
   }
   std::vector<int2> items;
   b->step_kernels = 0;
-  for (int k = 0; k < wf::kFusedClassCount; ++k) {
+  if (b->narrow) {  // one list, costliest items first (three CPML axes ... interior)
+    static constexpr int kOrder[wf::kFusedClassCount] = {7, 5, 3, 6, 1, 4, 2, 0};
+    for (int k : kOrder) items.insert(items.end(), lists[k].begin(), lists[k].end());
+    b->step_kernels = 1;
+  }
+  for (int k = 0; k < wf::kFusedClassCount && !b->narrow; ++k) {
     b->class_off[k] = static_cast<int>(items.size());
     b->class_n[k] = static_cast<int>(lists[k].size());
     if (b->class_n[k]) ++b->step_kernels;
@@ -700,10 +772,16 @@ wf_status batch_build(wf_batch *b) {
     WF_CUDA(nullptr, h2d_sync(b->d_tails[p], tails[p].data(), sizeof(TailArgs) * n, b->stream));
   }
   b->n_items = static_cast<int>(items.size());
-  WF_CUDA(nullptr, wf::fused_batch_prepare(b->cfg));
   int sms = 0;
   WF_CUDA(nullptr, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev));
-  for (int k = 0; k < wf::kFusedClassCount; ++k) {
+  if (b->narrow) {
+    WF_CUDA(nullptr, wf::fused_batch_narrow_prepare());
+    const int per_sm = std::max(1, wf::fused_batch_narrow_ctas_per_sm());
+    b->narrow_ctas = std::max(1, std::min(sms * per_sm, b->n_items));
+  } else {
+    WF_CUDA(nullptr, wf::fused_batch_prepare(b->cfg));
+  }
+  for (int k = 0; k < wf::kFusedClassCount && !b->narrow; ++k) {
     const int per_sm = std::max(1, wf::fused_batch_ctas_per_sm(b->cfg, k));
     b->class_ctas[k] = std::max(1, std::min(sms * per_sm, b->class_n[k]));
   }
@@ -718,6 +796,11 @@ wf_status batch_build(wf_batch *b) {
 // streams forked from it and joined back; the classes write disjoint cells.
 wf_status batch_kernel(wf_batch *b, int cur) {
   WF_CUDA(nullptr, cudaMemsetAsync(b->d_counter, 0, sizeof(int) * wf::kFusedClassCount, b->stream));
+  if (b->narrow) {
+    WF_CUDA(nullptr, wf::launch_fused_batch_narrow(b->d_scenes, b->d_items, b->n_items, b->d_counter,
+                                                   cur, b->narrow_ctas, b->stream));
+    return WF_OK;
+  }
   WF_CUDA(nullptr, cudaEventRecord(b->fork_ev, b->stream));
   // costliest items first, interior last (as in the single-grid step)
   static constexpr int kOrder[wf::kFusedClassCount] = {7, 5, 3, 6, 1, 4, 2, 0};
@@ -2213,7 +2296,8 @@ wf_handle *wf_batch_handle(wf_batch *b, int i) {
 wf_status wf_batch_set_tiling(wf_batch *b, const wf_tiling *t) {
   if (!b || !t) return fail(nullptr, WF_ERR_ARG, "null argument");
   FusedConfig c{t->tile_rows, t->z_chunk, t->stages};
-  if (!wf::fused_supported(c, wf::kPrecF32)) return fail(nullptr, WF_ERR_ARG, "tiling not instantiated");
+  if (!wf::fused_supported(c, wf::kPrecF32) && !wf::fused_batch_narrow(c))
+    return fail(nullptr, WF_ERR_ARG, "tiling not instantiated");
   DeviceGuard guard(b->dev);
   WF_CUDA(nullptr, cudaStreamSynchronize(b->stream));
   batch_drop(b);
@@ -2333,12 +2417,12 @@ wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int tys[] = {4, 8, 16}, stg[] = {3, 4}, zcs[] = {8, 12, 16, 24, 32, 64, 128};
+  const int tys[] = {4, 8, 16, wf::kColTileRows}, stg[] = {3, 4}, zcs[] = {8, 12, 16, 24, 32, 64, 128};
   for (int ty : tys)
     for (int sg : stg)
       for (int zc : zcs) {
         FusedConfig c{ty, zc, sg};
-        if (!wf::fused_supported(c, wf::kPrecF32)) continue;
+        if (!wf::fused_supported(c, wf::kPrecF32) && !wf::fused_batch_narrow(c)) continue;
         batch_drop(b);
         b->cfg = c;
         if (batch_build(b) != WF_OK) continue;

@@ -114,6 +114,19 @@ cudaError_t launch_fused_batch(const FusedConfig &c, const BatchScene *scenes, c
   return cudaErrorInvalidValue;
 }
 
+bool fused_batch_narrow(const FusedConfig &c) {
+  return c.ty == kColTileRows && c.stages == kColStages && c.zchunk >= 1;
+}
+
+cudaError_t fused_batch_narrow_prepare() { return batch_narrow_prepare_t(); }
+
+cudaError_t launch_fused_batch_narrow(const BatchScene *scenes, const int2 *items, int n_items,
+                                      int *counter, int parity, int ctas, cudaStream_t s) {
+  return batch_narrow_launch_t(scenes, items, n_items, counter, parity, ctas, s);
+}
+
+int fused_batch_narrow_ctas_per_sm() { return batch_narrow_ctas_per_sm_t(); }
+
 int fused_batch_ctas_per_sm(const FusedConfig &c, int ax) {
 #define X(T, S_) if (c.ty == T && c.stages == S_) return batch_ctas_per_sm_t<T, S_>(ax);
   WF_FUSED_CONFIGS(X)

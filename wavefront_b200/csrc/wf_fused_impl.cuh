@@ -781,11 +781,14 @@ __global__ void __launch_bounds__(Layout<TY, S, ST, LX>::THREADS, kCtasPerSm<TY,
 // and its TMA maps read from global memory.  The mbarrier ring is
 // re-initialised per item (every copy of the previous item has completed:
 // the body consumes or drains all it issued).
-template <int TY, int S, int AX>
-__global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, float> : 1)
+// LX < 32: the tiles are 4*LX cells wide (x0 = txi * 4*LX), as the x-CPML
+// column tiles of the single-grid step, so that narrow grids keep their
+// lanes busy.
+template <int TY, int S, int AX, int LX = 32>
+__global__ void __launch_bounds__(Layout<TY, S, float, LX>::THREADS, kCtasPerSm<TY, LX, AX, float>)
     k_fused_batch(const BatchScene *scenes, const int2 *items, int n_items, int *counter,
                   int parity) {
-  using L = Layout<TY, S, float>;
+  using L = Layout<TY, S, float, LX>;
   extern __shared__ unsigned char smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
@@ -814,7 +817,7 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, float
     item /= a.tiles_x;
     const int tyi = item % a.tiles_y;
     const int zc = item / a.tiles_y;
-    const int x0 = txi * kTileX, y0 = tyi * TY;
+    const int x0 = txi * L::TW, y0 = tyi * TY;
     const int k0 = zc * a.zchunk;
     const int k1 = min(k0 + a.zchunk, a.g.nz);
     float4 *s_coef = reinterpret_cast<float4 *>(smem);
@@ -835,10 +838,37 @@ __global__ void __launch_bounds__(32 * (TY + 1), TY <= 4 ? kCtasPerSm4<AX, float
     }
     first = false;
     __syncthreads();
-    fused_body<TY, S, false, AX, float>(&sc->maps[parity][0], &sc->maps[parity][1],
-                                        &sc->maps[parity][2], a, smem, x0, y0, k0, k1,
-                                        min(x0 + kTileX, a.g.nx));
+    fused_body<TY, S, false, AX, float, LX>(&sc->maps[parity][0], &sc->maps[parity][1],
+                                            &sc->maps[parity][2], a, smem, x0, y0, k0, k1,
+                                            min(x0 + L::TW, a.g.nx));
   }
+}
+
+// The batched step in one launch: every item of every grid on 16-wide,
+// 32-row tiles, all through the body that carries the psi code of all three
+// axes (its slab flags are per lane and per plane).
+using BatchNarrowL = Layout<kColRows, kColStages, float, kColLanes>;
+
+cudaError_t batch_narrow_prepare_t() {
+  return cudaFuncSetAttribute(k_fused_batch<kColRows, kColStages, 7, kColLanes>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, BatchNarrowL::BYTES);
+}
+
+cudaError_t batch_narrow_launch_t(const BatchScene *scenes, const int2 *items, int n_items,
+                                  int *counter, int parity, int ctas, cudaStream_t s) {
+  k_fused_batch<kColRows, kColStages, 7, kColLanes>
+      <<<ctas, BatchNarrowL::THREADS, BatchNarrowL::BYTES, s>>>(scenes, items, n_items, counter,
+                                                               parity);
+  return cudaGetLastError();
+}
+
+int batch_narrow_ctas_per_sm_t() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, k_fused_batch<kColRows, kColStages, 7, kColLanes>, BatchNarrowL::THREADS,
+          BatchNarrowL::BYTES) != cudaSuccess)
+    return 0;
+  return n;
 }
 
 #define WF_AX_CLASSES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7)

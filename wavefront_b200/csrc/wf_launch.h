@@ -100,6 +100,14 @@ cudaError_t launch_fused_batch(const FusedConfig &c, const BatchScene *scenes, c
                                cudaStream_t s);
 // CTAs per SM the batched kernel of a tiling and class fits (for sizing `ctas`).
 int fused_batch_ctas_per_sm(const FusedConfig &c, int ax);
+// The narrow batched step (tile_rows == kColTileRows): every grid cut into
+// kColWidth x kColTileRows tiles, all items in one persistent launch of the
+// all-axes body.
+bool fused_batch_narrow(const FusedConfig &c);
+cudaError_t fused_batch_narrow_prepare();
+cudaError_t launch_fused_batch_narrow(const BatchScene *scenes, const int2 *items, int n_items,
+                                      int *counter, int parity, int ctas, cudaStream_t s);
+int fused_batch_narrow_ctas_per_sm();
 // The step tail of n grids at once: one CTA per grid, t[i] as for launch_tail.
 cudaError_t launch_tail_batch(const TailArgs *t, int n, cudaStream_t s);
 
