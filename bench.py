@@ -504,7 +504,12 @@ def run_ours(args, rank, world, local_rank):
         return load(DeviceFieldGrid(sc.dims, kernel=kernel, device=local_rank, precision=PRECISION))
 
     # ---- device-resident throughput (value) + fused-kernel roofline -------
+    tcold = time.perf_counter()
     g = build()
+    if PRECISION == "f32" and not args.no_e2e:
+        g.reserve_download()  # the e2e leg's snapshot staging buffer, cached when g closes
+    g.sync()
+    cold_create_ms = (time.perf_counter() - tcold) * 1e3
     tiling = list(g.tiling())
     column_tiles = g.column_tiles
     g.step(args.warmup)
@@ -565,13 +570,15 @@ def run_ours(args, rank, world, local_rank):
         # the handle's device allocation is set-up, outside the timed region
         # (as the reference allocates its grids before engine::run times
         # anything); every host<->device data movement is inside it
-        tc = time.perf_counter()
+        # everything is timed, the handle's creation included: its device
+        # memory comes from the library's cache of the blocks the first
+        # handle freed (a cold first creation is reported apart)
+        t0 = time.perf_counter()
         g = DeviceFieldGrid(sc.dims, kernel="fused", device=local_rank, precision=PRECISION)
         async_snap = PRECISION == "f32"
         if async_snap:
-            g.reserve_download()  # the snapshot's staging buffer: set-up as well
-        g.sync()
-        t0 = time.perf_counter()
+            g.reserve_download()  # the snapshot's staging buffer
+        tc = time.perf_counter()
         load(g)
         g.sync()
         t_built = time.perf_counter()
@@ -591,8 +598,9 @@ def run_ours(args, rank, world, local_rank):
             L.check(L.lib().wf_download_blocks(g._h, C.c_void_p(snap.data_ptr())), g._h)
         g.sync()  # the snapshot download has landed
         e2e_s = time.perf_counter() - t0
-        phases = {"create_untimed": round((t0 - tc) * 1e3, 1),
-                  "upload": round((t_built - t0) * 1e3, 1),
+        phases = {"create": round((tc - t0) * 1e3, 1),
+                  "first_handle_create_and_upload_cold_untimed": round(cold_create_ms, 1),
+                  "upload": round((t_built - tc) * 1e3, 1),
                   "steps_and_probe_sums": round((t_stepped - t_built) * 1e3, 1),
                   "snapshot_wait": round((t0 + e2e_s - t_stepped) * 1e3, 1)}
         g.close()
@@ -605,11 +613,11 @@ def run_ours(args, rank, world, local_rank):
         e2e_line = {"value": round(e2e, 1), "unit": METRIC,
                     "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h / args.steps),
-                    "includes": "scene or material upload (pinned), CPML and source/probe "
-                                "table uploads, K steps, probe sums, the FieldBlock snapshot of "
-                                "step 0 downloaded to pinned memory (FP32: while the other steps "
-                                "run); the handle's device allocation, its snapshot staging "
-                                "buffer included, is untimed set-up (phases_ms.create_untimed)",
+                    "includes": "the handle's creation (device memory from the library's "
+                                "cache, warmed by the first handle of the run), scene or material "
+                                "upload (pinned), CPML and source/probe table uploads, K steps, "
+                                "probe sums, the FieldBlock snapshot of step 0 downloaded to "
+                                "pinned memory (FP32: while the other steps run)",
                     "phases_ms": phases}
 
     if rank == 0:

@@ -417,6 +417,19 @@ wf_status wf_batch_set_tiling(wf_batch *b, const wf_tiling *t);
  * and psi (sources and probes do not run during the trials). */
 wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best_ms);
 
+/* ---- device memory cache (no reference counterpart) ---------------------- */
+
+/* Device blocks the library frees (a destroyed handle's state buffers,
+ * material ids, psi arrays and tables) are kept in a per-device cache, at
+ * most 16 GiB per device, and handed to the next allocation of the same
+ * rounded size, so a handle created after another of the same shape skips
+ * CUDA's page mapping.  Freeing waits for the device first, as cudaFree
+ * does.  An allocation that runs out of memory returns the device's cache
+ * to CUDA and tries again.  wf_release_cached_memory returns the cache of
+ * `device` (-1: every device) to CUDA now; wf_cached_bytes reports it. */
+wf_status wf_release_cached_memory(int device);
+int64_t wf_cached_bytes(int device);
+
 /* ---- allocation-free stepping of caller-owned fields --------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -119,3 +119,27 @@ def test_snapshot_write_failure_surfaces_as_io_error():
         g.sync()
     finally:
         g.close()
+
+
+def test_device_memory_cache_reuses_and_releases():
+    """A destroyed handle's device blocks go to the library's cache and the
+    next handle of the same shape takes them back; the cache returns its
+    blocks to CUDA on request, and a handle built from reused (dirty)
+    blocks still starts from zero fields."""
+    lib = L.lib()
+    dims = wf.GridDims(64, 64, 64)
+    lib.wf_release_cached_memory(-1)
+    assert lib.wf_cached_bytes(0) == 0
+    g = wf.DeviceFieldGrid(dims)
+    g.set_fields(np.ones((6, 64, 64, 64), np.float32))
+    g.close()
+    cached = lib.wf_cached_bytes(0)
+    assert cached >= 2 * 6 * 4 * 64 ** 3  # both state buffers at least
+    g = wf.DeviceFieldGrid(dims)
+    try:
+        assert lib.wf_cached_bytes(0) < cached
+        assert not np.any(g.fields())
+    finally:
+        g.close()
+    assert lib.wf_release_cached_memory(-1) == L.WF_OK
+    assert lib.wf_cached_bytes(0) == 0

@@ -42,7 +42,8 @@ EXPORTS = [
     "wf_material_coeffs", "wf_effective_pml_thickness_blocks", "wf_pml_profile",
     "wf_waveform_eval", "wf_source_values", "wf_probe_first_step", "wf_probe_tables",
     "wf_spectrum", "wf_scene_voxelize", "wf_demo_sphere",
-    "wf_step_fields_noalloc", "wf_noalloc_last_error",
+    "wf_step_fields_noalloc", "wf_noalloc_last_error", "wf_release_cached_memory",
+    "wf_cached_bytes",
 ]
 
 
@@ -171,6 +172,10 @@ def lib() -> C.CDLL:
         L.wf_nn_mse.argtypes = [vp, vp, vp, vp, C.c_int64, vp]
         L.wf_nn_adam.argtypes = [vp, vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float,
                                  C.c_float, C.c_int, vp]
+        L.wf_release_cached_memory.argtypes = [C.c_int]
+        L.wf_release_cached_memory.restype = S
+        L.wf_cached_bytes.argtypes = [C.c_int]
+        L.wf_cached_bytes.restype = C.c_int64
         L.wf_nn_set_tensor_cores.argtypes = [C.c_int]
         L.wf_nn_set_tensor_cores.restype = S
         L.wf_nn_tensor_core_timeouts.argtypes = []

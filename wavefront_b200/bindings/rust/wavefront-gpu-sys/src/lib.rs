@@ -148,6 +148,8 @@ extern "C" {
     pub fn wf_batch_get_tiling(b: *const wf_batch, out: *mut wf_tiling) -> wf_status;
     pub fn wf_batch_set_tiling(b: *mut wf_batch, t: *const wf_tiling) -> wf_status;
     pub fn wf_batch_autotune(b: *mut wf_batch, steps: c_int, best: *mut wf_tiling, best_ms: *mut f32) -> wf_status;
+    pub fn wf_release_cached_memory(device: c_int) -> wf_status;
+    pub fn wf_cached_bytes(device: c_int) -> i64;
     pub fn wf_step_fields_noalloc(fields6: *mut f32, ids: *const u8, table_q16: *const [i32; 4], nx: c_int, ny: c_int, nz: c_int, boundary: *const i32, arith: c_int, nsteps: c_int, stream: *mut c_void) -> wf_status;
     pub fn wf_noalloc_last_error() -> *const c_char;
     pub fn wf_q16_from_f32(v: f32) -> i32;

@@ -24,6 +24,7 @@
 #include "../../include/wavefront_gpu.h"
 #include "wf_closure.h"
 #include "wf_launch.h"
+#include "wf_pool.h"
 #include "wf_scene.h"
 
 using wf::FusedArgs;
@@ -326,9 +327,9 @@ wf_status build_maps(wf_handle *h, bool allow_cols = true) {
     h->col_n[k] = static_cast<int>(clists[k].size());
     all.insert(all.end(), clists[k].begin(), clists[k].end());
   }
-  cudaFree(h->d_items);
+  wf::dev_free(h->d_items);
   h->d_items = nullptr;
-  WF_CUDA(h, cudaMalloc(&h->d_items, sizeof(int) * std::max<size_t>(all.size(), 1)));
+  WF_CUDA(h, wf::dev_alloc(&h->d_items, sizeof(int) * std::max<size_t>(all.size(), 1)));
   WF_CUDA(h, h2d_sync(h->d_items, all.data(), sizeof(int) * all.size(), h->stream));
   h->maps_ok = true;
   return WF_OK;
@@ -556,20 +557,20 @@ wf_status upload_src_probe_tables(wf_handle *h) {
   drop_graphs(h);
   ++h->version;
   h->shifts_dirty = true;  // source amplitudes enter the 16-bit shifts
-  if (h->d_src) cudaFree(h->d_src);
-  if (h->d_probe) cudaFree(h->d_probe);
+  if (h->d_src) wf::dev_free(h->d_src);
+  if (h->d_probe) wf::dev_free(h->d_probe);
   h->d_src = nullptr;
   h->d_probe = nullptr;
   if (!h->srcs.empty()) {
     std::vector<SrcDev> v;
     for (auto &s : h->srcs) v.push_back(s.d);
-    WF_CUDA(h, cudaMalloc(&h->d_src, sizeof(SrcDev) * v.size()));
+    WF_CUDA(h, wf::dev_alloc(&h->d_src, sizeof(SrcDev) * v.size()));
     WF_CUDA(h, h2d_sync(h->d_src, v.data(), sizeof(SrcDev) * v.size(), h->stream));
   }
   if (!h->probes.empty()) {
     std::vector<ProbeDev> v;
     for (auto &p : h->probes) v.push_back(p.d);
-    WF_CUDA(h, cudaMalloc(&h->d_probe, sizeof(ProbeDev) * v.size()));
+    WF_CUDA(h, wf::dev_alloc(&h->d_probe, sizeof(ProbeDev) * v.size()));
     WF_CUDA(h, h2d_sync(h->d_probe, v.data(), sizeof(ProbeDev) * v.size(), h->stream));
   }
   return WF_OK;
@@ -639,10 +640,10 @@ void batch_drop(wf_batch *b) {
     if (g) cudaGraphExecDestroy(g);
     g = nullptr;
   }
-  cudaFree(b->d_scenes);
-  cudaFree(b->d_items);
-  cudaFree(b->d_tails[0]);
-  cudaFree(b->d_tails[1]);
+  wf::dev_free(b->d_scenes);
+  wf::dev_free(b->d_items);
+  wf::dev_free(b->d_tails[0]);
+  wf::dev_free(b->d_tails[1]);
   b->d_scenes = nullptr;
   b->d_items = nullptr;
   b->d_tails[0] = b->d_tails[1] = nullptr;
@@ -763,12 +764,12 @@ wf_status batch_build(wf_batch *b) {
     if (b->class_n[k]) ++b->step_kernels;
     items.insert(items.end(), lists[k].begin(), lists[k].end());
   }
-  WF_CUDA(nullptr, cudaMalloc(&b->d_scenes, sizeof(wf::BatchScene) * n));
+  WF_CUDA(nullptr, wf::dev_alloc(&b->d_scenes, sizeof(wf::BatchScene) * n));
   WF_CUDA(nullptr, h2d_sync(b->d_scenes, scenes.data(), sizeof(wf::BatchScene) * n, b->stream));
-  WF_CUDA(nullptr, cudaMalloc(&b->d_items, sizeof(int2) * std::max<size_t>(items.size(), 1)));
+  WF_CUDA(nullptr, wf::dev_alloc(&b->d_items, sizeof(int2) * std::max<size_t>(items.size(), 1)));
   WF_CUDA(nullptr, h2d_sync(b->d_items, items.data(), sizeof(int2) * items.size(), b->stream));
   for (int p = 0; p < 2; ++p) {
-    WF_CUDA(nullptr, cudaMalloc(&b->d_tails[p], sizeof(TailArgs) * n));
+    WF_CUDA(nullptr, wf::dev_alloc(&b->d_tails[p], sizeof(TailArgs) * n));
     WF_CUDA(nullptr, h2d_sync(b->d_tails[p], tails[p].data(), sizeof(TailArgs) * n, b->stream));
   }
   b->n_items = static_cast<int>(items.size());
@@ -922,7 +923,7 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
   if ((e = cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup_fail(cuda_fail(nullptr, e, "cudaEventCreate"));
   for (int b = 0; b < 2; ++b) {
-    e = cudaMalloc(&h->fld[b], elem_bytes(h) * 6 * h->N);
+    e = wf::dev_alloc(&h->fld[b], elem_bytes(h) * 6 * h->N);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(fields)"));
     e = cudaMemsetAsync(h->fld[b], 0, elem_bytes(h) * 6 * h->N, h->stream);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMemset(fields)"));
@@ -930,24 +931,24 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
   if (store16(h)) {
     h->nslab = h->nz / 8;
     const size_t sb = sizeof(int) * 2 * h->nslab;
-    if ((e = cudaMalloc(&h->shift[0], sb)) != cudaSuccess ||
-        (e = cudaMalloc(&h->shift[1], sb)) != cudaSuccess ||
+    if ((e = wf::dev_alloc(&h->shift[0], sb)) != cudaSuccess ||
+        (e = wf::dev_alloc(&h->shift[1], sb)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->shift[0], 0, sb, h->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->shift[1], 0, sb, h->stream)) != cudaSuccess ||
-        (e = cudaMalloc(&h->slab_max, sb)) != cudaSuccess ||
+        (e = wf::dev_alloc(&h->slab_max, sb)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->slab_max, 0, sb, h->stream)) != cudaSuccess ||
-        (e = cudaMalloc(&h->d_ovf, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = wf::dev_alloc(&h->d_ovf, sizeof(unsigned long long))) != cudaSuccess ||
         (e = cudaMemsetAsync(h->d_ovf, 0, sizeof(unsigned long long), h->stream)) != cudaSuccess)
       return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(storage scales)"));
   }
   const size_t mbytes = static_cast<size_t>(h->mat_pitch) * d->ny * d->nz;
-  if ((e = cudaMalloc(&h->mat, mbytes)) != cudaSuccess ||
+  if ((e = wf::dev_alloc(&h->mat, mbytes)) != cudaSuccess ||
       (e = cudaMemsetAsync(h->mat, 0, mbytes, h->stream)) != cudaSuccess ||
-      (e = cudaMalloc(&h->coef, sizeof(float4) * 256)) != cudaSuccess ||
+      (e = wf::dev_alloc(&h->coef, sizeof(float4) * 256)) != cudaSuccess ||
       (e = cudaMemsetAsync(h->coef, 0, sizeof(float4) * 256, h->stream)) != cudaSuccess ||
-      (e = cudaMalloc(&h->d_step, sizeof(long long))) != cudaSuccess ||
+      (e = wf::dev_alloc(&h->d_step, sizeof(long long))) != cudaSuccess ||
       (e = cudaMemsetAsync(h->d_step, 0, sizeof(long long), h->stream)) != cudaSuccess ||
-      (e = cudaMalloc(&h->d_err, sizeof(int))) != cudaSuccess ||
+      (e = wf::dev_alloc(&h->d_err, sizeof(int))) != cudaSuccess ||
       (e = cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream)) != cudaSuccess)
     return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(state)"));
   if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
@@ -983,31 +984,31 @@ wf_status wf_destroy(wf_handle *h) {
   }
   if (h->staged) cudaEventDestroy(h->staged);
   if (h->copied) cudaEventDestroy(h->copied);
-  cudaFree(h->d_stage);
-  for (auto &f : h->fld) cudaFree(f);
-  for (auto &s : h->shift) cudaFree(s);
-  for (auto &w : h->cl_w) cudaFree(w);
-  cudaFree(h->cl_buf);
-  cudaFree(h->cl_face);
-  cudaFree(h->slab_max);
-  cudaFree(h->d_ovf);
-  cudaFree(h->mat);
-  cudaFree(h->coef);
-  cudaFree(h->d_step);
-  cudaFree(h->d_err);
-  cudaFree(h->d_src);
-  cudaFree(h->d_probe);
-  cudaFree(h->d_items);
+  wf::dev_free(h->d_stage);
+  for (auto &f : h->fld) wf::dev_free(f);
+  for (auto &s : h->shift) wf::dev_free(s);
+  for (auto &w : h->cl_w) wf::dev_free(w);
+  wf::dev_free(h->cl_buf);
+  wf::dev_free(h->cl_face);
+  wf::dev_free(h->slab_max);
+  wf::dev_free(h->d_ovf);
+  wf::dev_free(h->mat);
+  wf::dev_free(h->coef);
+  wf::dev_free(h->d_step);
+  wf::dev_free(h->d_err);
+  wf::dev_free(h->d_src);
+  wf::dev_free(h->d_probe);
+  wf::dev_free(h->d_items);
   for (auto &a : h->ax) {
-    cudaFree(a.prof);
-    cudaFree(a.psi[0]);
-    cudaFree(a.psi[1]);
+    wf::dev_free(a.prof);
+    wf::dev_free(a.psi[0]);
+    wf::dev_free(a.psi[1]);
   }
-  for (auto &s : h->srcs) cudaFree(s.vals);
+  for (auto &s : h->srcs) wf::dev_free(s.vals);
   for (auto &p : h->probes) {
-    cudaFree(p.base);
-    cudaFree(p.n);
-    cudaFree(p.trace);
+    wf::dev_free(p.base);
+    wf::dev_free(p.n);
+    wf::dev_free(p.trace);
   }
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1151,9 +1152,9 @@ wf_status wf_set_pml(wf_handle *h, int axis, int T, const float *b, const float 
   drop_graphs(h);
   h->maps_ok = false;  // the work lists depend on the CPML slabs
   AxisState &A = h->ax[axis];
-  cudaFree(A.prof);
-  cudaFree(A.psi[0]);
-  cudaFree(A.psi[1]);
+  wf::dev_free(A.prof);
+  wf::dev_free(A.psi[0]);
+  wf::dev_free(A.psi[1]);
   A = AxisState();
   if (T == 0) return WF_OK;
   A.T = T;
@@ -1171,10 +1172,10 @@ wf_status wf_set_pml(wf_handle *h, int axis, int T, const float *b, const float 
     prof[A.W + s] = a[c];
     prof[2 * A.W + s] = ik[c];
   }
-  WF_CUDA(h, cudaMalloc(&A.prof, sizeof(float) * prof.size()));
+  WF_CUDA(h, wf::dev_alloc(&A.prof, sizeof(float) * prof.size()));
   WF_CUDA(h, h2d_sync(A.prof, prof.data(), sizeof(float) * prof.size(), h->stream));
   for (int k = 0; k < 2; ++k) {
-    WF_CUDA(h, cudaMalloc(&A.psi[k], sizeof(float) * 4 * A.cells));
+    WF_CUDA(h, wf::dev_alloc(&A.psi[k], sizeof(float) * 4 * A.cells));
     WF_CUDA(h, memset_sync(A.psi[k], 0, sizeof(float) * 4 * A.cells, h->stream));  // PmlAux::ZERO
   }
   return WF_OK;
@@ -1191,7 +1192,7 @@ wf_status wf_add_source(wf_handle *h, int x, int y, int z, int comp, int mode,
   DeviceGuard guard(h->dev);
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   SrcRec r{};
-  WF_CUDA(h, cudaMalloc(&r.vals, sizeof(float) * std::max(nvalues, 1)));
+  WF_CUDA(h, wf::dev_alloc(&r.vals, sizeof(float) * std::max(nvalues, 1)));
   if (nvalues > 0)
     WF_CUDA(h, h2d_sync(r.vals, values, sizeof(float) * nvalues, h->stream));
   r.d.comp = comp;
@@ -1220,7 +1221,7 @@ wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
   ProbeRec r{};
   const size_t tab = static_cast<size_t>(nsteps) * nfreq;
   const size_t total = 2 * tab + 2 * static_cast<size_t>(nfreq) + 1;
-  WF_CUDA(h, cudaMalloc(&r.base, sizeof(double) * total));
+  WF_CUDA(h, wf::dev_alloc(&r.base, sizeof(double) * total));
   WF_CUDA(h, memset_sync(r.base, 0, sizeof(double) * total, h->stream));
   r.cos_tab = r.base;
   r.sin_tab = r.base + tab;
@@ -1230,9 +1231,9 @@ wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
     WF_CUDA(h, h2d_sync(r.cos_tab, cos_tab, sizeof(double) * tab, h->stream));
     WF_CUDA(h, h2d_sync(r.sin_tab, sin_tab, sizeof(double) * tab, h->stream));
   }
-  WF_CUDA(h, cudaMalloc(&r.n, sizeof(unsigned long long)));
+  WF_CUDA(h, wf::dev_alloc(&r.n, sizeof(unsigned long long)));
   WF_CUDA(h, memset_sync(r.n, 0, sizeof(unsigned long long), h->stream));
-  WF_CUDA(h, cudaMalloc(&r.trace, sizeof(float) * std::max(nsteps, 1)));
+  WF_CUDA(h, wf::dev_alloc(&r.trace, sizeof(float) * std::max(nsteps, 1)));
   WF_CUDA(h, memset_sync(r.trace, 0, sizeof(float) * std::max(nsteps, 1), h->stream));
   r.d.comp = comp;
   r.d.x = x;
@@ -1326,7 +1327,7 @@ wf_status wf_reserve_download(wf_handle *h) {
     return fail(h, WF_ERR_UNSUPPORTED, "asynchronous downloads need FP32 storage (use wf_download_blocks)");
   DeviceGuard guard(h->dev);
   if (!h->d_stage) {
-    WF_CUDA(h, cudaMalloc(&h->d_stage, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, wf::dev_alloc(&h->d_stage, sizeof(float) * 6 * h->N));
     WF_CUDA(h, cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking));
     WF_CUDA(h, cudaEventCreateWithFlags(&h->staged, cudaEventDisableTiming));
     WF_CUDA(h, cudaEventCreateWithFlags(&h->copied, cudaEventDisableTiming));
@@ -1384,12 +1385,12 @@ wf_status wf_probe_trace(wf_handle *h, int p, float *out, int n) {
 // Device scratch of 6*N floats for 16-bit conversions (freed on scope exit).
 struct Scratch {
   float *p = nullptr;
-  ~Scratch() { cudaFree(p); }
+  ~Scratch() { wf::dev_free(p); }
 };
 
 // FP32 SoA copy of the current 16-bit state into `tmp`.
 wf_status decode_current(wf_handle *h, Scratch &tmp) {
-  WF_CUDA(h, cudaMalloc(&tmp.p, sizeof(float) * 6 * h->N));
+  WF_CUDA(h, wf::dev_alloc(&tmp.p, sizeof(float) * 6 * h->N));
   WF_CUDA(h, wf::launch_decode_state(h->fld[h->cur], tmp.p, h->precision, h->nx, h->ny, h->nz,
                                      h->shift[h->cur], h->stream));
   return WF_OK;
@@ -1426,7 +1427,7 @@ wf_status wf_set_fields(wf_handle *h, const float *in6) {
   WF_CUDA(h, cudaStreamSynchronize(h->stream));
   if (store16(h)) {
     Scratch tmp;
-    WF_CUDA(h, cudaMalloc(&tmp.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, wf::dev_alloc(&tmp.p, sizeof(float) * 6 * h->N));
     WF_CUDA(h, cudaMemcpyAsync(tmp.p, in6, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice,
                                h->stream));
     wf_status s = encode_current(h, tmp.p);
@@ -1445,7 +1446,7 @@ wf_status wf_download_blocks(wf_handle *h, void *out) {
     Scratch soa, blk;
     wf_status s = decode_current(h, soa);
     if (s != WF_OK) return s;
-    WF_CUDA(h, cudaMalloc(&blk.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, wf::dev_alloc(&blk.p, sizeof(float) * 6 * h->N));
     WF_CUDA(h, wf::launch_soa_to_blocks(soa.p, blk.p, h->nx, h->ny, h->nz, h->stream));
     WF_CUDA(h, cudaMemcpyAsync(out, blk.p, sizeof(float) * 6 * h->N, cudaMemcpyDeviceToHost,
                                h->stream));
@@ -1465,8 +1466,8 @@ wf_status wf_upload_blocks(wf_handle *h, const void *in) {
   DeviceGuard guard(h->dev);
   if (store16(h)) {
     Scratch blk, soa;
-    WF_CUDA(h, cudaMalloc(&blk.p, sizeof(float) * 6 * h->N));
-    WF_CUDA(h, cudaMalloc(&soa.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, wf::dev_alloc(&blk.p, sizeof(float) * 6 * h->N));
+    WF_CUDA(h, wf::dev_alloc(&soa.p, sizeof(float) * 6 * h->N));
     WF_CUDA(h, cudaMemcpyAsync(blk.p, in, sizeof(float) * 6 * h->N, cudaMemcpyHostToDevice,
                                h->stream));
     WF_CUDA(h, wf::launch_blocks_to_soa(blk.p, soa.p, h->nx, h->ny, h->nz, h->stream));
@@ -1736,14 +1737,14 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
                         6u * 6 * kClHidden * 27};
   const void *src[3] = {w1, w2, w3};
   for (int l = 0; l < 3; ++l) {
-    if (!h->cl_w[l]) WF_CUDA(h, cudaMalloc(&h->cl_w[l], 2 * nw[l]));
+    if (!h->cl_w[l]) WF_CUDA(h, wf::dev_alloc(&h->cl_w[l], 2 * nw[l]));
     WF_CUDA(h, h2d_sync(h->cl_w[l], src[l], 2 * nw[l], h->stream, cudaMemcpyDefault));
   }
   if (!h->cl_buf) {
     const long long P = static_cast<long long>(wf::kBandDepth) * h->nx * h->nx;
-    WF_CUDA(h, cudaMalloc(&h->cl_buf, sizeof(float) * (6 * P * (wf::kBandIn + 2 * kClHidden + 6) + 16)));
+    WF_CUDA(h, wf::dev_alloc(&h->cl_buf, sizeof(float) * (6 * P * (wf::kBandIn + 2 * kClHidden + 6) + 16)));
     const int faces[6] = {0, 1, 2, 3, 4, 5};
-    WF_CUDA(h, cudaMalloc(&h->cl_face, sizeof(faces)));
+    WF_CUDA(h, wf::dev_alloc(&h->cl_face, sizeof(faces)));
     WF_CUDA(h, h2d_sync(h->cl_face, faces, sizeof(faces), h->stream));
   }
   h->cl_ge = gain_e;
@@ -1925,8 +1926,8 @@ void snapshot_thread(wf_snapshot_writer *w) {
 void snapshot_free(wf_snapshot_writer *w) {
   for (void *p : w->host)
     if (p) cudaFreeHost(p);
-  cudaFree(w->d_stage);
-  cudaFree(w->d_soa);
+  wf::dev_free(w->d_stage);
+  wf::dev_free(w->d_soa);
   if (w->staged) cudaEventDestroy(w->staged);
   for (cudaEvent_t e : w->copied)
     if (e) cudaEventDestroy(e);
@@ -1954,8 +1955,8 @@ wf_status wf_snapshot_open(wf_handle *h, const char *path, wf_snapshot_writer **
   }
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaHostAlloc(&w->host[i], w->bytes, cudaHostAllocDefault);
-  if (e == cudaSuccess) e = cudaMalloc(&w->d_stage, w->bytes);
-  if (e == cudaSuccess && store16(h)) e = cudaMalloc(&w->d_soa, w->bytes);
+  if (e == cudaSuccess) e = wf::dev_alloc(&w->d_stage, w->bytes);
+  if (e == cudaSuccess && store16(h)) e = wf::dev_alloc(&w->d_soa, w->bytes);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->copy, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w->staged, cudaEventDisableTiming);
   for (int i = 0; i < 2 && e == cudaSuccess; ++i)
@@ -2238,7 +2239,7 @@ wf_status wf_batch_create(int n, const wf_grid_desc *descs, wf_batch **out) {
     delete b;
     return cuda_fail(nullptr, e, "cudaStreamCreate");
   }
-  if ((e = cudaMalloc(&b->d_counter, sizeof(int) * wf::kFusedClassCount)) != cudaSuccess) {
+  if ((e = wf::dev_alloc(&b->d_counter, sizeof(int) * wf::kFusedClassCount)) != cudaSuccess) {
     wf_batch_destroy(b);
     return cuda_fail(nullptr, e, "cudaMalloc(counter)");
   }
@@ -2272,7 +2273,7 @@ wf_status wf_batch_destroy(wf_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_drop(b);
   for (wf_handle *h : b->h) wf_destroy(h);
-  cudaFree(b->d_counter);
+  wf::dev_free(b->d_counter);
   for (int k = 0; k < wf::kFusedClassCount - 1; ++k) {
     if (b->side[k]) {
       cudaStreamSynchronize(b->side[k]);
@@ -2387,11 +2388,11 @@ wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best
   // Trials advance fields and psi: keep device copies of both and put them back.
   std::vector<void *> saved;
   auto free_saved = [&]() {
-    for (void *p : saved) cudaFree(p);
+    for (void *p : saved) wf::dev_free(p);
   };
   for (wf_handle *h : b->h) {
     void *p = nullptr;
-    if (cudaMalloc(&p, sizeof(float) * 6 * h->N) != cudaSuccess) {
+    if (wf::dev_alloc(&p, sizeof(float) * 6 * h->N) != cudaSuccess) {
       free_saved();
       return fail(nullptr, WF_ERR_OOM, "autotune: no room to save the state");
     }
@@ -2400,7 +2401,7 @@ wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best
     for (auto &A : h->ax) {
       void *q = nullptr;
       if (A.T > 0) {
-        if (cudaMalloc(&q, sizeof(float) * 4 * A.cells) != cudaSuccess) {
+        if (wf::dev_alloc(&q, sizeof(float) * 4 * A.cells) != cudaSuccess) {
           free_saved();
           return fail(nullptr, WF_ERR_OOM, "autotune: no room to save the state");
         }
