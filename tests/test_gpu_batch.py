@@ -88,7 +88,8 @@ def test_batch_autotune_restores_state(oracle):
     try:
         best, ms = b.autotune(2)
         assert best in [(ty, zc, s) for ty in (4, 8, 16) for s in (3, 4)
-                        for zc in (8, 12, 16, 24, 32, 64, 128)]
+                        for zc in (8, 12, 16, 24, 32, 64, 128)] + [
+                            (32, zc, 3) for zc in (8, 12, 16, 24, 32, 64, 128)]
         assert ms > 0
         b.step(35)
         b.sync()

@@ -219,6 +219,10 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     }
     umma_commit(bar);
   }
+  // warp 0's other lanes wait here, not in the mbarrier's try-wait loop: a
+  // divergent warp alternates between its paths, and lanes suspended in the
+  // try-wait would hold back the lane issuing the MMAs
+  __syncwarp();
   const bool done = mbar_wait(bar, 0);
   tc_fence_after();
   if (!done) {
