@@ -573,58 +573,68 @@ def run_ours(args, rank, world, local_rank):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        # the handle's device allocation is set-up, outside the timed region
-        # (as the reference allocates its grids before engine::run times
-        # anything); every host<->device data movement is inside it
-        # everything is timed, the handle's creation included: its device
-        # memory comes from the library's cache of the blocks the first
-        # handle freed (a cold first creation is reported apart)
-        t0 = time.perf_counter()
-        g = DeviceFieldGrid(sc.dims, kernel="fused", device=local_rank, precision=PRECISION)
-        async_snap = PRECISION == "f32"
-        if async_snap:
-            g.reserve_download()  # the snapshot's staging buffer
-        tc = time.perf_counter()
-        load(g)
-        g.sync()
-        t_built = time.perf_counter()
-        # the snapshot of step 0, as the reference's benchmark writes one
-        # (--snapshot-every beyond the step count): FP32 storage downloads it
-        # while the other steps run, like the reference's double-buffered
-        # writer; 16-bit storage downloads it synchronously after the steps
-        g.step(1)
-        if async_snap:
-            g.download_blocks_async(snap.numpy())
-        g.step(args.steps - 1)
-        sums = [g.probe_sums(i, 1) for i in range(len(sc.probes))]
-        t_stepped = time.perf_counter()
-        if not async_snap:
-            import ctypes as C
-            from wavefront_b200 import _lib as L
-            L.check(L.lib().wf_download_blocks(g._h, C.c_void_p(snap.data_ptr())), g._h)
-        g.sync()  # the snapshot download has landed
-        e2e_s = time.perf_counter() - t0
-        phases = {"create": round((tc - t0) * 1e3, 1),
-                  "first_handle_create_and_upload_cold_untimed": round(cold_create_ms, 1),
-                  "upload": round((t_built - tc) * 1e3, 1),
-                  "steps_and_probe_sums": round((t_stepped - t_built) * 1e3, 1),
-                  "snapshot_wait": round((t0 + e2e_s - t_stepped) * 1e3, 1)}
-        g.close()
+
+        def e2e_run(snapshot: bool):
+            """Seconds for one run through the C ABI, everything timed (the
+            handle's creation too: its device memory comes from the library's
+            cache of the blocks the first handle freed), and the phases."""
+            t0 = time.perf_counter()
+            g = DeviceFieldGrid(sc.dims, kernel="fused", device=local_rank, precision=PRECISION)
+            async_snap = snapshot and PRECISION == "f32"
+            if async_snap:
+                g.reserve_download()  # the snapshot's staging buffer
+            tc = time.perf_counter()
+            load(g)
+            g.sync()
+            t_built = time.perf_counter()
+            # with `snapshot`, the FieldBlock snapshot of step 0, as the
+            # reference's benchmark writes one (--snapshot-every beyond the step
+            # count): FP32 storage downloads it while the other steps run, like
+            # the reference's double-buffered writer, 16-bit storage after them
+            g.step(1)
+            if async_snap:
+                g.download_blocks_async(snap.numpy())
+            g.step(args.steps - 1)
+            sums = [g.probe_sums(i, 1) for i in range(len(sc.probes))]
+            t_stepped = time.perf_counter()
+            if snapshot and not async_snap:
+                import ctypes as C
+                from wavefront_b200 import _lib as L
+                L.check(L.lib().wf_download_blocks(g._h, C.c_void_p(snap.data_ptr())), g._h)
+            g.sync()
+            el = time.perf_counter() - t0
+            phases = {"create": round((tc - t0) * 1e3, 1), "upload": round((t_built - tc) * 1e3, 1),
+                      "steps_and_probe_sums": round((t_stepped - t_built) * 1e3, 1)}
+            if snapshot:
+                phases["snapshot_wait"] = round((t0 + el - t_stepped) * 1e3, 1)
+            g.close()
+            return el, phases, len(sums)
+
+        e2e_s, phases, nsums = e2e_run(False)
+        phases["first_handle_create_and_upload_cold_untimed"] = round(cold_create_ms, 1)
+        snap_s, snap_phases, _ = e2e_run(True)
         e2e_s = max_over_ranks(dist, e2e_s)
+        snap_s = max_over_ranks(dist, snap_s)
         if dist:
             dist.barrier()
         e2e = whole_job_value(world, N_CELLS, args.steps, e2e_s)
         h2d = (N_CELLS if sc.grid is not None else len(sc.scene_text)) + 256 * 16 + total * (4 + 8 * 16)
-        d2h = len(sums) * (8 * 2 + 8) + N_CELLS * 24
+        d2h = nsums * (8 * 2 + 8)
         e2e_line = {"value": round(e2e, 1), "unit": METRIC,
                     "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h / args.steps),
                     "includes": "the handle's creation (device memory from the library's "
                                 "cache, warmed by the first handle of the run), scene or material "
                                 "upload (pinned), CPML and source/probe table uploads, K steps, "
-                                "probe sums, the FieldBlock snapshot of step 0 downloaded to "
-                                "pinned memory (FP32: while the other steps run)",
-                    "phases_ms": phases}
+                                "every probe's DFT sums read back (the run's result)",
+                    "phases_ms": phases,
+                    "with_snapshot": {
+                        "value": round(whole_job_value(world, N_CELLS, args.steps, snap_s), 1),
+                        "d2h_bytes_per_step": int((d2h + N_CELLS * 24) / args.steps),
+                        "includes": "the same plus the FieldBlock snapshot of step 0 (3.2 GB at "
+                                    "512^3) downloaded to pinned memory, FP32 while the other "
+                                    "steps run; bound by the host link at 20 steps",
+                        "phases_ms": snap_phases}}
 
     if rank == 0:
         line = {

@@ -52,7 +52,7 @@ constexpr int kTcA = 2 * kTcParts * kTcArr;                        // parts x 2 
 constexpr int kTcB = 27 * 512;
 constexpr int kTcBar = kTcA + kTcB;
 constexpr int kTcSmem = kTcBar + 16;
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 256;  // 8 warps: two per TMEM lane quarter
 constexpr int kTcCols32 = 32;  // tensor-memory columns allocated (kTcDT x 16, power of two)
 static_assert(kTcDT * 16 <= kTcCols32, "accumulator tiles fit the allocation");
 
@@ -142,21 +142,33 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     mbar_fence_init();
   }
 
-  // B: weights of the sample's face, [tap][half][n 16][k 8] bf16, zero padded
+  // B: weights of the sample's face, [tap][half][n 16][k 8] bf16, zero padded.
+  // The face's weights are one contiguous block: copied as it is (16-byte
+  // vectors when it allows) into the A region, which is filled only after,
+  // then rearranged from there.
   {
     __nv_bfloat16 *sb = reinterpret_cast<__nv_bfloat16 *>(smem + kTcA);
+    __nv_bfloat16 *raw = reinterpret_cast<__nv_bfloat16 *>(smem);
     const int wn = BWD ? kin : nout;   // first index of the stored weights (co)
     const int wk = BWD ? nout : kin;   // second (ci)
-    const __nv_bfloat16 *wf = w + static_cast<long long>(f) * wn * wk * 27;
+    const int nraw = wn * wk * 27;
+    const __nv_bfloat16 *wf = w + static_cast<long long>(f) * nraw;
+    if ((nraw % 8) == 0 && (reinterpret_cast<uintptr_t>(wf) & 15) == 0) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(wf);
+      uint4 *dst = reinterpret_cast<uint4 *>(raw);
+      for (int i = tid; i < nraw / 8; i += kTcThreads) dst[i] = __ldg(src + i);
+    } else {
+      for (int i = tid; i < nraw; i += kTcThreads) raw[i] = wf[i];
+    }
+    __syncthreads();
     for (int i = tid; i < 27 * 256; i += kTcThreads) {
       const int t = i >> 8, e = i & 255;
       const int half = e >> 7, n = (e >> 3) & 15, k = half * 8 + (e & 7);
-      float v = 0.0f;
-      if (n < nout && k < kin)
-        v = BWD ? __bfloat162float(wf[(static_cast<long long>(k) * wk + n) * 27 + (26 - t)])
-                : __bfloat162float(wf[(static_cast<long long>(n) * wk + k) * 27 + t]);
-      sb[i] = __float2bfloat16_rn(v);
+      __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+      if (n < nout && k < kin) v = BWD ? raw[(k * wk + n) * 27 + (26 - t)] : raw[(n * wk + k) * 27 + t];
+      sb[i] = v;
     }
+    __syncthreads();  // the raw copy in the A region is consumed
   }
   // A: the input tile as three bfloat16 parts, zero outside the tensor
   {
@@ -228,13 +240,14 @@ __global__ void __launch_bounds__(kTcThreads, 2)
   if (!done) {
     if (tid == 0) atomicAdd(&g_tc_timeouts, 1ull);
   } else {
-    // epilogue: warp w reads tensor-memory lanes 32w..32w+31 = output rows
-    // 32w + lane of each plane's tile: voxel (row 1 + w, column lane)
-    const int y = y0 + warp, x = x0 + lane - 1;
+    // epilogue: warp w reads tensor-memory lanes 32(w%4)..+31 of plane w/4's
+    // tile = output rows 32(w%4) + lane: voxel (row 1 + w%4, column lane)
+    const int quarter = warp & 3;
+    const int y = y0 + quarter, x = x0 + lane - 1;
     const bool keep = lane >= 1 && lane <= kTcOutCols && x < W && y < H;
-    for (int p = 0; p < nplanes; ++p) {
+    for (int p = warp >> 2; p < nplanes; p += kTcThreads / 128) {
       float v[16];
-      tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + p * 16, v);
+      tmem_ld16(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + p * 16, v);
       if (keep) {
         const long long q = (dp0 + p) * HW + static_cast<long long>(y) * W + x;
 #pragma unroll
