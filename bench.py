@@ -467,6 +467,67 @@ def run_closure(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_conv(args, rank, world, local_rank):
+    """The closure network's convolutions alone, at the closure's size (6 face
+    bands of 8 x 232 x 232 voxels, --grid sets the band's edge): one forward
+    convolution with GELU per layer shape (10->16, 16->16, 16->6), on the
+    tensor cores (tcgen05 implicit GEMM) and on the CUDA cores; CUDA events
+    over `--steps` launches after `--warmup`.  value = useful TFLOP/s of the
+    16->16 layer on the tensor cores."""
+    import ctypes as C
+
+    import torch
+    from wavefront_b200 import _lib as L
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return
+    n, D, H = 6, 8, args.grid or 232
+    dev = torch.device("cuda", local_rank)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out, launches = {}, 0
+    face = torch.arange(6, dtype=torch.int32, device=dev)
+    gen = torch.Generator(device=dev).manual_seed(0)
+    with ClockSampler(local_rank) as clk:
+        for ci, co in ((10, 16), (16, 16), (16, 6)):
+            x = torch.randn(n, ci, D, H, H, device=dev, generator=gen)
+            wb = (torch.randn(6, co, ci, 27, device=dev, generator=gen) * 0.2).to(torch.bfloat16)
+            z = torch.empty(n, co, D, H, H, device=dev)
+            a = torch.empty_like(z)
+            for tc in (1, 0):
+                L.lib().wf_nn_set_tensor_cores(tc)
+
+                def conv():
+                    L.check(L.lib().wf_nn_conv3d_forward(
+                        C.c_void_p(x.data_ptr()), C.c_void_p(wb.data_ptr()),
+                        C.c_void_p(face.data_ptr()), C.c_void_p(z.data_ptr()),
+                        C.c_void_p(a.data_ptr()), n, ci, co, D, H, H, 1, st))
+                for _ in range(args.warmup):
+                    conv()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(args.steps):
+                    conv()
+                e1.record()
+                torch.cuda.synchronize()
+                launches += args.steps
+                ms = e0.elapsed_time(e1) / args.steps
+                flops = 2.0 * n * D * H * H * ci * co * 27
+                out[f"{ci}->{co}_{'tensor_cores' if tc else 'cuda_cores'}"] = {
+                    "ms": round(ms, 4), "tflops": round(flops / ms / 1e9, 1)}
+    L.lib().wf_nn_set_tensor_cores(1)
+    v = out["16->16_tensor_cores"]["tflops"]
+    print(json.dumps({
+        "metric": "closure conv TFLOP/s (useful, 16->16 layer, tensor cores)", "value": v,
+        "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": out["16->16_tensor_cores"]["ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 x3 parts, fp32 accumulate",
+        "data": "synthetic",
+        "config": {"workload": f"closure_conv_6_faces_8x{H}x{H}", "layers": out,
+                   "parallelism": "1 GPU"},
+        "e2e": {"value": None, "unit": "TFLOP/s", "skipped": "a kernel micro-benchmark"},
+        "gpu_launches": launches, "clocks": clk.summary()}), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from wavefront_b200 import configs
@@ -821,7 +882,8 @@ def main():
     ap.add_argument("--grid", type=int, default=0,
                     help="cube edge (default 512 for two_spheres, 1024 for random_spheres)")
     ap.add_argument("--workload", default="two_spheres",
-                    choices=["two_spheres", "random_spheres", "batched", "closure", "demo_sphere"],
+                    choices=["two_spheres", "random_spheres", "batched", "closure", "conv",
+                             "demo_sphere"],
                     help="two_spheres: the 512^3 headline; random_spheres: the mixed-precision "
                          "scene; demo_sphere: the reference's own benchmark shape (256^3 demo "
                          "sphere, 8-cell CPML)")
@@ -867,6 +929,8 @@ def main():
         run_batched(args, rank, world, local_rank)
     elif args.workload == "closure":
         run_closure(args, rank, world, local_rank)
+    elif args.workload == "conv":
+        run_conv(args, rank, world, local_rank)
     elif args.slabs or (world > 1 and not args.replicas and PRECISION == "f32"):
         # under torchrun the grid is split into one z slab per rank (strong
         # scaling); --replicas runs an independent copy per rank instead
