@@ -753,9 +753,20 @@ wf_status batch_build(wf_batch *b) {
   }
   std::vector<int2> items;
   b->step_kernels = 0;
-  if (b->narrow) {  // one list, costliest items first (three CPML axes ... interior)
+  if (b->narrow) {
+    // one list, grid by grid (largest grids first), and within a grid its
+    // costliest items first (three CPML axes ... interior), each class in
+    // tile order: the tiles of a grid run close together in time, so the
+    // halo rows and columns they share are still in L2
     static constexpr int kOrder[wf::kFusedClassCount] = {7, 5, 3, 6, 1, 4, 2, 0};
-    for (int k : kOrder) items.insert(items.end(), lists[k].begin(), lists[k].end());
+    std::vector<std::vector<int2>> per_grid(n);
+    for (int k : kOrder)
+      for (const int2 &it : lists[k]) per_grid[it.x].push_back(it);
+    std::vector<int> gorder(n);
+    for (size_t i = 0; i < n; ++i) gorder[i] = static_cast<int>(i);
+    std::stable_sort(gorder.begin(), gorder.end(),
+                     [b](int p, int q) { return b->h[p]->N > b->h[q]->N; });
+    for (int i : gorder) items.insert(items.end(), per_grid[i].begin(), per_grid[i].end());
     b->step_kernels = 1;
   }
   for (int k = 0; k < wf::kFusedClassCount && !b->narrow; ++k) {
