@@ -157,6 +157,40 @@ def test_closure_in_step_equals_explicit_pipeline():
         g2.close()
 
 
+def test_tensor_core_closure_step_matches_cuda_core_step():
+    """The in-step closure on the tensor cores with packed operands (one TMA
+    box per tile, weights pre-arranged, the next layer's split written by the
+    epilogue) against the same step with the CUDA-core convolutions, over
+    three steps from random fields on a 48^3 grid (tile edges in x and y)."""
+    dims = wf.GridDims(48, 48, 48)
+    sc = configs.plain_cube_64(steps=1, n=48)
+    net = CL.ClosureNet(seed=7)
+    net.w[2].mul_(50.0)
+    net.wb[2].copy_(net.w[2].to(torch.bfloat16))
+    rng = np.random.default_rng(8)
+    f0 = (rng.standard_normal((6, 48, 48, 48)) * 0.01).astype(np.float32)
+    out = []
+    try:
+        for tc in (1, 0):
+            L.lib().wf_nn_set_tensor_cores(tc)
+            g = wf.DeviceFieldGrid(dims, kernel="fused")
+            try:
+                g.set_materials(wf.MaterialGrid(dims), wf.MaterialTable.vacuum_filled(sc.dt, sc.dx))
+                CL.set_thin_cpml(g, sc.dt, sc.dx)
+                g.set_fields(f0)
+                net.attach(g)
+                g.step(3)
+                g.sync()
+                out.append(g.fields())
+            finally:
+                g.close()
+    finally:
+        L.lib().wf_nn_set_tensor_cores(1)
+    assert L.lib().wf_nn_tensor_core_timeouts() == 0
+    assert not np.array_equal(out[0], f0)
+    assert np.abs(out[0] - out[1]).max() <= 1e-5 * np.abs(out[1]).max()
+
+
 def test_energy_guard_in_step_and_never_raises_band_energy():
     """With the guard on, a step equals the explicit pipeline with the guard
     applied by hand, and each face's correction can only lower the energy of

@@ -3,6 +3,7 @@
 // kernels, and the moves of a grid's boundary bands in and out of them.
 #pragma once
 
+#include <cuda.h>
 #include <stdint.h>
 
 namespace wf {
@@ -39,6 +40,17 @@ int nn_conv_fwd_tc(const float *in, const void *w_bf16, const int *face, float *
                    int ci, int co, int D, int H, int W, int act, void *stream);
 int nn_conv_bwd_data_tc(const float *dz, const void *w_bf16, const int *face, float *din, int n,
                         int ci, int co, int D, int H, int W, void *stream);
+// The in-step closure on the tensor cores with its operands prepared once per
+// layer (wf_closure_fast.cu): packed band tensors [face][6 arrays][P] of
+// 16-byte words (the three bfloat16 parts of 16 channels), a 5-D TMA map over
+// each, weights pre-arranged [face][27][512 bytes].
+int closure_fast_rms(const float *X, int C, long long P, float *part, float *s, void *stream);
+int closure_fast_pack(const float *X, int C, long long P, const float *s, void *packed, void *stream);
+int closure_fast_pack_weights(const void *w, int co, int ci, void *wp, void *stream);
+int closure_fast_conv(const CUtensorMap &tm_in, const void *wp, void *out_packed, float *out_y,
+                      const float *s, int nout, int D, int H, int W, bool last, void *stream);
+unsigned long long closure_fast_timeouts();
+constexpr int kClosureRmsParts = 148;  // partial sums per face of closure_fast_rms
 void nn_set_tensor_cores(int on);
 int nn_tensor_cores();
 unsigned long long nn_tc_timeouts();

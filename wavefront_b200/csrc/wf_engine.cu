@@ -98,6 +98,12 @@ struct wf_handle {
   float cl_ge = 1.0f, cl_gh = 1.0f;
   bool cl_guard = false;  // wf_set_closure_guard
   int *cl_face = nullptr;                       // device {0, 1, ..., 5}
+  // tensor-core closure with packed operands: three packed band tensors, the
+  // FP32 output, RMS partials and scales; packed weights; TMA maps
+  unsigned char *cl_fast = nullptr;
+  void *cl_wp = nullptr;
+  CUtensorMap cl_tm[3];
+  bool cl_fast_ok = false;
   long long version = 0;               // bumped when device tables are reallocated
   long long kernel_launches = 0;       // step + tail kernels issued so far
   long long graph_kernels[2] = {0, 0};  // kernels in one replay of graph[parity]
@@ -388,7 +394,32 @@ constexpr int kClHidden = 16;  // closure hidden channels
 // faces (times the gains), each face divided by its band's E RMS -> conv
 // 10->16 GELU -> conv 16->16 GELU -> conv 16->6 -> times that RMS -> fields
 // += (over the gains).
+// The same closure with the tensor-core kernels on packed operands
+// (wf_closure_fast.cu): gather, RMS (fixed-order partial sums), pack divided
+// by the RMS, three convolutions, each writing the next one's packed input,
+// the last one FP32 times the RMS, scatter.
+cudaError_t closure_enqueue_fast(wf_handle *h) {
+  const int n = h->nx, D = wf::kBandDepth;
+  const long long P = static_cast<long long>(D) * n * n;
+  const size_t packed = 6 * 6 * static_cast<size_t>(P) * 16, wbytes = 6 * 27 * 512;
+  unsigned char *pk[3] = {h->cl_fast, h->cl_fast + packed, h->cl_fast + 2 * packed};
+  float *Y = reinterpret_cast<float *>(h->cl_fast + 3 * packed);
+  float *part = Y + 6 * 6 * P, *scale = part + 6 * 256;
+  const unsigned char *wp = static_cast<const unsigned char *>(h->cl_wp);
+  float *X = h->cl_buf;
+  const wf::BandGrid g = band_grid(h, h->cur ^ 1);
+  int e = wf::band_gather(g, X, n, n, h->cl_ge, h->cl_gh, h->stream);
+  if (!e) e = wf::closure_fast_rms(X, wf::kBandIn, P, part, scale, h->stream);
+  if (!e) e = wf::closure_fast_pack(X, wf::kBandIn, P, scale, pk[0], h->stream);
+  if (!e) e = wf::closure_fast_conv(h->cl_tm[0], wp, pk[1], nullptr, scale, kClHidden, D, n, n, false, h->stream);
+  if (!e) e = wf::closure_fast_conv(h->cl_tm[1], wp + wbytes, pk[2], nullptr, scale, kClHidden, D, n, n, false, h->stream);
+  if (!e) e = wf::closure_fast_conv(h->cl_tm[2], wp + 2 * wbytes, nullptr, Y, scale, 6, D, n, n, true, h->stream);
+  if (!e) e = wf::band_scatter_add(g, Y, n, n, h->cl_ge, h->cl_gh, h->stream);
+  return static_cast<cudaError_t>(e);
+}
+
 cudaError_t closure_enqueue(wf_handle *h) {
+  if (h->cl_fast_ok && !h->cl_guard && wf::nn_tensor_cores()) return closure_enqueue_fast(h);
   const int n = h->nx, D = wf::kBandDepth;
   const long long P = static_cast<long long>(D) * n * n;
   float *X = h->cl_buf, *A1 = X + 6 * wf::kBandIn * P, *A2 = A1 + 6 * kClHidden * P,
@@ -1000,6 +1031,8 @@ wf_status wf_destroy(wf_handle *h) {
   for (auto &s : h->shift) wf::dev_free(s);
   for (auto &w : h->cl_w) wf::dev_free(w);
   wf::dev_free(h->cl_buf);
+  wf::dev_free(h->cl_fast);
+  wf::dev_free(h->cl_wp);
   wf::dev_free(h->cl_face);
   wf::dev_free(h->slab_max);
   wf::dev_free(h->d_ovf);
@@ -1761,6 +1794,31 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
   h->cl_ge = gain_e;
   h->cl_gh = gain_h;
   h->closure = true;
+  // the tensor-core path's operands: packed weights and band buffers, and a
+  // TMA map over each packed band tensor (the buffers never move)
+  h->cl_fast_ok = false;
+  if (encode_fn()) {
+    const int n = h->nx, D = wf::kBandDepth;
+    const size_t P = static_cast<size_t>(D) * n * n;
+    const size_t packed = 6 * 6 * P * 16, wbytes = 6 * 27 * 512;
+    if (!h->cl_wp) WF_CUDA(h, wf::dev_alloc(&h->cl_wp, 3 * wbytes));
+    if (!h->cl_fast)
+      WF_CUDA(h, wf::dev_alloc(&h->cl_fast, 3 * packed + sizeof(float) * (6 * 6 * P + 6 * 256 + 64)));
+    const int co[3] = {kClHidden, kClHidden, 6}, ci[3] = {wf::kBandIn, kClHidden, kClHidden};
+    for (int l = 0; l < 3; ++l)
+      WF_CUDA(h, static_cast<cudaError_t>(wf::closure_fast_pack_weights(
+                     h->cl_w[l], co[l], ci[l], static_cast<unsigned char *>(h->cl_wp) + l * wbytes,
+                     h->stream)));
+    WF_CUDA(h, cudaStreamSynchronize(h->stream));
+    const cuuint64_t dims[5] = {8, (cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)D, 36};
+    const cuuint64_t strides[4] = {16, 16ull * n, 16ull * n * n, 16ull * n * n * D};
+    const cuuint32_t box[5] = {8, 32, 6, 4, 6};
+    for (int l = 0; l < 3; ++l)
+      if (!encode(&h->cl_tm[l], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, h->cl_fast + l * packed, dims,
+                  strides, box))
+        return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(closure bands) failed");
+    h->cl_fast_ok = true;
+  }
   return WF_OK;
 }
 
@@ -1836,7 +1894,9 @@ wf_status wf_nn_set_tensor_cores(int enable) {
   return WF_OK;
 }
 
-int64_t wf_nn_tensor_core_timeouts(void) { return static_cast<int64_t>(wf::nn_tc_timeouts()); }
+int64_t wf_nn_tensor_core_timeouts(void) {
+  return static_cast<int64_t>(wf::nn_tc_timeouts() + wf::closure_fast_timeouts());
+}
 
 wf_status wf_nn_gelu_backward(const float *dout, const float *pre, float *dpre, int64_t m,
                               void *stream) {
