@@ -394,14 +394,17 @@ def run_closure(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     if rank != 0:
         return
-    interior = 224
+    interior = args.grid or 224
     dx = 1.0e-3
     dt = configs.courant_dt(dx)
     wf_ = default_waveform("ricker", float(np.float32(configs.C0 / (20.0 * dx))))
     total = args.warmup + args.steps
-    X, R, F, _ = CL.generate(96, seed=1, device=local_rank)
-    net, _ = CL.train(X, R, F, 1.0, iters=4000, lr=3e-4, device=local_rank)
-    del X, R, F
+    if args.closure_timing_only:
+        net = CL.ClosureNet(device=local_rank, seed=1)
+    else:
+        X, R, F, _ = CL.generate(96, seed=1, device=local_rank)
+        net, _ = CL.train(X, R, F, 1.0, iters=4000, lr=3e-4, device=local_rank)
+        del X, R, F
 
     def timed(n, pml, closure):
         dims = GridDims(n, n, n)
@@ -437,14 +440,15 @@ def run_closure(args, rank, world, local_rank):
     with ClockSampler(local_rank) as clk:
         closure_ms, launches = timed(interior + 8, "thin", True)
     thin_ms, _ = timed(interior + 8, "thin", False)
-    refl = {k: CL.reflection_test(**kw)["max_rel_error"] for k, kw in (
-        ("thin_layer_alone", {"truncated": True}),
-        ("thin_layer_with_closure_gain_0.5", {"net": net, "alpha": 0.5, "truncated": True}),
-        ("thin_layer_with_closure_gain_1_energy_guard",
-         {"net": net, "alpha": 1.0, "truncated": True, "guard": True}),
-        ("thin_layer_with_closure_gain_0.5_energy_guard",
-         {"net": net, "alpha": 0.5, "truncated": True, "guard": True}),
-        ("plain_cpml_4", {"cpml": 4}), ("plain_cpml_16", {"cpml": 16}))}
+    refl = {} if args.closure_timing_only else {
+        k: CL.reflection_test(**kw)["max_rel_error"] for k, kw in (
+            ("thin_layer_alone", {"truncated": True}),
+            ("thin_layer_with_closure_gain_0.5", {"net": net, "alpha": 0.5, "truncated": True}),
+            ("thin_layer_with_closure_gain_1_energy_guard",
+             {"net": net, "alpha": 1.0, "truncated": True, "guard": True}),
+            ("thin_layer_with_closure_gain_0.5_energy_guard",
+             {"net": net, "alpha": 0.5, "truncated": True, "guard": True}),
+            ("plain_cpml_4", {"cpml": 4}), ("plain_cpml_16", {"cpml": 16}))}
     value = interior ** 3 / (closure_ms / 1e3) / 1e6
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": 1,
@@ -452,13 +456,13 @@ def run_closure(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "interior": [interior] * 3,
-                   "cells_counted": "physical interior (224^3) per step",
+                   "cells_counted": f"physical interior ({interior}^3) per step",
                    "closure": "per-face 3x3x3 conv 10-16-16-6, GELU, bf16 weights, fp32 accumulation, "
                               "8-cell band, correction gain 0.5",
                    "parallelism": "1 GPU"},
-        "comparison_ms_per_step": {"cpml16_256^3": round(thick_ms, 4),
-                                   "thin4_232^3_with_closure": round(closure_ms, 4),
-                                   "thin4_232^3_alone": round(thin_ms, 4)},
+        "comparison_ms_per_step": {f"cpml16_{n16}^3": round(thick_ms, 4),
+                                   f"thin4_{interior + 8}^3_with_closure": round(closure_ms, 4),
+                                   f"thin4_{interior + 8}^3_alone": round(thin_ms, 4)},
         "reflection_test_max_rel_error": {k: (round(v, 5) if np.isfinite(v) else None)
                                           for k, v in refl.items()},
         "gpu_launches": int(launches),
@@ -894,6 +898,9 @@ def main():
                          "z slabs with ghost-block exchange (FP32)")
     ap.add_argument("--columns", default="on", choices=["on", "off"],
                     help="x-CPML slabs as 16-wide column tiles (on) or inside the wide tiles")
+    ap.add_argument("--closure-timing-only", action="store_true",
+                    help="closure workload: untrained random weights, no training and no "
+                         "reflection test (wall times only; for profiling)")
     ap.add_argument("--replicas", action="store_true",
                     help="under torchrun: an independent replica of the workload per rank "
                          "(weak scaling) instead of one z slab per rank")
@@ -909,7 +916,7 @@ def main():
     if args.workload == "batched":
         WORKLOAD = "batched_sweep_256_scenes_32-128^3_fp32_cpml10_ricker"
     elif args.workload == "closure":
-        WORKLOAD = "learned_closure_224^3_interior_thin4_vs_cpml16_ricker"
+        WORKLOAD = f"learned_closure_{args.grid or 224}^3_interior_thin4_vs_cpml16_ricker"
     elif args.workload == "random_spheres":
         WORKLOAD = f"random_spheres_{GRID}^3_{PRECISION}_storage_cpml16_sinusoid_8probes"
     elif args.workload == "demo_sphere":

@@ -296,37 +296,115 @@ __device__ __forceinline__ long long psi_index(const BandGrid &g, int ax, int x,
   return (static_cast<long long>(s) * g.ny + y) * g.nx + x;
 }
 
-// X[f][10][8][H][W]: 6 fields scaled by gain (E by ge, H by gh), then the 4
-// psi of the face's normal axis (terms of E differences by ge, of H by gh).
-__global__ void k_band_gather(BandGrid g, float *X, int H, int W, float ge, float gh) {
-  const int f = blockIdx.y;
-  const long long P = static_cast<long long>(kBandDepth) * H * W;
-  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p >= P) return;
-  const int v = static_cast<int>(p % W), u = static_cast<int>((p / W) % H), d = static_cast<int>(p / (static_cast<long long>(W) * H));
-  int x, y, z;
-  band_cell(g, f, d, u, v, x, y, z);
-  float *out = X + static_cast<long long>(f) * kBandIn * P + p;
-  const long long cell = (static_cast<long long>(z) * g.ny + y) * g.nx + x;
-  for (int c = 0; c < 6; ++c) out[c * P] = g.fields[c * g.N + cell] * (c < 3 ? ge : gh);
-  const long long k = psi_index(g, f >> 1, x, y, z);
-  for (int c = 0; c < 4; ++c)
-    out[(6 + c) * P] = k >= 0 ? g.psi[f >> 1].p[c * g.psi[f >> 1].cells + k] * (c < 2 ? ge : gh) : 0.0f;
+// The band copies move every cell between the grid (x fastest) and the band
+// tensors (v fastest), two layouts whose unit-stride axes differ on every face:
+// the grid's x is the band's depth d on the x faces and u on the y and z
+// faces.  Each CTA therefore stages a tile in shared memory and reads and
+// writes both sides along their own unit stride: TA cells along the band axis
+// that is x in the grid, 32 along v, TO along the third band axis.
+template <int AX>
+struct BandTile {
+  static constexpr int TA = AX == 0 ? kBandDepth : 32;  // along the grid's x
+  static constexpr int TO = AX == 0 ? 4 : 1;            // along the third axis
+  static constexpr int kElems = TA * 32 * TO;           // 1024: 4 per thread
+  static constexpr int kZ = AX == 0 ? 1 : kBandDepth;   // CTAs along z per face
+};
+static_assert(BandTile<0>::kElems == 1024 && BandTile<1>::kElems == 1024, "band tile size");
+
+// Band coordinates (d, u) of tile element (a, o) of CTA (by, sub).
+template <int AX>
+__device__ __forceinline__ void band_du(int al, int ol, int by, int sub, int &d, int &u) {
+  if (AX == 0) {
+    d = al;
+    u = by * BandTile<0>::TO + ol;
+  } else {
+    d = sub;
+    u = by * 32 + al;
+  }
 }
 
-// fields += Y / gain over every face's band (faces in order; a cell in two
-// bands gets both corrections, edges first by the lower face index)
-__global__ void k_band_scatter_add(BandGrid g, const float *Y, int H, int W, float ge, float gh,
-                                   int f) {
+// X[f][10][8][H][W]: 6 fields scaled by gain (E by ge, H by gh), then the 4
+// psi of the face's normal axis (terms of E differences by ge, of H by gh).
+// One launch per axis covers its two faces.
+template <int AX>
+__global__ void __launch_bounds__(256) k_band_gather(BandGrid g, float *X, int H, int W, float ge,
+                                                     float gh) {
+  using T = BandTile<AX>;
+  __shared__ float s[kBandIn][T::TO][T::TA][33];
+  const int side = blockIdx.z / T::kZ, sub = blockIdx.z % T::kZ, f = 2 * AX + side;
+  const int v0 = blockIdx.x * 32;
   const long long P = static_cast<long long>(kBandDepth) * H * W;
-  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p >= P) return;
-  const int v = static_cast<int>(p % W), u = static_cast<int>((p / W) % H), d = static_cast<int>(p / (static_cast<long long>(W) * H));
-  int x, y, z;
-  band_cell(g, f, d, u, v, x, y, z);
-  const float *in = Y + static_cast<long long>(f) * 6 * P + p;
-  const long long cell = (static_cast<long long>(z) * g.ny + y) * g.nx + x;
-  for (int c = 0; c < 6; ++c) g.fields[c * g.N + cell] += in[c * P] / (c < 3 ? ge : gh);
+  const BandPsi &ps = g.psi[AX];
+#pragma unroll
+  for (int j = 0; j < T::kElems / 256; ++j) {  // grid side: a fastest
+    const int e = threadIdx.x + 256 * j, al = e % T::TA, vl = (e / T::TA) % 32, ol = e / (T::TA * 32);
+    int d, u;
+    band_du<AX>(al, ol, blockIdx.y, sub, d, u);
+    const int v = v0 + vl;
+    if (d < kBandDepth && u < H && v < W) {
+      int x, y, z;
+      band_cell(g, f, d, u, v, x, y, z);
+      const long long cell = (static_cast<long long>(z) * g.ny + y) * g.nx + x;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) s[c][ol][al][vl] = g.fields[c * g.N + cell] * (c < 3 ? ge : gh);
+      const long long k = psi_index(g, AX, x, y, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        s[6 + c][ol][al][vl] = k >= 0 ? ps.p[c * ps.cells + k] * (c < 2 ? ge : gh) : 0.0f;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < T::kElems / 256; ++j) {  // band side: v fastest
+    const int e = threadIdx.x + 256 * j, vl = e % 32, al = (e / 32) % T::TA, ol = e / (32 * T::TA);
+    int d, u;
+    band_du<AX>(al, ol, blockIdx.y, sub, d, u);
+    const int v = v0 + vl;
+    if (d < kBandDepth && u < H && v < W) {
+      float *out = X + static_cast<long long>(f) * kBandIn * P + (static_cast<long long>(d) * H + u) * W + v;
+#pragma unroll
+      for (int c = 0; c < kBandIn; ++c) out[c * P] = s[c][ol][al][vl];
+    }
+  }
+}
+
+// fields += Y / gain over face f's band.  The faces go in order, one launch
+// each, so a cell in two bands gets both corrections, edges first by the
+// lower face index.
+template <int AX>
+__global__ void __launch_bounds__(256) k_band_scatter_add(BandGrid g, const float *Y, int H, int W,
+                                                          float ge, float gh, int f) {
+  using T = BandTile<AX>;
+  __shared__ float s[6][T::TO][T::TA][33];
+  const int sub = blockIdx.z, v0 = blockIdx.x * 32;
+  const long long P = static_cast<long long>(kBandDepth) * H * W;
+#pragma unroll
+  for (int j = 0; j < T::kElems / 256; ++j) {  // band side: v fastest
+    const int e = threadIdx.x + 256 * j, vl = e % 32, al = (e / 32) % T::TA, ol = e / (32 * T::TA);
+    int d, u;
+    band_du<AX>(al, ol, blockIdx.y, sub, d, u);
+    const int v = v0 + vl;
+    if (d < kBandDepth && u < H && v < W) {
+      const float *in = Y + static_cast<long long>(f) * 6 * P + (static_cast<long long>(d) * H + u) * W + v;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) s[c][ol][al][vl] = in[c * P];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < T::kElems / 256; ++j) {  // grid side: a fastest
+    const int e = threadIdx.x + 256 * j, al = e % T::TA, vl = (e / T::TA) % 32, ol = e / (T::TA * 32);
+    int d, u;
+    band_du<AX>(al, ol, blockIdx.y, sub, d, u);
+    const int v = v0 + vl;
+    if (d < kBandDepth && u < H && v < W) {
+      int x, y, z;
+      band_cell(g, f, d, u, v, x, y, z);
+      const long long cell = (static_cast<long long>(z) * g.ny + y) * g.nx + x;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) g.fields[c * g.N + cell] += s[c][ol][al][vl] / (c < 3 ? ge : gh);
+    }
+  }
 }
 
 // Student state (nx, ny, nz) = teacher state at offset `off` on every axis:
@@ -482,16 +560,28 @@ int nn_adam(float *w, void *w_bf16, const float *g, float *m1, float *m2, long l
 }
 
 int band_gather(const BandGrid &g, float *X, int H, int W, float ge, float gh, void *stream) {
-  const long long P = static_cast<long long>(kBandDepth) * H * W;
-  k_band_gather<<<dim3(blocks_for(P, 256), 6), 256, 0, static_cast<cudaStream_t>(stream)>>>(g, X, H, W, ge, gh);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned bx = blocks_for(W, 32);
+  k_band_gather<0><<<dim3(bx, blocks_for(H, BandTile<0>::TO), 2 * BandTile<0>::kZ), 256, 0, st>>>(
+      g, X, H, W, ge, gh);
+  k_band_gather<1><<<dim3(bx, blocks_for(H, 32), 2 * BandTile<1>::kZ), 256, 0, st>>>(g, X, H, W, ge, gh);
+  k_band_gather<2><<<dim3(bx, blocks_for(H, 32), 2 * BandTile<2>::kZ), 256, 0, st>>>(g, X, H, W, ge, gh);
   return cudaGetLastError();
 }
 
 int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, float gh,
                      void *stream) {
-  const long long P = static_cast<long long>(kBandDepth) * H * W;
-  for (int f = 0; f < 6; ++f)
-    k_band_scatter_add<<<blocks_for(P, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(g, Y, H, W, ge, gh, f);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned bx = blocks_for(W, 32);
+  for (int f = 0; f < 6; ++f) {
+    if (f < 2)
+      k_band_scatter_add<0><<<dim3(bx, blocks_for(H, BandTile<0>::TO), BandTile<0>::kZ), 256, 0, st>>>(
+          g, Y, H, W, ge, gh, f);
+    else if (f < 4)
+      k_band_scatter_add<1><<<dim3(bx, blocks_for(H, 32), BandTile<1>::kZ), 256, 0, st>>>(g, Y, H, W, ge, gh, f);
+    else
+      k_band_scatter_add<2><<<dim3(bx, blocks_for(H, 32), BandTile<2>::kZ), 256, 0, st>>>(g, Y, H, W, ge, gh, f);
+  }
   return cudaGetLastError();
 }
 

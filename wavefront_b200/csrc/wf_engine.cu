@@ -1810,11 +1810,13 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
                      h->cl_w[l], co[l], ci[l], static_cast<unsigned char *>(h->cl_wp) + l * wbytes,
                      h->stream)));
     WF_CUDA(h, cudaStreamSynchronize(h->stream));
-    const cuuint64_t dims[5] = {8, (cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)D, 36};
-    const cuuint64_t strides[4] = {16, 16ull * n, 16ull * n * n, 16ull * n * n * D};
-    const cuuint32_t box[5] = {8, 32, 6, 4, 6};
+    // one box = one plane of a tile's input: 6 rows of 32 voxels of the six
+    // arrays; x and the 8 channels of a word form one 512-byte box row
+    const cuuint64_t dims[4] = {8ull * n, (cuuint64_t)n, (cuuint64_t)D, 36};
+    const cuuint64_t strides[3] = {16ull * n, 16ull * n * n, 16ull * n * n * D};
+    const cuuint32_t box[4] = {8 * 32, 6, 1, 6};
     for (int l = 0; l < 3; ++l)
-      if (!encode(&h->cl_tm[l], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, h->cl_fast + l * packed, dims,
+      if (!encode(&h->cl_tm[l], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, h->cl_fast + l * packed, dims,
                   strides, box))
         return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(closure bands) failed");
     h->cl_fast_ok = true;
