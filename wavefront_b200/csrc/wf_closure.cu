@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "wf_band.cuh"
 #include "wf_closure.h"
 
 namespace wf {
@@ -270,59 +271,6 @@ __global__ void k_adam(float *w, __nv_bfloat16 *wb, const float *g, float *m1, f
 
 // ---- band gather / scatter on a grid's state --------------------------------
 
-// Cell (x, y, z) of band coordinates (d, u, v) of face f (axis f/2, side f%2).
-__device__ __forceinline__ void band_cell(const BandGrid &g, int f, int d, int u, int v, int &x,
-                                          int &y, int &z) {
-  const int ax = f >> 1;
-  const int n = ax == 0 ? g.nx : (ax == 1 ? g.ny : g.nz);
-  const int c = (f & 1) ? n - 1 - d : d;
-  if (ax == 0) { x = c; y = u; z = v; }
-  else if (ax == 1) { x = u; y = c; z = v; }
-  else { x = u; y = v; z = c; }
-}
-
-// The psi slot index of cell (x, y, z) on axis `ax`, or -1 outside its slab.
-__device__ __forceinline__ long long psi_index(const BandGrid &g, int ax, int x, int y, int z) {
-  const BandPsi &P = g.psi[ax];
-  if (P.T <= 0) return -1;
-  const int n = ax == 0 ? g.nx : (ax == 1 ? g.ny : g.nz);
-  const int c = ax == 0 ? x : (ax == 1 ? y : z);
-  int s = -1;
-  if (c < P.T) s = c;
-  else if (c >= n - P.T) s = c - (n - P.W);
-  if (s < 0) return -1;
-  if (ax == 0) return (static_cast<long long>(z) * g.ny + y) * P.pitch + s;
-  if (ax == 1) return (static_cast<long long>(z) * P.W + s) * g.nx + x;
-  return (static_cast<long long>(s) * g.ny + y) * g.nx + x;
-}
-
-// The band copies move every cell between the grid (x fastest) and the band
-// tensors (v fastest), two layouts whose unit-stride axes differ on every face:
-// the grid's x is the band's depth d on the x faces and u on the y and z
-// faces.  Each CTA therefore stages a tile in shared memory and reads and
-// writes both sides along their own unit stride: TA cells along the band axis
-// that is x in the grid, 32 along v, TO along the third band axis.
-template <int AX>
-struct BandTile {
-  static constexpr int TA = AX == 0 ? kBandDepth : 32;  // along the grid's x
-  static constexpr int TO = AX == 0 ? 4 : 1;            // along the third axis
-  static constexpr int kElems = TA * 32 * TO;           // 1024: 4 per thread
-  static constexpr int kZ = AX == 0 ? 1 : kBandDepth;   // CTAs along z per face
-};
-static_assert(BandTile<0>::kElems == 1024 && BandTile<1>::kElems == 1024, "band tile size");
-
-// Band coordinates (d, u) of tile element (a, o) of CTA (by, sub).
-template <int AX>
-__device__ __forceinline__ void band_du(int al, int ol, int by, int sub, int &d, int &u) {
-  if (AX == 0) {
-    d = al;
-    u = by * BandTile<0>::TO + ol;
-  } else {
-    d = sub;
-    u = by * 32 + al;
-  }
-}
-
 // X[f][10][8][H][W]: 6 fields scaled by gain (E by ge, H by gh), then the 4
 // psi of the face's normal axis (terms of E differences by ge, of H by gh).
 // One launch per axis covers its two faces.
@@ -368,15 +316,16 @@ __global__ void __launch_bounds__(256) k_band_gather(BandGrid g, float *X, int H
   }
 }
 
-// fields += Y / gain over face f's band.  The faces go in order, one launch
-// each, so a cell in two bands gets both corrections, edges first by the
+// fields += Y / gain over the bands of faces f0 .. f0 + nf - 1 (both faces of
+// axis AX in one launch when their bands are disjoint).  The axes go in
+// order, so a cell in two bands gets both corrections, edges first by the
 // lower face index.
 template <int AX>
 __global__ void __launch_bounds__(256) k_band_scatter_add(BandGrid g, const float *Y, int H, int W,
-                                                          float ge, float gh, int f) {
+                                                          float ge, float gh, int f0) {
   using T = BandTile<AX>;
   __shared__ float s[6][T::TO][T::TA][33];
-  const int sub = blockIdx.z, v0 = blockIdx.x * 32;
+  const int f = f0 + blockIdx.z / T::kZ, sub = blockIdx.z % T::kZ, v0 = blockIdx.x * 32;
   const long long P = static_cast<long long>(kBandDepth) * H * W;
 #pragma unroll
   for (int j = 0; j < T::kElems / 256; ++j) {  // band side: v fastest
@@ -573,14 +522,21 @@ int band_scatter_add(const BandGrid &g, const float *Y, int H, int W, float ge, 
                      void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const unsigned bx = blocks_for(W, 32);
-  for (int f = 0; f < 6; ++f) {
-    if (f < 2)
-      k_band_scatter_add<0><<<dim3(bx, blocks_for(H, BandTile<0>::TO), BandTile<0>::kZ), 256, 0, st>>>(
-          g, Y, H, W, ge, gh, f);
-    else if (f < 4)
-      k_band_scatter_add<1><<<dim3(bx, blocks_for(H, 32), BandTile<1>::kZ), 256, 0, st>>>(g, Y, H, W, ge, gh, f);
-    else
-      k_band_scatter_add<2><<<dim3(bx, blocks_for(H, 32), BandTile<2>::kZ), 256, 0, st>>>(g, Y, H, W, ge, gh, f);
+  const int extent[3] = {g.nx, g.ny, g.nz};
+  for (int ax = 0; ax < 3; ++ax) {
+    // the two faces' bands are disjoint when the axis holds two band depths
+    const int nf = extent[ax] >= 2 * kBandDepth ? 2 : 1;
+    for (int f = 2 * ax; f < 2 * ax + 2; f += nf) {
+      if (ax == 0)
+        k_band_scatter_add<0><<<dim3(bx, blocks_for(H, BandTile<0>::TO), nf * BandTile<0>::kZ), 256, 0,
+                                st>>>(g, Y, H, W, ge, gh, f);
+      else if (ax == 1)
+        k_band_scatter_add<1><<<dim3(bx, blocks_for(H, 32), nf * BandTile<1>::kZ), 256, 0, st>>>(
+            g, Y, H, W, ge, gh, f);
+      else
+        k_band_scatter_add<2><<<dim3(bx, blocks_for(H, 32), nf * BandTile<2>::kZ), 256, 0, st>>>(
+            g, Y, H, W, ge, gh, f);
+    }
   }
   return cudaGetLastError();
 }

@@ -42,15 +42,25 @@ int nn_conv_bwd_data_tc(const float *dz, const void *w_bf16, const int *face, fl
                         int ci, int co, int D, int H, int W, void *stream);
 // The in-step closure on the tensor cores with its operands prepared once per
 // layer (wf_closure_fast.cu): packed band tensors [face][6 arrays][P] of
-// 16-byte words (the three bfloat16 parts of 16 channels), a 5-D TMA map over
-// each, weights pre-arranged [face][27][512 bytes].
-int closure_fast_rms(const float *X, int C, long long P, float *part, float *s, void *stream);
-int closure_fast_pack(const float *X, int C, long long P, const float *s, void *packed, void *stream);
+// 16-byte words (the three bfloat16 parts of 16 channels), a 4-D TMA map over
+// each, weights pre-arranged [face][9][2][48][8] bfloat16.
+// Layer 1's packed input (the band cells times the gains, unscaled) straight
+// from a cubic grid, and per CTA the sum of squares of its E values in
+// part[f * closure_fast_parts(H, W) + CTA].
+int closure_fast_gather(const BandGrid &g, void *packed, float *part, int H, int W, float ge,
+                        float gh, void *stream);
+// s[f] = sqrt(sum of face f's partial sums / 3P) + 1e-30 (fixed order)
+int closure_fast_rms(const float *part, int H, int W, long long P, float *s, void *stream);
+long long closure_fast_parts(int H, int W);  // partial sums per face (the largest axis's)
 int closure_fast_pack_weights(const void *w, int co, int ci, void *wp, void *stream);
+// One layer.  in_scale (layer 1): the accumulator is divided by in_scale[f]
+// (times its reciprocal) before the activation, the network's input
+// normalisation applied after the convolution.  last: out_y = FP32 output
+// times s[f]; otherwise out_packed = the next layer's packed input.
 int closure_fast_conv(const CUtensorMap &tm_in, const void *wp, void *out_packed, float *out_y,
-                      const float *s, int nout, int D, int H, int W, bool last, void *stream);
+                      const float *s, const float *in_scale, int nout, int D, int H, int W, bool last,
+                      void *stream);
 unsigned long long closure_fast_timeouts();
-constexpr int kClosureRmsParts = 148;  // partial sums per face of closure_fast_rms
 void nn_set_tensor_cores(int on);
 int nn_tensor_cores();
 unsigned long long nn_tc_timeouts();

@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "wf_band.cuh"
 #include "wf_closure.h"
 #include "wf_internal.cuh"
 
@@ -132,56 +133,95 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
                : "memory");
 }
 
-// The three bfloat16 parts of 16 FP32 values, as six 16-byte words:
-// out[2 * part + half] holds channels 8 * half .. 8 * half + 7 of `part`.
-__device__ __forceinline__ void split16(float v[16], uint4 out[6]) {
-#pragma unroll
-  for (int part = 0; part < 3; ++part) {
-    uint32_t q[8];
-#pragma unroll
-    for (int c = 0; c < 16; c += 2) {
-      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[c]), h1 = __float2bfloat16_rn(v[c + 1]);
-      q[c / 2] = static_cast<uint32_t>(__bfloat16_as_ushort(h0)) |
-                 (static_cast<uint32_t>(__bfloat16_as_ushort(h1)) << 16);
-      v[c] -= __bfloat162float(h0);
-      v[c + 1] -= __bfloat162float(h1);
-    }
-    out[2 * part] = make_uint4(q[0], q[1], q[2], q[3]);
-    out[2 * part + 1] = make_uint4(q[4], q[5], q[6], q[7]);
-  }
-}
 
 }  // namespace
 
 namespace {
 
-constexpr int kRmsBlocks = 148;  // partial sums per face
-
-// Sum of squares of the E channels (0..2) of each face band X[6][C][P]: a
-// fixed grid of partial sums (deterministic order), then one CTA per face
-// folds them: s[f] = sqrt(sum / 3P) + 1e-30, as face_rms computes it.
-__global__ void k_face_sumsq(const float *X, int C, long long P, float *part) {
+// Layer 1's packed input straight from the grid: face f's band cells (the 6
+// fields and the 4 psi of its normal axis, times the gains; channels 10-15
+// zero) split into three bfloat16 parts, through the transposing tile of
+// band_gather (grid side along x, band side along v).  Each CTA also writes
+// the sum of squares of its E values to part[f * stride + CTA], summed in a
+// fixed order.  One launch covers both faces of axis AX.
+template <int AX>
+__global__ void __launch_bounds__(256) k_band_gather_pack(BandGrid g, uint4 *packed, float *part,
+                                                          long long stride, int H, int W, float ge,
+                                                          float gh) {
+  using T = BandTile<AX>;
+  __shared__ float s[kBandIn][T::TO][T::TA][33];
   __shared__ float s_sum[256];
-  const int f = blockIdx.y;
-  const float *x = X + static_cast<long long>(f) * C * P;
+  const int side = blockIdx.z / T::kZ, sub = blockIdx.z % T::kZ, f = 2 * AX + side;
+  const int v0 = blockIdx.x * 32;
+  const long long P = static_cast<long long>(kBandDepth) * H * W;
+  const BandPsi &ps = g.psi[AX];
   float acc = 0.0f;
-  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < 3 * P;
-       i += static_cast<long long>(gridDim.x) * blockDim.x)
-    acc += x[i] * x[i];
+#pragma unroll
+  for (int j = 0; j < T::kElems / 256; ++j) {  // grid side: a fastest
+    const int e = threadIdx.x + 256 * j, al = e % T::TA, vl = (e / T::TA) % 32, ol = e / (T::TA * 32);
+    int d, u;
+    band_du<AX>(al, ol, blockIdx.y, sub, d, u);
+    const int v = v0 + vl;
+    if (d < kBandDepth && u < H && v < W) {
+      int x, y, z;
+      band_cell(g, f, d, u, v, x, y, z);
+      const long long cell = (static_cast<long long>(z) * g.ny + y) * g.nx + x;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const float val = g.fields[c * g.N + cell] * (c < 3 ? ge : gh);
+        s[c][ol][al][vl] = val;
+        if (c < 3) acc += val * val;
+      }
+      const long long k = psi_index(g, AX, x, y, z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        s[6 + c][ol][al][vl] = k >= 0 ? ps.p[c * ps.cells + k] * (c < 2 ? ge : gh) : 0.0f;
+    }
+  }
   s_sum[threadIdx.x] = acc;
   __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+#pragma unroll
+  for (int j = 0; j < T::kElems / 256; ++j) {  // band side: v fastest
+    const int e = threadIdx.x + 256 * j, vl = e % 32, al = (e / 32) % T::TA, ol = e / (32 * T::TA);
+    int d, u;
+    band_du<AX>(al, ol, blockIdx.y, sub, d, u);
+    const int v = v0 + vl;
+    if (d < kBandDepth && u < H && v < W) {
+      float val[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) val[c] = c < kBandIn ? s[c][ol][al][vl] : 0.0f;
+      uint4 w[6];
+      split16(val, w);
+      uint4 *o = packed + static_cast<long long>(f) * 6 * P + (static_cast<long long>(d) * H + u) * W + v;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) o[q * P] = w[q];
+    }
+  }
+  for (int k = 128; k > 0; k >>= 1) {
     if (threadIdx.x < k) s_sum[threadIdx.x] += s_sum[threadIdx.x + k];
     __syncthreads();
   }
-  if (threadIdx.x == 0) part[f * gridDim.x + blockIdx.x] = s_sum[0];
+  if (threadIdx.x == 0)
+    part[f * stride + (static_cast<long long>(sub) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] =
+        s_sum[0];
 }
 
-__global__ void k_face_rms_fold(const float *part, int nb, long long P, float *s) {
+// CTAs per face of k_band_gather_pack<AX>
+__host__ __device__ inline long long gather_parts(int ax, int H, int W) {
+  const long long bx = (W + 31) / 32;
+  return ax == 0 ? bx * ((H + BandTile<0>::TO - 1) / BandTile<0>::TO)
+                 : bx * ((H + 31) / 32) * BandTile<1>::kZ;
+}
+
+// s[f] = sqrt(sum / 3P) + 1e-30 from face f's partial sums, as face_rms
+// computes it (fixed order: strided per thread, then a tree).
+__global__ void k_face_rms_fold(const float *part, long long stride, int H, int W, long long P,
+                                float *s) {
   __shared__ float s_sum[256];
   const int f = blockIdx.x;
+  const long long nb = gather_parts(f >> 1, H, W);
   float acc = 0.0f;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += part[f * nb + i];
+  for (long long i = threadIdx.x; i < nb; i += blockDim.x) acc += part[f * stride + i];
   s_sum[threadIdx.x] = acc;
   __syncthreads();
   for (int k = blockDim.x / 2; k > 0; k >>= 1) {
@@ -189,23 +229,6 @@ __global__ void k_face_rms_fold(const float *part, int nb, long long P, float *s
     __syncthreads();
   }
   if (threadIdx.x == 0) s[f] = sqrtf(s_sum[0] / static_cast<float>(3 * P)) + 1e-30f;
-}
-
-// packed[f][6][P] (16-byte words) from X[f][C][P] / s[f]; channels C..15 zero
-__global__ void k_pack_band(const float *X, int C, long long P, const float *s, uint4 *packed) {
-  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int f = blockIdx.y;
-  if (p >= P) return;
-  const float *x = X + static_cast<long long>(f) * C * P + p;
-  float v[16];
-  const float m = 1.0f / s[f];  // as face_scale divides: times the reciprocal
-#pragma unroll
-  for (int c = 0; c < 16; ++c) v[c] = c < C ? x[c * P] * m : 0.0f;
-  uint4 w[6];
-  split16(v, w);
-  uint4 *o = packed + static_cast<long long>(f) * 6 * P + p;
-#pragma unroll
-  for (int q = 0; q < 6; ++q) o[q * P] = w[q];
 }
 
 // Wp[f][r = 3 (dy + 1) + dx + 1][half][n 48][k 8] bf16 from W[f][co][ci][27]
@@ -266,7 +289,8 @@ __device__ __forceinline__ FastTile fast_tile(long long t, int txc, int tyc) {
 template <bool LAST>
 __global__ void __launch_bounds__(kFThreads, 1)
     k_conv_fast(const __grid_constant__ CUtensorMap tm_in, const __nv_bfloat16 *wp,
-                uint4 *out_packed, float *out_y, const float *s, int nout, int H, int W) {
+                uint4 *out_packed, float *out_y, const float *s, const float *in_scale, int nout,
+                int H, int W) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
@@ -423,6 +447,11 @@ __global__ void __launch_bounds__(kFThreads, 1)
             for (int o = 0; o < 16; ++o)
               if (o < nout) out_y[(static_cast<long long>(tl.f) * nout + o) * P + q] = v[h][o] * sf;
           } else {
+            if (in_scale) {
+              const float m = 1.0f / in_scale[tl.f];  // as face_scale divides: times the reciprocal
+#pragma unroll
+              for (int o = 0; o < 16; ++o) v[h][o] *= m;
+            }
 #pragma unroll
             for (int o = 0; o < 16; ++o) v[h][o] = o < nout ? gelu_f(v[h][o]) : 0.0f;
             uint4 wv[6];
@@ -457,16 +486,29 @@ inline unsigned nblocks(long long n, int t) { return static_cast<unsigned>((n + 
 
 }  // namespace
 
-int closure_fast_rms(const float *X, int C, long long P, float *part, float *s, void *stream) {
+long long closure_fast_parts(int H, int W) {
+  const long long a = gather_parts(0, H, W), b = gather_parts(1, H, W);
+  return a > b ? a : b;
+}
+
+int closure_fast_gather(const BandGrid &g, void *packed, float *part, int H, int W, float ge,
+                        float gh, void *stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_face_sumsq<<<dim3(kRmsBlocks, 6), 256, 0, st>>>(X, C, P, part);
-  k_face_rms_fold<<<6, 256, 0, st>>>(part, kRmsBlocks, P, s);
+  uint4 *pk = static_cast<uint4 *>(packed);
+  const long long stride = closure_fast_parts(H, W);
+  const unsigned bx = nblocks(W, 32);
+  k_band_gather_pack<0><<<dim3(bx, nblocks(H, BandTile<0>::TO), 2 * BandTile<0>::kZ), 256, 0, st>>>(
+      g, pk, part, stride, H, W, ge, gh);
+  k_band_gather_pack<1><<<dim3(bx, nblocks(H, 32), 2 * BandTile<1>::kZ), 256, 0, st>>>(
+      g, pk, part, stride, H, W, ge, gh);
+  k_band_gather_pack<2><<<dim3(bx, nblocks(H, 32), 2 * BandTile<2>::kZ), 256, 0, st>>>(
+      g, pk, part, stride, H, W, ge, gh);
   return cudaGetLastError();
 }
 
-int closure_fast_pack(const float *X, int C, long long P, const float *s, void *packed, void *stream) {
-  k_pack_band<<<dim3(nblocks(P, 256), 6), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      X, C, P, s, static_cast<uint4 *>(packed));
+int closure_fast_rms(const float *part, int H, int W, long long P, float *s, void *stream) {
+  k_face_rms_fold<<<6, 256, 0, static_cast<cudaStream_t>(stream)>>>(part, closure_fast_parts(H, W), H,
+                                                                     W, P, s);
   return cudaGetLastError();
 }
 
@@ -477,7 +519,8 @@ int closure_fast_pack_weights(const void *w, int co, int ci, void *wp, void *str
 }
 
 int closure_fast_conv(const CUtensorMap &tm_in, const void *wp, void *out_packed, float *out_y,
-                      const float *s, int nout, int D, int H, int W, bool last, void *stream) {
+                      const float *s, const float *in_scale, int nout, int D, int H, int W, bool last,
+                      void *stream) {
   if (D != kFD) return cudaErrorInvalidValue;
   static bool attr[2] = {false, false};
   const void *fn = last ? reinterpret_cast<const void *>(k_conv_fast<true>)
@@ -496,10 +539,10 @@ int closure_fast_conv(const CUtensorMap &tm_in, const void *wp, void *out_packed
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const __nv_bfloat16 *w = static_cast<const __nv_bfloat16 *>(wp);
   if (last)
-    k_conv_fast<true><<<grid, kFThreads, kFSmem, st>>>(tm_in, w, nullptr, out_y, s, nout, H, W);
+    k_conv_fast<true><<<grid, kFThreads, kFSmem, st>>>(tm_in, w, nullptr, out_y, s, nullptr, nout, H, W);
   else
     k_conv_fast<false><<<grid, kFThreads, kFSmem, st>>>(tm_in, w, static_cast<uint4 *>(out_packed),
-                                                        nullptr, s, nout, H, W);
+                                                        nullptr, s, in_scale, nout, H, W);
   return cudaGetLastError();
 }
 

@@ -404,18 +404,33 @@ cudaError_t closure_enqueue_fast(wf_handle *h) {
   const size_t packed = 6 * 6 * static_cast<size_t>(P) * 16, wbytes = 6 * 27 * 512;
   unsigned char *pk[3] = {h->cl_fast, h->cl_fast + packed, h->cl_fast + 2 * packed};
   float *Y = reinterpret_cast<float *>(h->cl_fast + 3 * packed);
-  float *part = Y + 6 * 6 * P, *scale = part + 6 * 256;
+  float *scale = Y + 6 * 6 * P, *part = scale + 64;
   const unsigned char *wp = static_cast<const unsigned char *>(h->cl_wp);
-  float *X = h->cl_buf;
   const wf::BandGrid g = band_grid(h, h->cur ^ 1);
-  int e = wf::band_gather(g, X, n, n, h->cl_ge, h->cl_gh, h->stream);
-  if (!e) e = wf::closure_fast_rms(X, wf::kBandIn, P, part, scale, h->stream);
-  if (!e) e = wf::closure_fast_pack(X, wf::kBandIn, P, scale, pk[0], h->stream);
-  if (!e) e = wf::closure_fast_conv(h->cl_tm[0], wp, pk[1], nullptr, scale, kClHidden, D, n, n, false, h->stream);
-  if (!e) e = wf::closure_fast_conv(h->cl_tm[1], wp + wbytes, pk[2], nullptr, scale, kClHidden, D, n, n, false, h->stream);
-  if (!e) e = wf::closure_fast_conv(h->cl_tm[2], wp + 2 * wbytes, nullptr, Y, scale, 6, D, n, n, true, h->stream);
+  int e = wf::closure_fast_gather(g, pk[0], part, n, n, h->cl_ge, h->cl_gh, h->stream);
+  if (!e) e = wf::closure_fast_rms(part, n, n, P, scale, h->stream);
+  if (!e)
+    e = wf::closure_fast_conv(h->cl_tm[0], wp, pk[1], nullptr, scale, scale, kClHidden, D, n, n, false,
+                              h->stream);
+  if (!e)
+    e = wf::closure_fast_conv(h->cl_tm[1], wp + wbytes, pk[2], nullptr, scale, nullptr, kClHidden, D, n,
+                              n, false, h->stream);
+  if (!e)
+    e = wf::closure_fast_conv(h->cl_tm[2], wp + 2 * wbytes, nullptr, Y, scale, nullptr, 6, D, n, n, true,
+                              h->stream);
   if (!e) e = wf::band_scatter_add(g, Y, n, n, h->cl_ge, h->cl_gh, h->stream);
   return static_cast<cudaError_t>(e);
+}
+
+// Kernels closure_enqueue issues: the scatter takes one launch per axis whose
+// two bands are disjoint (two otherwise); the packed path gathers, folds the
+// RMS and runs the three layers; the FP32 path gathers, reduces the RMS,
+// scales in and out around its three layers, and guards when asked.
+int closure_launches(const wf_handle *h) {
+  int scatter = 0;
+  for (int n : {h->nx, h->ny, h->nz}) scatter += n >= 2 * wf::kBandDepth ? 1 : 2;
+  if (h->cl_fast_ok && !h->cl_guard && wf::nn_tensor_cores()) return 3 + 1 + 3 + scatter;
+  return 3 + 1 + 1 + 3 + 1 + (h->cl_guard ? 2 : 0) + scatter;
 }
 
 cudaError_t closure_enqueue(wf_handle *h) {
@@ -555,7 +570,7 @@ wf_status enqueue_one(wf_handle *h) {
   if (h->closure) {
     e = closure_enqueue(h);
     if (e != cudaSuccess) return cuda_fail(h, e, "closure launch");
-    h->kernel_launches += 13;  // gather, RMS, 2 scales, 3 convs, 6 face scatters
+    h->kernel_launches += closure_launches(h);
   }
   if (h->timing) {
     cudaEvent_t ev = timing_event(h);
@@ -1803,7 +1818,8 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
     const size_t packed = 6 * 6 * P * 16, wbytes = 6 * 27 * 512;
     if (!h->cl_wp) WF_CUDA(h, wf::dev_alloc(&h->cl_wp, 3 * wbytes));
     if (!h->cl_fast)
-      WF_CUDA(h, wf::dev_alloc(&h->cl_fast, 3 * packed + sizeof(float) * (6 * 6 * P + 6 * 256 + 64)));
+      WF_CUDA(h, wf::dev_alloc(&h->cl_fast, 3 * packed + sizeof(float) * (6 * 6 * P + 64 +
+                                                                          6 * wf::closure_fast_parts(n, n))));
     const int co[3] = {kClHidden, kClHidden, 6}, ci[3] = {wf::kBandIn, kClHidden, kClHidden};
     for (int l = 0; l < 3; ++l)
       WF_CUDA(h, static_cast<cudaError_t>(wf::closure_fast_pack_weights(
