@@ -388,7 +388,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
             ok = mbar_wait(full(z), i & 1);
             if (!ok) break;
             ++s_pl_used[z];
-            tc_fence_after();
+            // (the TMA's complete_tx on full(z) orders the plane before these
+            // MMAs, as in a TMA-to-UMMA pipeline: no tcgen05 fence here)
             const uint32_t d = d0 + 16 * z;  // planes z - 1, z, z + 1
 #pragma unroll
             for (int r = 0; r < 9; ++r) {
