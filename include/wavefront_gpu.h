@@ -346,7 +346,10 @@ wf_status wf_set_closure(wf_handle *h, const void *w1_bf16, const void *w2_bf16,
  * guarantee: the Yee scheme's conserved energy pairs E and H at staggered
  * times, and the CPML's psi is not covered. */
 wf_status wf_set_closure_guard(wf_handle *h, int on);
-/* The current state's bands into device X[6][10][8][n][n] (scaled as above). */
+/* The current state's bands into device X[6][10][8][n][n] (scaled as above).
+ * Both band moves are enqueued on the handle's own (non-blocking) stream: a
+ * caller that produces Y or consumes X on another stream orders the two
+ * itself (wf_sync, or an event). */
 wf_status wf_band_gather(wf_handle *h, float *X, float gain_e, float gain_h);
 /* fields += Y[6][6][8][n][n] / gain over the current state's bands. */
 wf_status wf_band_scatter_add(wf_handle *h, const float *Y, float gain_e, float gain_h);

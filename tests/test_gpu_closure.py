@@ -12,6 +12,7 @@
    plain CPML judging both through the reflection test.
 """
 import ctypes as C
+import types
 
 import numpy as np
 import pytest
@@ -114,16 +115,20 @@ def test_tensor_core_and_cuda_core_convs_agree():
     assert err <= 1e-5, err
 
 
-def test_closure_in_step_equals_explicit_pipeline():
+@pytest.mark.parametrize("n", [16, 24, 32])
+def test_closure_in_step_equals_explicit_pipeline(n):
     """One step with the closure attached against the same step without it
-    followed by the closure's pipeline by hand (random fields, thin layer)."""
-    sc = configs.plain_cube_64(steps=1, n=32)
+    followed by the closure's pipeline by hand (random fields, thin layer).
+    From 32 cells the step runs the packed tensor-core path; narrower grids
+    keep the FP32-in path."""
+    dx = 1.0e-3
+    sc = types.SimpleNamespace(dx=dx, dt=configs.courant_dt(dx))
     net = CL.ClosureNet(seed=2)
     net.w[2].mul_(50.0)
     net.wb[2].copy_(net.w[2].to(torch.bfloat16))
-    dims = wf.GridDims(32, 32, 32)
+    dims = wf.GridDims(n, n, n)
     rng = np.random.default_rng(5)
-    f0 = (rng.standard_normal((6, 32, 32, 32)) * 0.01).astype(np.float32)
+    f0 = (rng.standard_normal((6, n, n, n)) * 0.01).astype(np.float32)
     g1 = wf.DeviceFieldGrid(dims, kernel="fused")
     g2 = wf.DeviceFieldGrid(dims, kernel="fused")
     try:
@@ -135,8 +140,8 @@ def test_closure_in_step_equals_explicit_pipeline():
         g1.step(1)
         g2.step(1)
         g2.sync()
-        P = 8 * 32 * 32
-        X = torch.empty(6, 10, 8, 32, 32, device=net.dev)
+        P = 8 * n * n
+        X = torch.empty(6, 10, 8, n, n, device=net.dev)
         L.check(L.lib().wf_band_gather(g2._h, CL._p(X), net.gain_e, net.gain_h))
         torch.cuda.synchronize()
         s = torch.sqrt(torch.sum(X[:, :3].reshape(6, -1) ** 2, dim=1) / (3 * P)) + 1e-30
@@ -144,6 +149,7 @@ def test_closure_in_step_equals_explicit_pipeline():
         faces = torch.arange(6, dtype=torch.int32, device=net.dev)
         y, _ = net.forward(Xs.contiguous(), faces)
         Y = (y * s.view(6, 1, 1, 1, 1)).contiguous()
+        torch.cuda.synchronize()  # Y comes from torch's stream; the scatter runs on the handle's
         L.check(L.lib().wf_band_scatter_add(g2._h, CL._p(Y), net.gain_e, net.gain_h))
         torch.cuda.synchronize()
         got, want = g1.fields(), g2.fields()
@@ -195,7 +201,8 @@ def test_energy_guard_in_step_and_never_raises_band_energy():
     """With the guard on, a step equals the explicit pipeline with the guard
     applied by hand, and each face's correction can only lower the energy of
     its band's six fields (sum of squares in the gained units)."""
-    sc = configs.plain_cube_64(steps=1, n=32)
+    n = 32
+    sc = configs.plain_cube_64(steps=1, n=n)
     net = CL.ClosureNet(seed=4)
     net.w[2].mul_(400.0)  # a correction large enough that the guard must act
     net.wb[2].copy_(net.w[2].to(torch.bfloat16))
@@ -213,8 +220,8 @@ def test_energy_guard_in_step_and_never_raises_band_energy():
         g1.step(1)
         g2.step(1)
         g2.sync()
-        P = 8 * 32 * 32
-        X = torch.empty(6, 10, 8, 32, 32, device=net.dev)
+        P = 8 * n * n
+        X = torch.empty(6, 10, 8, n, n, device=net.dev)
         L.check(L.lib().wf_band_gather(g2._h, CL._p(X), net.gain_e, net.gain_h))
         torch.cuda.synchronize()
         s = torch.sqrt(torch.sum(X[:, :3].reshape(6, -1) ** 2, dim=1) / (3 * P)) + 1e-30
@@ -233,6 +240,7 @@ def test_energy_guard_in_step_and_never_raises_band_energy():
         e_before = torch.sum((F * F).reshape(6, -1).double(), dim=1)
         e_after = torch.sum(((F + Yg) ** 2).reshape(6, -1).double(), dim=1)
         assert bool(torch.all(e_after <= e_before * (1 + 1e-6)))
+        torch.cuda.synchronize()  # Yg comes from torch's stream; the scatter runs on the handle's
         L.check(L.lib().wf_band_scatter_add(g2._h, CL._p(Yg), net.gain_e, net.gain_h))
         torch.cuda.synchronize()
         got, want = g1.fields(), g2.fields()

@@ -1810,9 +1810,11 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
   h->cl_gh = gain_h;
   h->closure = true;
   // the tensor-core path's operands: packed weights and band buffers, and a
-  // TMA map over each packed band tensor (the buffers never move)
+  // TMA map over each packed band tensor (the buffers never move).  Grids
+  // narrower than one 32-voxel box row, or a map the driver refuses, keep
+  // the FP32-in path.
   h->cl_fast_ok = false;
-  if (encode_fn()) {
+  if (encode_fn() && h->nx >= 32) {
     const int n = h->nx, D = wf::kBandDepth;
     const size_t P = static_cast<size_t>(D) * n * n;
     const size_t packed = 6 * 6 * P * 16, wbytes = 6 * 27 * 512;
@@ -1831,11 +1833,11 @@ wf_status wf_set_closure(wf_handle *h, const void *w1, const void *w2, const voi
     const cuuint64_t dims[4] = {8ull * n, (cuuint64_t)n, (cuuint64_t)D, 36};
     const cuuint64_t strides[3] = {16ull * n, 16ull * n * n, 16ull * n * n * D};
     const cuuint32_t box[4] = {8 * 32, 6, 1, 6};
+    bool mapped = true;
     for (int l = 0; l < 3; ++l)
-      if (!encode(&h->cl_tm[l], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, h->cl_fast + l * packed, dims,
-                  strides, box))
-        return fail(h, WF_ERR_CUDA, "cuTensorMapEncodeTiled(closure bands) failed");
-    h->cl_fast_ok = true;
+      mapped = mapped && encode(&h->cl_tm[l], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, h->cl_fast + l * packed,
+                                dims, strides, box);
+    h->cl_fast_ok = mapped;
   }
   return WF_OK;
 }
