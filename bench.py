@@ -31,6 +31,7 @@ Rust reference cannot be built here) with all host threads.
 from __future__ import annotations
 
 import argparse
+import copy
 import json
 import os
 import statistics
@@ -192,10 +193,14 @@ def description(args, steps):
 def scenario(args, steps, device_voxelize=None):
     """The workload for the CUDA path; random spheres above 256^3 are
     voxelized on the device (the host voxelizer's 32 full-grid passes take
-    minutes at 1024^3)."""
+    minutes at 1024^3).  device_voxelize True leaves any text scene to the
+    device voxelizer (the end-to-end leg: the scene text crosses the host
+    link, not the ids)."""
     from wavefront_b200 import configs
-    dv = args.workload == "random_spheres" and (GRID > 256 if device_voxelize is None
-                                                else device_voxelize)
+    if device_voxelize is None:
+        dv = args.workload == "random_spheres" and GRID > 256
+    else:
+        dv = bool(device_voxelize)
     return configs.from_desc(description(args, steps), device_voxelize=dv)
 
 
@@ -545,11 +550,11 @@ def run_ours(args, rank, world, local_rank):
     desc = description(args, total)
     sc = scenario(args, total)
 
-    def load(g, extra=0):
+    def load(g, extra=0, sc=sc):
         """Scene or material ids, CPML profiles, tiling, source values and probe
         tables (for the run's steps plus `extra`) into a fresh handle."""
-        if sc.grid is None:
-            g.set_scene(sc.scene_text, sc.table, sc.dt, sc.dx)
+        if sc.grid is None:  # the device voxelizer registers the scene's materials
+            g.set_scene(sc.scene_text, copy.deepcopy(sc.table), sc.dt, sc.dx)
         else:
             g.set_materials(sc.grid, sc.table)
         if sc.pml is not None:
@@ -630,11 +635,15 @@ def run_ours(args, rank, world, local_rank):
     # ---- end to end through the C ABI from host buffers -----------------
     e2e_line = {"value": None, "unit": METRIC, "skipped": "--no-e2e"}
     if not args.no_e2e:
-        if sc.grid is not None:  # host ids travel pinned; a device scene sends only its text
-            pin_ids = torch.from_numpy(sc.grid.ids).pin_memory()
+        # a text scene is voxelized on the device (its ids equal the host
+        # voxelizer's), so the scene text crosses the host link, not the ids;
+        # host ids travel pinned
+        sce = scenario(args, total, device_voxelize=True) if (desc["scene"] or {}).get("text") else sc
+        if sce.grid is not None:
+            pin_ids = torch.from_numpy(sce.grid.ids).pin_memory()
         snap = torch.empty(N_CELLS * 6, dtype=torch.float32).pin_memory()
-        if sc.grid is not None:
-            sc.grid.ids = pin_ids.numpy()
+        if sce.grid is not None:
+            sce.grid.ids = pin_ids.numpy()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -649,7 +658,7 @@ def run_ours(args, rank, world, local_rank):
             if async_snap:
                 g.reserve_download()  # the snapshot's staging buffer
             tc = time.perf_counter()
-            load(g)
+            load(g, sc=sce)
             g.sync()
             t_built = time.perf_counter()
             # with `snapshot`, the FieldBlock snapshot of step 0, as the
@@ -683,14 +692,15 @@ def run_ours(args, rank, world, local_rank):
         if dist:
             dist.barrier()
         e2e = whole_job_value(world, N_CELLS, args.steps, e2e_s)
-        h2d = (N_CELLS if sc.grid is not None else len(sc.scene_text)) + 256 * 16 + total * (4 + 8 * 16)
+        h2d = (N_CELLS if sce.grid is not None else len(sce.scene_text)) + 256 * 16 + total * (4 + 8 * 16)
         d2h = nsums * (8 * 2 + 8)
         e2e_line = {"value": round(e2e, 1), "unit": METRIC,
                     "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h / args.steps),
                     "includes": "the handle's creation (device memory from the library's "
-                                "cache, warmed by the first handle of the run), scene or material "
-                                "upload (pinned), CPML and source/probe table uploads, K steps, "
+                                "cache, warmed by the first handle of the run), the scene text "
+                                "voxelized on the device (or material ids uploaded pinned), CPML "
+                                "and source/probe table uploads, K steps, "
                                 "every probe's DFT sums read back (the run's result)",
                     "phases_ms": phases,
                     "with_snapshot": {
