@@ -173,7 +173,10 @@ wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
 
 /* Enqueues nsteps full timesteps: H everywhere, E everywhere, sources in
  * order, probes (src/engine.rs:747-782).  Asynchronous on the handle's
- * stream; long runs replay captured CUDA graphs. */
+ * stream; long runs replay captured CUDA graphs.  The fused step forks its
+ * work classes onto side streams forked from and joined back to the handle's
+ * stream; the handle takes them at its first fused step, from a per-device
+ * cache of idle sets that wf_destroy refills. */
 wf_status wf_step(wf_handle *h, int nsteps);
 /* Waits for the stream and reports any latched device error. */
 wf_status wf_sync(wf_handle *h);
