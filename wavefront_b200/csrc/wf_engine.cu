@@ -89,6 +89,7 @@ struct wf_handle {
   std::vector<ProbeRec> probes;
   SrcDev *d_src = nullptr;
   ProbeDev *d_probe = nullptr;
+  bool tables_dirty = false;  // d_src / d_probe lag srcs / probes (flush_tables)
   long long *d_step = nullptr;
   int *d_err = nullptr;
   long long steps_done = 0;
@@ -551,6 +552,8 @@ cudaError_t closure_enqueue(wf_handle *h) {
 }
 
 // Tail arguments of a step that reads buffer h->cur (16-bit fields included).
+wf_status flush_tables(wf_handle *h);  // below, with the descriptor upload
+
 TailArgs tail_args(const wf_handle *h) {
   TailArgs t{};
   t.f = h->fld[h->cur ^ 1];
@@ -678,6 +681,10 @@ wf_status enqueue_one(wf_handle *h) {
   }
   // 16-bit storage always runs the tail: it picks the next step's shifts
   if (!h->srcs.empty() || !h->probes.empty() || store16(h)) {
+    if (h->tables_dirty) {
+      wf_status s = flush_tables(h);
+      if (s != WF_OK) return s;
+    }
     e = wf::launch_tail(tail_args(h), h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "tail kernel launch");
     h->kernel_launches += 1;
@@ -689,6 +696,10 @@ wf_status enqueue_one(wf_handle *h) {
 // 16-bit storage: the slab maxima of the current state (from its data) and
 // the shifts the next step writes with.
 wf_status refresh_shifts(wf_handle *h) {
+  if (h->tables_dirty) {  // the tail arguments below hold the descriptor arrays
+    wf_status s = flush_tables(h);
+    if (s != WF_OK) return s;
+  }
   WF_CUDA(h, wf::launch_state_max(h->fld[h->cur], h->precision, h->nx, h->ny, h->nz,
                                   h->shift[h->cur], h->slab_max, h->stream));
   TailArgs t = tail_args(h);
@@ -702,6 +713,7 @@ wf_status upload_src_probe_tables(wf_handle *h) {
   drop_graphs(h);
   ++h->version;
   h->shifts_dirty = true;  // source amplitudes enter the 16-bit shifts
+  h->tables_dirty = false;
   if (h->d_src) wf::dev_free(h->d_src);
   if (h->d_probe) wf::dev_free(h->d_probe);
   h->d_src = nullptr;
@@ -721,6 +733,29 @@ wf_status upload_src_probe_tables(wf_handle *h) {
   return WF_OK;
 }
 
+// A source or probe was added: its descriptor array is uploaded once, before
+// the next step or batch build (flush_tables), rather than after every add;
+// captured graphs and batch tables that hold the old arrays are dropped now.
+void tables_changed(wf_handle *h) {
+  drop_graphs(h);
+  ++h->version;
+  h->shifts_dirty = true;
+  h->tables_dirty = true;
+}
+
+// Uploads the descriptor arrays if an add left them stale.  Outside any
+// stream capture (it allocates and synchronizes).
+// The 16-bit shift flag is left as it is: the add itself set it, and a
+// checkpoint restore since then may have cleared it (the restored shifts are
+// the ones the next step must use).
+wf_status flush_tables(wf_handle *h) {
+  if (!h->tables_dirty) return WF_OK;
+  const bool shifts_dirty = h->shifts_dirty;
+  const wf_status s = upload_src_probe_tables(h);
+  h->shifts_dirty = shifts_dirty;
+  return s;
+}
+
 bool tables_cover(const wf_handle *h, long long upto, std::string *why) {
   for (size_t i = 0; i < h->srcs.size(); ++i)
     if (h->srcs[i].d.nvals < upto) {
@@ -737,13 +772,17 @@ bool tables_cover(const wf_handle *h, long long upto, std::string *why) {
   return true;
 }
 
-wf_status check_device_error(wf_handle *h) {
-  int flag = 0;
-  WF_CUDA(h, cudaMemcpy(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+wf_status device_error_status(wf_handle *h, int flag) {
   if (flag & wf::kErrTimeout)
     return fail(h, WF_ERR_TIMEOUT, "a device-side bounded wait timed out (TMA stage never arrived)");
   if (flag) return fail(h, WF_ERR_DEVICE_FLAG, "device error flag set: " + std::to_string(flag));
   return WF_OK;
+}
+
+wf_status check_device_error(wf_handle *h) {
+  int flag = 0;
+  WF_CUDA(h, cudaMemcpy(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  return device_error_status(h, flag);
 }
 
 }  // namespace
@@ -876,6 +915,7 @@ wf_status batch_build(wf_batch *b) {
       h->cfg_user_set = true;
       st = build_maps(h, false);  // the batched kernel tiles the whole x range
     }
+    if (st == WF_OK) st = flush_tables(h);
     if (st != WF_OK) return st;
     const int cur = h->cur;
     for (int p = 0; p < 2; ++p) {
@@ -1070,9 +1110,13 @@ wf_status wf_create(const wf_grid_desc *d, wf_handle **out) {
     h->own_stream = true;
   }
   // (the side streams of the fused step are taken at its first use, acquire_streams)
+  // Only the state the first step reads starts at zero: every step writes
+  // every cell of the other buffer before anything reads it (the work classes
+  // of the fused step, or the split H and E passes, cover the whole grid).
   for (int b = 0; b < 2; ++b) {
     e = wf::dev_alloc(&h->fld[b], elem_bytes(h) * 6 * h->N);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMalloc(fields)"));
+    if (b != h->cur) continue;
     e = cudaMemsetAsync(h->fld[b], 0, elem_bytes(h) * 6 * h->N, h->stream);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(nullptr, e, "cudaMemset(fields)"));
   }
@@ -1340,7 +1384,8 @@ wf_status wf_add_source(wf_handle *h, int x, int y, int z, int comp, int mode,
   r.d.vals = r.vals;
   h->srcs.push_back(r);
   if (out_index) *out_index = static_cast<int>(h->srcs.size()) - 1;
-  return upload_src_probe_tables(h);
+  tables_changed(h);
+  return WF_OK;
 }
 
 wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
@@ -1358,19 +1403,26 @@ wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
   const size_t tab = static_cast<size_t>(nsteps) * nfreq;
   const size_t total = 2 * tab + 2 * static_cast<size_t>(nfreq) + 1;
   WF_CUDA(h, wf::dev_alloc(&r.base, sizeof(double) * total));
-  WF_CUDA(h, memset_sync(r.base, 0, sizeof(double) * total, h->stream));
   r.cos_tab = r.base;
   r.sin_tab = r.base + tab;
   r.sc = r.base + 2 * tab;
   r.ss = r.sc + nfreq;
-  if (tab) {
-    WF_CUDA(h, h2d_sync(r.cos_tab, cos_tab, sizeof(double) * tab, h->stream));
-    WF_CUDA(h, h2d_sync(r.sin_tab, sin_tab, sizeof(double) * tab, h->stream));
+  // one copy lays out the whole block (cos and sin tables, then zeroed DFT
+  // sums); the count and the trace are cleared on the stream, and the copy
+  // at the end of the call waits for all three
+  {
+    std::vector<double> blk(total, 0.0);
+    if (tab) {
+      std::memcpy(blk.data(), cos_tab, sizeof(double) * tab);
+      std::memcpy(blk.data() + tab, sin_tab, sizeof(double) * tab);
+    }
+    WF_CUDA(h, cudaMemcpyAsync(r.base, blk.data(), sizeof(double) * total, cudaMemcpyHostToDevice,
+                               h->stream));
   }
   WF_CUDA(h, wf::dev_alloc(&r.n, sizeof(unsigned long long)));
-  WF_CUDA(h, memset_sync(r.n, 0, sizeof(unsigned long long), h->stream));
+  WF_CUDA(h, cudaMemsetAsync(r.n, 0, sizeof(unsigned long long), h->stream));
   WF_CUDA(h, wf::dev_alloc(&r.trace, sizeof(float) * std::max(nsteps, 1)));
-  WF_CUDA(h, memset_sync(r.trace, 0, sizeof(float) * std::max(nsteps, 1), h->stream));
+  WF_CUDA(h, cudaMemsetAsync(r.trace, 0, sizeof(float) * std::max(nsteps, 1), h->stream));
   r.d.comp = comp;
   r.d.x = x;
   r.d.y = y;
@@ -1387,7 +1439,9 @@ wf_status wf_add_probe(wf_handle *h, int x, int y, int z, int comp, int nfreq,
   r.d.trace = r.trace;
   h->probes.push_back(r);
   if (out_index) *out_index = static_cast<int>(h->probes.size()) - 1;
-  return upload_src_probe_tables(h);
+  tables_changed(h);
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));  // complete on return, as every set-up call
+  return WF_OK;
 }
 
 wf_status wf_step(wf_handle *h, int nsteps) {
@@ -1406,6 +1460,10 @@ wf_status wf_step(wf_handle *h, int nsteps) {
   }
   if (use_fused(h) && !h->fork_ev) {  // the side streams, outside any capture too
     wf_status s = acquire_streams(h);
+    if (s != WF_OK) return s;
+  }
+  if (h->tables_dirty) {  // sources/probes added since the last step
+    wf_status s = flush_tables(h);
     if (s != WF_OK) return s;
   }
   if (store16(h) && h->shifts_dirty) {
@@ -1500,16 +1558,22 @@ int64_t wf_kernel_launches(const wf_handle *h) { return h ? h->kernel_launches :
 wf_status wf_probe_sums(wf_handle *h, int p, double *c, double *s, uint64_t *n) {
   if (!h || p < 0 || p >= static_cast<int>(h->probes.size())) return fail(h, WF_ERR_ARG, "bad probe index");
   DeviceGuard guard(h->dev);
-  WF_CUDA(h, cudaStreamSynchronize(h->stream));
   const ProbeRec &r = h->probes[p];
-  if (c && r.d.nfreq) WF_CUDA(h, cudaMemcpy(c, r.sc, sizeof(double) * r.d.nfreq, cudaMemcpyDeviceToHost));
-  if (s && r.d.nfreq) WF_CUDA(h, cudaMemcpy(s, r.ss, sizeof(double) * r.d.nfreq, cudaMemcpyDeviceToHost));
-  if (n) {
-    unsigned long long v = 0;
-    WF_CUDA(h, cudaMemcpy(&v, r.n, sizeof(v), cudaMemcpyDeviceToHost));
-    *n = v;
-  }
-  return check_device_error(h);
+  // the cos and sin sums are adjacent: one copy of both, plus the count and
+  // the error flag, read on the handle's stream after the steps, one wait
+  std::vector<double> cs(2 * static_cast<size_t>(r.d.nfreq));
+  unsigned long long v = 0;
+  int flag = 0;
+  if (!cs.empty())
+    WF_CUDA(h, cudaMemcpyAsync(cs.data(), r.sc, sizeof(double) * cs.size(), cudaMemcpyDeviceToHost,
+                               h->stream));
+  if (n) WF_CUDA(h, cudaMemcpyAsync(&v, r.n, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  WF_CUDA(h, cudaMemcpyAsync(&flag, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  WF_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (c) std::copy(cs.begin(), cs.begin() + r.d.nfreq, c);
+  if (s) std::copy(cs.begin() + r.d.nfreq, cs.end(), s);
+  if (n) *n = v;
+  return device_error_status(h, flag);
 }
 
 wf_status wf_probe_trace(wf_handle *h, int p, float *out, int n) {
