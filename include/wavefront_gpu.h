@@ -432,7 +432,9 @@ wf_status wf_batch_autotune(wf_batch *b, int steps, wf_tiling *best, float *best
  * CUDA's page mapping.  Freeing waits for the device first, as cudaFree
  * does.  An allocation that runs out of memory returns the device's cache
  * to CUDA and tries again.  wf_release_cached_memory returns the cache of
- * `device` (-1: every device) to CUDA now; wf_cached_bytes reports it. */
+ * `device` (-1: every device) to CUDA now, and destroys the idle side-stream
+ * sets kept for the fused step (call it before resetting a device that the
+ * library has used); wf_cached_bytes reports the cached bytes. */
 wf_status wf_release_cached_memory(int device);
 int64_t wf_cached_bytes(int device);
 

@@ -292,6 +292,29 @@ void release_streams(wf_handle *h) {
   destroy_set(ss);
 }
 
+}  // namespace
+
+namespace wf {
+
+void release_idle_stream_sets(int dev) {
+  std::map<int, std::vector<StreamSet>> sets;
+  {
+    std::lock_guard<std::mutex> lk(g_sets_mu);
+    for (auto &kv : g_idle_sets) {
+      if (dev >= 0 && kv.first != dev) continue;
+      sets[kv.first].swap(kv.second);
+    }
+  }
+  for (auto &kv : sets) {
+    DeviceGuard guard(kv.first);
+    for (auto &ss : kv.second) destroy_set(ss);
+  }
+}
+
+}  // namespace wf
+
+namespace {
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {

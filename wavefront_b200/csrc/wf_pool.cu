@@ -132,6 +132,7 @@ extern "C" {
 
 wf_status wf_release_cached_memory(int device) {
   wf::dev_release(device);
+  wf::release_idle_stream_sets(device);
   return WF_OK;
 }
 

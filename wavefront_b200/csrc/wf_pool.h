@@ -17,5 +17,7 @@ cudaError_t dev_alloc(T **p, size_t n) {
 void dev_free(void *p);
 size_t dev_cached_bytes(int dev);
 void dev_release(int dev);  // -1: every device
+// Destroys the idle stream sets the fused step keeps per device (wf_engine.cu).
+void release_idle_stream_sets(int dev);  // -1: every device
 
 }  // namespace wf
