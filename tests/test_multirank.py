@@ -150,3 +150,20 @@ def test_bench_slab_leg_two_gloo_ranks(tmp_path):
                                        abs=0.06)
     assert d["e2e"]["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] > 0
     assert d["config"]["rank0_planes_stepped_per_step"] == 32 + 8
+
+
+def test_e2e_leg_sends_the_scene_text(monkeypatch):
+    """The e2e leg's workload leaves a text scene to the device voxelizer
+    (only the text crosses the host link); the device-resident leg keeps the
+    host-voxelized ids; a scene without text (demo sphere) keeps its ids."""
+    import argparse
+    from wavefront_b200 import configs
+    monkeypatch.setattr(bench, "GRID", 64)
+    args = argparse.Namespace(workload="two_spheres")
+    dev = bench.scenario(args, 10, device_voxelize=True)
+    host = bench.scenario(args, 10)
+    assert dev.grid is None and dev.scene_text == configs.two_spheres_text(64)
+    assert host.grid is not None and host.scene_text is None
+    assert host.grid.ids.any()
+    demo = bench.scenario(argparse.Namespace(workload="demo_sphere"), 10, device_voxelize=True)
+    assert demo.grid is not None and demo.scene_text is None
