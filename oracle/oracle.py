@@ -305,8 +305,9 @@ class Sim:
 
     def set_storage(self, kind: str):
         """16-bit field storage emulation: "f32" (off), "f16" or "bf16" (both
-        round to nearest even).  Call after the sources are added (their
-        amplitudes enter the shifts)."""
+        round to nearest even), or "f16r8" (binary16 plus a residual byte,
+        an emulation with no device form, for the error study).  Call after
+        the sources are added (their amplitudes enter the shifts)."""
         if self._f("set_storage")(self._h, STORAGE_KINDS[kind]) != 0:
             raise ValueError("storage emulation needs the f32 oracle")
 
@@ -322,7 +323,9 @@ class Sim:
         return np.array(e[:], np.int32), np.array(h[:], np.int32)
 
 
-STORAGE_KINDS = {"f32": 0, "f16": 1, "bf16": 2}
+# "f16r8" (emulation only, no device form): binary16 plus a residual byte
+# per value, the byte cost of a compensated store, for the error study
+STORAGE_KINDS = {"f32": 0, "f16": 1, "bf16": 2, "f16r8": 3}
 
 
 def store_shift(bound: float) -> int:

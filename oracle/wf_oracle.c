@@ -332,10 +332,20 @@ static inline float or_round_bf16(float v) {
  * even.  The result is exactly what a device kernel reads back after storing
  * u in that format. */
 float or_round16(float u, int kind) {
-  if (kind == 1) {
+  if (kind == 1 || kind == 3) {
     if (u > 65504.0f) u = 65504.0f;
     if (u < -65504.0f) u = -65504.0f;
-    return (float)(_Float16)u;
+    const float h = (float)(_Float16)u;
+    if (kind == 1) return h;
+    /* kind 3 (emulation only, no device form): binary16 plus a residual
+     * byte, the rounding error u - h (exact in f32) rounded to a signed
+     * multiple of 1/256 of h's last place; h + residual is exact in f32
+     * (at most 19 significant bits). */
+    const float ulp = fabsf(h) >= 6.103515625e-05f ? ldexpf(1.0f, ilogbf(h) - 10)
+                                                   : ldexpf(1.0f, -24);
+    float q = rintf((u - h) / ulp * 256.0f);
+    q = q > 127.0f ? 127.0f : (q < -128.0f ? -128.0f : q);
+    return h + q * (ulp / 256.0f);
   }
   return or_round_bf16(u);
 }
